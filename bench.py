@@ -1,0 +1,355 @@
+"""Benchmark: batched symmetric eigendecompositions per second on B200.
+
+Default workload: the ensemble-covariance-like (LETKF-style) batch,
+L = 4096 matrices of n = 128, FP64, A = (k-1) I + Y^T Y with Y k x n iid
+N(0,1)/sqrt(n), k = n; full eigenvalues + eigenvectors, sorted.  A step is
+one solve of one batch; each step solves its own pristine copy (all copies
+are resident in HBM before the timed region; one batch is 537 MB, larger
+than L2, so no flush is needed).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank solves its own batch (independent matrices, no
+collective on the data path: weak scaling); time = max over ranks.
+
+`--impl reference` times the reference method on the host cores instead:
+the CPU restatement of the reference's tred1 -> tql2 -> hhtr2sy path
+(oracle/, OpenMP over matrices, all threads), on a bounded sample per step.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "eigeng-batched_b200"))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--L", type=int, default=4096)
+    ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
+    ap.add_argument("--family", default="letkf", choices=["letkf", "symu"])
+    ap.add_argument("--method", default="tql2", choices=["tql2", "imtql2", "jacobi"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--extra", action="store_true", help="also time n=32 (L=16384) and n=256 (L=2048)")
+    ap.add_argument("--out", default=None, help="also append the JSON line to this file")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_batch(torch, family, L, n, dtype, seed, device):
+    """Seeded synthetic batch generated on the device (column-major matrices,
+    symmetric).  LETKF-style: (n-1) I + Y^T Y, Y n x n iid N(0,1)/sqrt(n)."""
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    out = torch.empty((L, n, n), dtype=dtype, device=device)
+    step = 256
+    for s in range(0, L, step):
+        e = min(L, s + step)
+        if family == "letkf":
+            y = torch.randn((e - s, n, n), generator=g, dtype=torch.float64, device=device) / np.sqrt(n)
+            a = y.transpose(1, 2) @ y + (n - 1) * torch.eye(n, dtype=torch.float64, device=device)
+        else:
+            b = torch.rand((e - s, n, n), generator=g, dtype=torch.float64, device=device) * 2 - 1
+            a = 0.5 * (b + b.transpose(1, 2))
+        out[s:e] = a.to(dtype)
+    return out
+
+
+def alg_bytes(n, esize):
+    """Compulsory bytes per matrix: read A, write V and w (SURVEY 8(d) model)."""
+    return esize * (2 * n * n + n)
+
+
+def phase_bytes(n, esize, recs):
+    """Algorithmic bytes per matrix of each phase: 1 reads A and writes Q, d, e;
+    2 reads d, e and writes the rotation records and w; 3 reads Q, the
+    records and w and writes V and w."""
+    rb = 2 * esize * recs
+    return (esize * (2 * n * n + 2 * n), esize * 3 * n + rb, esize * (2 * n * n + 2 * n) + rb)
+
+
+def cpu_time_oracle(a_np, n, method, budget_s, nthreads):
+    """Times the CPU restatement on a bounded sample: repeats solves of a
+    fresh copy of the sample until budget_s seconds have passed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.lib()
+    done, t0 = 0, time.perf_counter()
+    while True:
+        a = a_np.copy()
+        O.eigen_batch(a, n, method=method, nthreads=nthreads)
+        done += a_np.shape[0]
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            return done / el, done, el
+
+
+def run_reference(args):
+    """Reference arm: the reference method on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    nth = os.cpu_count() or 1
+    dt = np.float64 if args.dtype == "f64" else np.float32
+    n = args.n
+    per = max(1.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
+    sample = max(nth, 64)
+    gen = O.letkf_like if args.family == "letkf" else O.sym_uniform
+    a_np = gen(sample, n, seed=1).astype(dt)
+    method = {"tql2": 0, "imtql2": 1, "jacobi": 2}[args.method]
+    for _ in range(args.warmup):
+        cpu_time_oracle(a_np[: max(1, nth)], n, method, 0.0, nth)
+    rates = []
+    for _ in range(args.steps):
+        r, cnt, el = cpu_time_oracle(a_np, n, method, per, nth)
+        rates.append(r)
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": f"eigendecomps/s (n={n}, {args.dtype}, {args.family}, L={args.L})",
+        "value": value, "unit": "matrices/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * args.L / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.dtype, "data": "synthetic (seeded, same family and shape)",
+        "config": {"workload": f"{args.family} L={args.L} n={n} {args.dtype} {args.method} sorted",
+                   "L_per_gpu": args.L, "n": n},
+        "cpu_baseline": {"value": value, "unit": "matrices/s", "cores": nth, "kind": "port",
+                         "sample": f"{sample} matrices of the workload family re-solved for ~{per:.0f} s per step"},
+        "e2e": {"value": value, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    import eigeng_b200 as E
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    dt = torch.float64 if args.dtype == "f64" else torch.float32
+    esize = 8 if dt == torch.float64 else 4
+    n, L = args.n, args.L
+    method = {"tql2": E.TQL2, "imtql2": E.IMTQL2, "jacobi": E.JACOBI}[args.method]
+    nbuf = args.steps + args.warmup
+    base = make_batch(torch, args.family, L, n, dt, seed=1234 + rank, device=dev)
+    copies = [base.clone() for _ in range(nbuf)]
+    w = torch.empty((L, n), dtype=dt, device=dev)
+    info = torch.zeros(L, dtype=torch.int32, device=dev)
+    wk = E.workspace(L, n, n, dt, dev) if method != E.JACOBI else None
+    stream = torch.cuda.current_stream()
+
+    def solve(a):
+        st = E.eigen_GPU_batch_ex(a, w, wk, n, info=info, method=method, stream=stream)
+        if st != 0:
+            raise RuntimeError(f"solve failed: cudaError {st}")
+
+    for i in range(args.warmup):
+        solve(copies[i])
+    barrier()
+    # correctness of the timed configuration: the reference's gate on copy 0
+    e1, e2, fl = E.check(base, w, copies[args.warmup - 1] if args.warmup else copies[0], n)
+    torch.cuda.synchronize()
+    gate_fail = int((fl != 0).sum().item())
+    info_fail = int((info != 0).sum().item())
+
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        t0.record(stream)
+        for i in range(args.steps):
+            solve(copies[args.warmup + i])
+        t1.record(stream)
+        barrier()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * L * args.steps / (ms / 1000.0)
+
+    # per-phase kernel times on the launching stream (one extra traced solve
+    # per step count, same inputs as the timed region)
+    phases = []
+    for i in range(args.steps):
+        a = base.clone()
+        with E.PhaseTrace(chunks=1) as tr:
+            solve(a)
+        phases.extend(tr.ms())
+    ph = np.array(phases).mean(axis=0) if phases else np.zeros(3)
+    hbm, peak_kind = peaks()
+
+    # record counts (mean rotations per matrix) for the algorithmic byte model
+    recs = 1.1 * n * n
+    pb = phase_bytes(n, esize, recs)
+    names = ["tridiag_qt", "ql_rotations", "apply_rotations"]
+    dom = int(np.argmax(ph))
+    achieved = pb[dom] * L / (ph[dom] / 1000.0) / 1e9 if ph[dom] > 0 else 0.0
+
+    line = {
+        "metric": f"eigendecomps/s (n={n}, {args.dtype}, {args.family}, L={L})",
+        "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.dtype, "data": "synthetic (seeded on device; LETKF-like family of the config)",
+        "config": {"workload": f"{args.family} L={L} n={n} {args.dtype} {args.method} sorted",
+                   "L_per_gpu": L, "n": n, "l2_flush": "inputs larger than L2 (fresh copy per step)",
+                   "parallelism": f"replicas x{world} (independent matrices)"},
+        "gpu_launches": 3 * args.steps,
+        "correctness": {"reference_gate_flags": gate_fail, "info_nonzero": info_fail,
+                        "max_err1": float(e1.max().item()), "max_err2": float(e2.max().item())},
+        "phases_ms": {k: float(v) for k, v in zip(names, ph)},
+        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                     "alg_bytes_per_matrix": pb[dom]},
+        "hbm_fraction_whole_solve": alg_bytes(n, esize) * value / world / 1e9 / hbm,
+        "clocks": clk.summary(),
+    }
+
+    if not args.no_e2e:
+        # end to end through the C ABI with host buffers: pinned H2D of the
+        # inputs, solve, D2H of eigenvectors and eigenvalues, every step
+        host_in = base.cpu().pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        host_w = torch.empty((L, n), dtype=dt).pin_memory()
+        dev_a = torch.empty_like(base)
+        for _ in range(2):
+            dev_a.copy_(host_in, non_blocking=True)
+            solve(dev_a)
+            host_out.copy_(dev_a, non_blocking=True)
+            host_w.copy_(w, non_blocking=True)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1_ = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            dev_a.copy_(host_in, non_blocking=True)
+            solve(dev_a)
+            host_out.copy_(dev_a, non_blocking=True)
+            host_w.copy_(w, non_blocking=True)
+        e1_.record(stream)
+        barrier()
+        ems = e0.elapsed_time(e1_)
+        if world > 1:
+            tt = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        line["e2e"] = {"value": world * L * args.steps / (ems / 1000.0), "unit": "matrices/s",
+                       "h2d_bytes_per_step": L * n * n * esize, "d2h_bytes_per_step": L * n * n * esize + L * n * esize}
+
+    if rank == 0 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        nth = os.cpu_count() or 1
+        sample = base[: max(64, nth)].cpu().numpy().reshape(-1, n, n)
+        r, cnt, el = cpu_time_oracle(sample, n, {"tql2": 0, "imtql2": 1, "jacobi": 2}[args.method], 10.0, nth)
+        line["cpu_baseline"] = {"value": r, "unit": "matrices/s", "cores": nth, "kind": "port",
+                                "sample": f"{sample.shape[0]} matrices of the workload re-solved {cnt // sample.shape[0]}x "
+                                          f"in {el:.1f} s"}
+
+    if rank == 0:
+        s = json.dumps(line)
+        print(s, flush=True)
+        if args.out:
+            with open(args.out, "a") as f:
+                f.write(s + "\n")
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+// Common device helpers of the B200 batched symmetric eigensolver.
+//
+// Storage convention everywhere: column-major, element (r, c) of a matrix
+// with leading dimension ld at p[r + c*ld] (0-based).  Matrix k of a batch
+// starts at a + k*nm*n and its eigenvalues at w + k*n, as in the reference
+// (eigen_GPU_batch.cu:89-90, eigen_GPU_batch.hpp:104-118).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace eigb {
+
+template <class T> struct Num;
+template <> struct Num<double> {
+  static __host__ __device__ constexpr double eps() { return 2.220446049250313080847e-16; }
+  // QL deflation tolerance factor of the reference, tql2_tiled.hpp:8
+  static __host__ __device__ constexpr double tolmul() { return 512.0; }
+};
+template <> struct Num<float> {
+  static __host__ __device__ constexpr float eps() { return 1.1920928955078125e-07f; }
+  static __host__ __device__ constexpr float tolmul() { return 16.0f; }
+};
+
+// 1/sqrt(x): CUDA's double rsqrt (1 ulp) and the correctly rounded float
+// intrinsic.
+__device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsq(float x) { return __frsqrt_rn(x); }
+__device__ __forceinline__ double sqr_t(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqr_t(float x) { return sqrtf(x); }
+__device__ __forceinline__ double fabs_t(double x) { return fabs(x); }
+__device__ __forceinline__ float fabs_t(float x) { return fabsf(x); }
+__device__ __forceinline__ double fmax_t(double x, double y) { return fmax(x, y); }
+__device__ __forceinline__ float fmax_t(float x, float y) { return fmaxf(x, y); }
+__device__ __forceinline__ double copysign_t(double x, double y) { return copysign(x, y); }
+__device__ __forceinline__ float copysign_t(float x, float y) { return copysignf(x, y); }
+
+// Zero guard used wherever the reference divides by a possibly vanishing
+// product (misc_gpu.hpp:474-509 flip0to1).
+template <class T> __device__ __forceinline__ T flip0to1(T x) { return x == T(0) ? T(1) : x; }
+
+// Plane rotation for (a, b): r = hypot(a, b), c = a/r, s = b/r, with one
+// reciprocal square root instead of a square root and two divisions.  For
+// a = b = 0 it returns the identity (c = 1, s = 0, r = 0).  Like the
+// reference's pythag (misc_gpu.hpp:533-548) the squares are formed
+// unscaled, so |a|,|b| must stay below sqrt(overflow threshold).
+template <class T>
+__device__ __forceinline__ void givens(T a, T b, T &c, T &s, T &r)
+{
+  const T sig = fma(a, a, b * b);
+  if (sig > T(0)) {
+    const T y = rsq(sig);
+    c = a * y;
+    s = b * y;
+    r = sig * y;
+  } else {
+    c = T(1);
+    s = T(0);
+    r = T(0);
+  }
+}
+
+// sqrt(p*p + 1) without overflow for large |p| (the shift of tql2/imtql2,
+// reference pythag1, misc_gpu.hpp:514-530).
+template <class T>
+__device__ __forceinline__ T hypot1(T p)
+{
+  const T ap = fabs_t(p);
+  const T big = T(sizeof(T) == 8 ? 1e150 : 1e18);
+  return ap > big ? ap : sqr_t(fma(p, p, T(1)));
+}
+
+// Rotation records: a record is (c, s); a segment header carries two ints
+// (top rotation index i0, number of rotations that follow).  A segment
+// applies rotations i0, i0-1, ..., i0-cnt+1, rotation i acting on columns
+// (i, i+1) of Z:  z_{i+1} <- s z_i + c z_{i+1},  z_i <- c z_i - s z_{i+1}
+// (tql2_tiled.hpp:116-121 chain order).
+template <class T> struct __align__(2 * sizeof(T)) Rec { T c, s; };
+
+__device__ __forceinline__ Rec<double> make_hdr(int i0, int cnt, double)
+{
+  Rec<double> h;
+  h.c = __longlong_as_double((long long)i0);
+  h.s = __longlong_as_double((long long)cnt);
+  return h;
+}
+__device__ __forceinline__ Rec<float> make_hdr(int i0, int cnt, float)
+{
+  Rec<float> h;
+  h.c = __int_as_float(i0);
+  h.s = __int_as_float(cnt);
+  return h;
+}
+__device__ __forceinline__ int hdr_i0(const Rec<double> &h) { return (int)__double_as_longlong(h.c); }
+__device__ __forceinline__ int hdr_cnt(const Rec<double> &h) { return (int)__double_as_longlong(h.s); }
+__device__ __forceinline__ int hdr_i0(const Rec<float> &h) { return __float_as_int(h.c); }
+__device__ __forceinline__ int hdr_cnt(const Rec<float> &h) { return __float_as_int(h.s); }
+
+// Per-matrix status block in the workspace.
+struct Meta {
+  int nrec;      // records written by the QL pass
+  int overflow;  // 1: record capacity exceeded, the apply pass regenerates
+  int ierr;      // 0 or the failing QL index (1-based, as the reference)
+  int pad;
+};
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T x)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__device__ __forceinline__ int warp_min_int(int x)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+
+// A team is the set of threads that cooperate on one matrix: one warp
+// (several independent matrices per CTA) or the whole CTA.
+struct WarpTeam {
+  int rank;  // 0..31
+  __device__ WarpTeam() : rank(threadIdx.x & 31) {}
+  __device__ __forceinline__ int size() const { return 32; }
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+  // Sum over the warp, result in every lane; the trailing __syncwarp orders
+  // the shared-memory accesses around it like the CTA barrier does.
+  template <class T> __device__ __forceinline__ T sum(T x, T *)
+  {
+    x = warp_sum(x);
+    __syncwarp();
+    return x;
+  }
+};
+
+struct CtaTeam {
+  int rank;
+  int nthr;
+  int flip;
+  __device__ CtaTeam() : rank(threadIdx.x), nthr(blockDim.x), flip(0) {}
+  __device__ __forceinline__ int size() const { return nthr; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  // Sum over the CTA, result in every thread.  `red` holds 2*32 slots; the
+  // two halves alternate so back-to-back reductions need one barrier each.
+  template <class T> __device__ __forceinline__ T sum(T x, T *red)
+  {
+    x = warp_sum(x);
+    T *buf = red + (flip ? 32 : 0);
+    flip ^= 1;
+    if ((rank & 31) == 0) buf[rank >> 5] = x;
+    __syncthreads();
+    const int nw = (nthr + 31) >> 5;
+    T s = T(0);
+    for (int k = 0; k < nw; k++) s += buf[k];
+    return s;
+  }
+};
+
+}  // namespace eigb

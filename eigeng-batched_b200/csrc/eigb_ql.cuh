@@ -1,0 +1,263 @@
+// Phase 2: QL iteration on the tridiagonal (d, e), emitting plane rotations.
+//
+// The eigenvalue recurrence of QL is a serial chain per matrix; it does not
+// depend on the eigenvectors.  It therefore runs one matrix per thread
+// (a warp advances 32 independent chains at once) and writes the rotations
+// as a stream of records that phase 3 applies to Q with a whole team per
+// matrix.  The same generator also runs inside phase 3 (one thread, small
+// chunks) for the rare matrix whose stream exceeded its capacity.
+//
+// The generator is resumable: it returns when the output buffer is full,
+// keeping every loop variable in QLGen, and continues from the same
+// rotation on the next call.
+//
+// tql2: explicit-shift QL, tql2_tiled.hpp:3-192 / tql2.hpp:3-213.
+// imtql2: implicit Wilkinson-shift QL, imtql2_tiled.hpp:3-176 / imtql2.hpp.
+// Deflation tolerances, the sweep limit and the e(n) = 0 convention follow
+// the reference; the rotation (c, s, r) is formed with one reciprocal
+// square root (givens()) rather than hypot + two divisions.
+#pragma once
+#include "eigb_common.cuh"
+
+namespace eigb {
+
+enum { QL_TQL2 = 0, QL_IMTQL2 = 1 };
+enum { PC_START = 0, PC_ROT = 1, PC_DONE = 2 };
+
+template <class T> struct QLGen {
+  int pc, l, m, i, itr, ierr;
+  int seg_pos, seg_cnt, seg_i0;
+  T shift, tst1, c, c2, c3, s, s2, p, el1, dl1, ei, di1, r, delta;
+};
+
+// Strided view of one chain's d and e (interleaved across the threads of a
+// block so that divergent indices stay bank-conflict free).
+template <class T> struct DEView {
+  T *d, *e;
+  int st;
+  __device__ __forceinline__ T &D(int i) const { return d[(size_t)i * st]; }
+  __device__ __forceinline__ T &E(int i) const { return e[(size_t)i * st]; }
+};
+
+template <class T>
+__device__ __forceinline__ void ql_close_seg(QLGen<T> &g, Rec<T> *buf)
+{
+  if (g.seg_pos >= 0) {
+    buf[g.seg_pos] = make_hdr(g.seg_i0, g.seg_cnt, T(0));
+    g.seg_pos = -1;
+  }
+}
+
+// Runs until done or until `cap` records are in buf; returns the number of
+// records written.  g.pc == PC_DONE when the iteration has finished; then
+// g.ierr is 0 or the failing index l (1-based, tql2_tiled.hpp:138).
+template <class T>
+__device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec<T> *buf, const int cap,
+                       const int max_sweep)
+{
+  const T tol = Num<T>::eps() * Num<T>::tolmul();
+  int nrec = 0;
+  if (g.pc == PC_DONE) return 0;
+  if (g.pc == PC_ROT) goto resume_rot;
+  g.ierr = 0;
+  g.shift = T(0);
+  g.tst1 = T(0);
+  g.seg_pos = -1;
+  if (n <= 1) goto finish;
+  for (g.l = 0; g.l < n; g.l++) {
+    {
+      const T t = (fabs_t(v.D(g.l)) + fabs_t(v.E(g.l))) * tol;
+      g.tst1 = fmax_t(g.tst1, t);
+      int m = g.l;
+      while (m < n && !(fabs_t(v.E(m)) <= g.tst1)) m++;
+      if (m >= n) {  // only with NaN data
+        g.ierr = g.l + 1;
+        goto finish;
+      }
+      g.m = m;
+    }
+    if (g.m != g.l) {
+      for (g.itr = 0; g.itr < max_sweep; g.itr++) {
+        {  // explicit shift, tql2_tiled.hpp:64-80
+          const int l = g.l;
+          const T dl_old = v.D(l);
+          const T el = v.E(l);
+          const T p = (v.D(l + 1) - dl_old) / (el + el);
+          const T r = hypot1(p);
+          const T psr = p + copysign_t(r, p);
+          const T dl = el / psr;
+          g.dl1 = el * psr;
+          v.D(l) = dl;
+          v.D(l + 1) = g.dl1;
+          const T delta = dl_old - dl;
+          for (int j = l + 2; j < n; j++) v.D(j) -= delta;
+          g.shift += delta;
+        }
+        g.c = T(1); g.c2 = T(1); g.c3 = T(1);
+        g.s = T(0); g.s2 = T(0);
+        g.p = v.D(g.m);
+        g.el1 = v.E(g.l + 1);
+        g.ei = T(0);
+        for (g.i = g.m - 1; g.i >= g.l; g.i--) {
+          if (nrec + (g.seg_pos < 0 ? 2 : 1) > cap) {
+            ql_close_seg(g, buf);
+            g.pc = PC_ROT;
+            return nrec;
+          }
+        resume_rot:
+          if (g.seg_pos < 0) {
+            g.seg_pos = nrec++;
+            g.seg_cnt = 0;
+            g.seg_i0 = g.i;
+          }
+          {  // QL step, tql2_tiled.hpp:94-115
+            const int i = g.i;
+            g.c3 = g.c2;
+            g.c2 = g.c;
+            g.s2 = g.s;
+            const T ei = v.E(i);
+            const T di = v.D(i);
+            const T gg = g.c * ei;
+            const T h = g.c * g.p;
+            T c, s, r;
+            givens(g.p, ei, c, s, r);
+            const T ei1 = g.s * r;
+            g.p = c * di - s * gg;
+            const T di1 = h + s * (c * gg + s * di);
+            v.E(i + 1) = ei1;
+            v.D(i + 1) = di1;
+            g.c = c;
+            g.s = s;
+            g.ei = ei;
+            Rec<T> rec;
+            rec.c = c;
+            rec.s = s;
+            buf[nrec++] = rec;
+            g.seg_cnt++;
+          }
+        }
+        ql_close_seg(g, buf);
+        {  // tql2_tiled.hpp:126-135
+          const T r = (-g.s * g.s2 * g.c3 * g.el1 * g.ei) / g.dl1;
+          v.E(g.l) = g.s * r;
+          v.D(g.l) = g.c * r;
+        }
+        if (fabs_t(v.E(g.l)) <= g.tst1) break;
+      }
+      if (g.itr >= max_sweep) {
+        g.ierr = g.l + 1;
+        goto finish;
+      }
+    }
+    v.D(g.l) += g.shift;
+  }
+finish:
+  ql_close_seg(g, buf);
+  g.pc = PC_DONE;
+  return nrec;
+}
+
+template <class T>
+__device__ int ql_imtql2(QLGen<T> &g, const DEView<T> v, const int n, Rec<T> *buf, const int cap,
+                         const int max_sweep)
+{
+  const T tol = Num<T>::eps() * Num<T>::tolmul();
+  int nrec = 0;
+  if (g.pc == PC_DONE) return 0;
+  if (g.pc == PC_ROT) goto resume_rot;
+  g.ierr = 0;
+  g.seg_pos = -1;
+  if (n <= 1) goto finish;
+  for (g.l = 0; g.l < n; g.l++) {
+    for (g.itr = 0; g.itr <= max_sweep; g.itr++) {
+      {  // deflation test, imtql2_tiled.hpp:56-61
+        int m = n - 1;
+        for (int mm = g.l; mm < n - 1; mm++) {
+          const T t1 = (fabs_t(v.D(mm)) + fabs_t(v.D(mm + 1))) * tol;
+          const T t2 = fabs_t(v.E(mm));
+          if (!(t2 > t1)) {
+            m = mm;
+            break;
+          }
+        }
+        g.m = m;
+      }
+      if (g.m == g.l) break;
+      {  // Wilkinson-type shift, imtql2_tiled.hpp:67-75
+        const T dl = v.D(g.l), dl1 = v.D(g.l + 1), el = v.E(g.l);
+        const T f = (dl1 - dl) / (el + el);
+        const T gg = hypot1(f);
+        g.di1 = v.D(g.m);
+        g.r = (g.di1 - dl) + el / (f + copysign_t(gg, f));
+      }
+      g.s = T(1);
+      g.c = T(1);
+      g.delta = T(0);
+      for (g.i = g.m - 1; g.i >= g.l; g.i--) {
+        if (nrec + (g.seg_pos < 0 ? 2 : 1) > cap) {
+          ql_close_seg(g, buf);
+          g.pc = PC_ROT;
+          return nrec;
+        }
+      resume_rot:
+        {  // imtql2_tiled.hpp:86-115
+          const int i = g.i;
+          const T ei = v.E(i);
+          const T f = g.s * ei;
+          T c, s, r;
+          givens(g.r, f, c, s, r);
+          if (r == T(0)) {
+            g.r = T(0);
+            break;
+          }
+          if (g.seg_pos < 0) {
+            g.seg_pos = nrec++;
+            g.seg_cnt = 0;
+            g.seg_i0 = i;
+          }
+          const T b = g.c * ei;
+          const T dix = g.di1 - g.delta;
+          g.di1 = v.D(i);
+          const T q = (g.di1 - dix) * s + T(2) * c * b;
+          const T dx1 = fma(s, q, dix);
+          g.delta = dx1 - dix;
+          v.E(i + 1) = r;
+          v.D(i + 1) = dx1;
+          g.r = c * q - b;
+          g.c = c;
+          g.s = s;
+          Rec<T> rec;
+          rec.c = c;
+          rec.s = s;
+          buf[nrec++] = rec;
+          g.seg_cnt++;
+        }
+      }
+      ql_close_seg(g, buf);
+      {
+        const int j = (g.i + 1 > g.l) ? g.i + 1 : g.l;
+        v.D(j) -= g.delta;
+        v.E(j) = g.r;
+        v.E(g.m) = T(0);
+      }
+    }
+    if (g.itr > max_sweep) {
+      g.ierr = g.l + 1;
+      goto finish;
+    }
+  }
+finish:
+  ql_close_seg(g, buf);
+  g.pc = PC_DONE;
+  return nrec;
+}
+
+template <class T>
+__device__ __forceinline__ int ql_run(int method, QLGen<T> &g, const DEView<T> v, const int n,
+                                      Rec<T> *buf, const int cap, const int max_sweep)
+{
+  return method == QL_IMTQL2 ? ql_imtql2(g, v, n, buf, cap, max_sweep)
+                             : ql_tql2(g, v, n, buf, cap, max_sweep);
+}
+
+}  // namespace eigb

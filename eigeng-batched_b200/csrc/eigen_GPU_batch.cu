@@ -1,0 +1,383 @@
+// Host launcher and C ABI of the B200 batched symmetric eigensolver.
+//
+// Drop-in for the reference's eigen_GPU_batch_DP / eigen_GPU_batch_FP
+// (eigen_GPU_batch.h:26-30, eigen_GPU_batch.cu:327-367) with the same
+// workspace-query convention, plus an extended entry point with options and
+// per-matrix status, and the accuracy gate eigen_GPU_check_{DP,FP}.
+//
+// Per call, for each chunk of matrices (all on the caller's stream, no host
+// synchronisation, no allocation):
+//   phase 1  tridiagonalize, form Q^T in place of A, write d/e to workspace
+//   phase 2  QL on (d, e), one matrix per thread, rotation records out
+//   phase 3  apply the records to Q, sort, write eigenvectors and values
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "eigb_kernels.cuh"
+#include "../../include/eigen_GPU_batch.h"
+
+namespace eigb {
+namespace {
+
+constexpr int kMaxDev = 64;
+constexpr size_t kWsBudget = (size_t)4 << 30;  // workspace target per call
+constexpr long kMinChunk = 512;
+
+struct DevProps {
+  int sms = 0;
+  int smem_optin = 0;
+  int l2 = 0;
+  bool ok = false;
+};
+DevProps g_props[kMaxDev];
+std::mutex g_mu;
+
+// Device properties, read once per device (the reference queries
+// cudaGetDeviceProperties on every call, eigen_GPU_batch.hpp:33-43).
+cudaError_t dev_props(DevProps &out)
+{
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_mu);
+  DevProps &p = g_props[dev];
+  if (!p.ok) {
+    if ((err = cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
+    if ((err = cudaDeviceGetAttribute(&p.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
+      return err;
+    if ((err = cudaDeviceGetAttribute(&p.l2, cudaDevAttrL2CacheSize, dev)) != cudaSuccess) return err;
+    p.ok = true;
+  }
+  out = p;
+  return cudaSuccess;
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// phase timing events set by eigen_GPU_batch_trace
+cudaEvent_t *g_trace = nullptr;
+int g_ntrace = 0;
+
+inline void trace(long chunk, int slot, cudaStream_t stream)
+{
+  cudaEvent_t *ev;
+  int nev;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ev = g_trace;
+    nev = g_ntrace;
+  }
+  const long i = 4 * chunk + slot;
+  if (ev && 4 * chunk + 3 < nev) cudaEventRecord(ev[i], stream);
+}
+
+template <class T> size_t k1c_smem_bytes(int n) { return sizeof(T) * (64 + 2 * (size_t)n + 1 + (size_t)n * (n | 1)); }
+template <class T> size_t k2_smem_per_thread(int n) { return sizeof(T) * 2 * (size_t)n; }
+
+// Layout of the workspace for one chunk of Lc matrices.
+template <class T> struct Plan {
+  int n = 0, nm = 0;
+  long L = 0, Lc = 0;
+  int rcap = 0;
+  bool sm = false;  // Z / S staged in shared memory (n > 32)
+  size_t off_d = 0, off_e = 0, off_meta = 0, off_rec = 0, off_z = 0, bytes = 0;
+};
+
+template <class T> int rec_capacity(int n)
+{
+  // tql2 / imtql2 take ~1.1 n^2 rotations plus one header per sweep on
+  // random matrices; twice that leaves ample margin, and a matrix that still
+  // overflows is finished by phase 3 itself.
+  return 2 * n * n + 4 * n + 32;
+}
+
+template <class T>
+cudaError_t make_plan(long L, int nm, int n, const DevProps &dp, Plan<T> &pl, const eigen_GPU_batch_opts *opts)
+{
+  const int rcap_opt = opts ? opts->rec_cap : 0;
+  pl.n = n;
+  pl.nm = nm;
+  pl.L = L;
+  pl.rcap = rcap_opt > 0 ? std::max(rcap_opt, 4) : rec_capacity<T>(n);
+  const size_t optin = (size_t)dp.smem_optin;
+  pl.sm = n > 32 && k1c_smem_bytes<T>(n) <= optin && k3c_smem_bytes<T>(n, true) <= optin;
+  if (n > 32 && !pl.sm && k3c_smem_bytes<T>(n, false) > optin) return cudaErrorInvalidValue;
+  const size_t per = sizeof(T) * 2 * (size_t)n + sizeof(Meta) + sizeof(Rec<T>) * (size_t)pl.rcap +
+                     ((n > 32 && !pl.sm) ? sizeof(T) * (size_t)n * n : 0);
+  long lc = (long)(kWsBudget / per);
+  lc = std::max(lc, kMinChunk);
+  if (opts && opts->chunk > 0) lc = opts->chunk;
+  pl.Lc = std::min(L, lc);
+  size_t off = 0;
+  pl.off_d = off;
+  off = align256(off + sizeof(T) * (size_t)n * pl.Lc);
+  pl.off_e = off;
+  off = align256(off + sizeof(T) * (size_t)n * pl.Lc);
+  pl.off_meta = off;
+  off = align256(off + sizeof(Meta) * (size_t)pl.Lc);
+  pl.off_rec = off;
+  off = align256(off + sizeof(Rec<T>) * (size_t)pl.rcap * pl.Lc);
+  pl.off_z = off;
+  if (n > 32 && !pl.sm) off = align256(off + sizeof(T) * (size_t)n * n * pl.Lc);
+  pl.bytes = off;
+  return cudaSuccess;
+}
+
+bool bad_args(long L, int nm, int n, int m) { return L < 1 || nm < n || n < 1 || m < 1 || m > n || n > 1024; }
+
+template <class T>
+cudaError_t buffer_size(long L, int nm, int n, int m, size_t *lwork, const eigen_GPU_batch_opts *opts = nullptr)
+{
+  if (lwork) *lwork = 0;
+  if (bad_args(L, nm, n, m)) return cudaErrorInvalidValue;
+  if (n == 1) return cudaSuccess;
+  if (opts && opts->method == EIGEN_GPU_BATCH_JACOBI) return cudaSuccess;
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  Plan<T> pl;
+  if ((err = make_plan<T>(L, nm, n, dp, pl, opts)) != cudaSuccess) return err;
+  if (lwork) *lwork = pl.bytes;
+  return cudaSuccess;
+}
+
+template <class K> cudaError_t set_smem(K kern, size_t bytes)
+{
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <class T>
+cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork, int *info,
+                const eigen_GPU_batch_opts *opts, cudaStream_t stream)
+{
+  if (bad_args(L, nm, n, m) || a == nullptr || w == nullptr) return cudaErrorInvalidValue;
+  int method = EIGEN_GPU_BATCH_TQL2, sort = 1, max_sweep = 100;
+  if (opts) {
+    method = opts->method;
+    sort = opts->sort ? 1 : 0;
+    if (opts->max_sweep > 0) max_sweep = opts->max_sweep;
+  }
+  if (method < EIGEN_GPU_BATCH_TQL2 || method > EIGEN_GPU_BATCH_JACOBI) return cudaErrorInvalidValue;
+  if (method == EIGEN_GPU_BATCH_JACOBI && n > 32) return cudaErrorInvalidValue;
+  cudaError_t err;
+  if (n == 1) {
+    const int blocks = (int)std::min<long>((L + 255) / 256, 4096);
+    k_n1<T><<<blocks, 256, 0, stream>>>(L, nm, a, w);
+    if (info) cudaMemsetAsync(info, 0, sizeof(int) * (size_t)L, stream);
+    return cudaGetLastError();
+  }
+  DevProps dp;
+  if ((err = dev_props(dp)) != cudaSuccess) return err;
+
+  KP<T> p{};
+  p.n = n;
+  p.nm = nm;
+  p.method = (method == EIGEN_GPU_BATCH_IMTQL2) ? QL_IMTQL2 : QL_TQL2;
+  p.max_sweep = max_sweep;
+  p.sort = sort;
+
+  if (method == EIGEN_GPU_BATCH_JACOBI) {
+    const size_t smem = sizeof(JacSlot<T>) * K1W_NW;
+    if ((err = set_smem(k_jacobi_warp<T>, smem)) != cudaSuccess) return err;
+    p.a = a;
+    p.w = w;
+    p.info = info;
+    p.Lc = L;
+    const long blocks = (L + K1W_NW - 1) / K1W_NW;
+    k_jacobi_warp<T><<<(unsigned)blocks, 32 * K1W_NW, smem, stream>>>(p);
+    return cudaGetLastError();
+  }
+
+  Plan<T> pl;
+  if ((err = make_plan<T>(L, nm, n, dp, pl, opts)) != cudaSuccess) return err;
+  if (wk == nullptr || (lwork != 0 && lwork < pl.bytes)) return cudaErrorInvalidValue;
+  char *base = static_cast<char *>(wk);
+  p.d = reinterpret_cast<T *>(base + pl.off_d);
+  p.e = reinterpret_cast<T *>(base + pl.off_e);
+  p.meta = reinterpret_cast<Meta *>(base + pl.off_meta);
+  p.rec = reinterpret_cast<Rec<T> *>(base + pl.off_rec);
+  p.zs = reinterpret_cast<T *>(base + pl.off_z);
+  p.rcap = pl.rcap;
+
+  // launch geometry
+  const size_t k1w_smem = sizeof(T) * k1w_slot<T>() * K1W_NW;
+  const size_t k3w_smem = sizeof(K3WSlot<T>) * K3W_NW;
+  const int cta = std::min(1024, ((n + 31) / 32) * 32);
+  const size_t k1c_smem = pl.sm ? k1c_smem_bytes<T>(n) : sizeof(T) * (64 + 2 * (size_t)n + 1);
+  const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.sm);
+  int k2_tpb = 32;
+  {
+    const size_t per = k2_smem_per_thread<T>(n);
+    const size_t budget = std::min<size_t>((size_t)dp.smem_optin, 96 * 1024);
+    k2_tpb = (int)std::max<size_t>(1, std::min<size_t>(32, budget / per));
+    if ((size_t)k2_tpb * per > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
+  }
+  const size_t k2_smem = k2_smem_per_thread<T>(n) * k2_tpb;
+  if (n <= 32) {
+    if ((err = set_smem(k1_warp<T>, k1w_smem)) != cudaSuccess) return err;
+    if ((err = set_smem(k3_warp<T>, k3w_smem)) != cudaSuccess) return err;
+  } else if (pl.sm) {
+    if ((err = set_smem(k1_cta<T, true>, k1c_smem)) != cudaSuccess) return err;
+    if ((err = set_smem(k3_cta<T, true>, k3c_smem)) != cudaSuccess) return err;
+  } else {
+    if ((err = set_smem(k1_cta<T, false>, k1c_smem)) != cudaSuccess) return err;
+    if ((err = set_smem(k3_cta<T, false>, k3c_smem)) != cudaSuccess) return err;
+  }
+  if ((err = set_smem(k2_ql<T>, k2_smem)) != cudaSuccess) return err;
+
+  for (long c0 = 0; c0 < L; c0 += pl.Lc) {
+    const long lc = std::min(pl.Lc, L - c0);
+    const long chunk = c0 / pl.Lc;
+    trace(chunk, 0, stream);
+    p.a = a + (size_t)c0 * nm * n;
+    p.w = w + (size_t)c0 * n;
+    p.info = info ? info + c0 : nullptr;
+    p.Lc = lc;
+    if (n <= 32) {
+      const unsigned nb = (unsigned)((lc + K1W_NW - 1) / K1W_NW);
+      k1_warp<T><<<nb, 32 * K1W_NW, k1w_smem, stream>>>(p);
+    } else if (pl.sm) {
+      k1_cta<T, true><<<(unsigned)lc, cta, k1c_smem, stream>>>(p);
+    } else {
+      k1_cta<T, false><<<(unsigned)lc, cta, k1c_smem, stream>>>(p);
+    }
+    trace(chunk, 1, stream);
+    k2_ql<T><<<(unsigned)((lc + k2_tpb - 1) / k2_tpb), k2_tpb, k2_smem, stream>>>(p);
+    trace(chunk, 2, stream);
+    if (n <= 32) {
+      const unsigned nb = (unsigned)((lc + K3W_NW - 1) / K3W_NW);
+      k3_warp<T><<<nb, 32 * K3W_NW, k3w_smem, stream>>>(p);
+    } else if (pl.sm) {
+      k3_cta<T, true><<<(unsigned)lc, cta, k3c_smem, stream>>>(p);
+    } else {
+      k3_cta<T, false><<<(unsigned)lc, cta, k3c_smem, stream>>>(p);
+    }
+    trace(chunk, 3, stream);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
+template <class T>
+void dropin(const int L, const int nm, const int n, const int m, T *a, T *w, T *wk, cudaStream_t stream)
+{
+  if (wk == nullptr) {
+    // size query: the byte count is written through w, a host pointer in
+    // this mode (eigen_GPU_batch.cu:332-339); 0 for n == 1
+    size_t lwork = 0;
+    if (n > 1) buffer_size<T>(L, nm, n, m, &lwork);
+    if (w) *reinterpret_cast<size_t *>(w) = lwork;
+    return;
+  }
+  run<T>(L, nm, n, m, a, w, wk, 0, nullptr, nullptr, stream);
+}
+
+template <class T>
+cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, const T *z, double *err1, double *err2,
+                      int *flags, float *ref_flags, cudaStream_t stream)
+{
+  if (bad_args(L, nm, n, m) || !a0 || !w || !z) return cudaErrorInvalidValue;
+  const long blocks = std::min<long>((L + 3) / 4, 65535);
+  k_check<T><<<(unsigned)blocks, 128, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+  return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace eigb
+
+extern "C" {
+
+void eigen_GPU_batch_DP(const int L, const int nm, const int n, const int m, double *a, double *w, double *wk,
+                        const cudaStream_t stream)
+{
+  eigb::dropin<double>(L, nm, n, m, a, w, wk, stream);
+}
+
+void eigen_GPU_batch_FP(const int L, const int nm, const int n, const int m, float *a, float *w, float *wk,
+                        const cudaStream_t stream)
+{
+  eigb::dropin<float>(L, nm, n, m, a, w, wk, stream);
+}
+
+cudaError_t eigen_GPU_batch_BufferSize_DP(const int L, const int nm, const int n, const int m, size_t *lwork)
+{
+  return eigb::buffer_size<double>(L, nm, n, m, lwork);
+}
+
+cudaError_t eigen_GPU_batch_BufferSize_FP(const int L, const int nm, const int n, const int m, size_t *lwork)
+{
+  return eigb::buffer_size<float>(L, nm, n, m, lwork);
+}
+
+cudaError_t eigen_GPU_batch_ex_BufferSize_DP(const int L, const int nm, const int n, const int m,
+                                             const eigen_GPU_batch_opts *opts, size_t *lwork)
+{
+  return eigb::buffer_size<double>(L, nm, n, m, lwork, opts);
+}
+
+cudaError_t eigen_GPU_batch_ex_BufferSize_FP(const int L, const int nm, const int n, const int m,
+                                             const eigen_GPU_batch_opts *opts, size_t *lwork)
+{
+  return eigb::buffer_size<float>(L, nm, n, m, lwork, opts);
+}
+
+cudaError_t eigen_GPU_batch_ex_DP(const int L, const int nm, const int n, const int m, double *a, double *w, void *wk,
+                                  const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                  const cudaStream_t stream)
+{
+  return eigb::run<double>(L, nm, n, m, a, w, wk, lwork, info, opts, stream);
+}
+
+cudaError_t eigen_GPU_batch_ex_FP(const int L, const int nm, const int n, const int m, float *a, float *w, void *wk,
+                                  const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                  const cudaStream_t stream)
+{
+  return eigb::run<float>(L, nm, n, m, a, w, wk, lwork, info, opts, stream);
+}
+
+void eigen_GPU_check_DP(const int L, const int nm, const int n, const int m, double *a, double *w, double *z,
+                        const cudaStream_t stream)
+{
+  if (eigb::check_run<double>(L, nm, n, m, a, w, z, nullptr, nullptr, nullptr, reinterpret_cast<float *>(a),
+                              stream) == cudaSuccess)
+    eigb::k_check_print<double><<<1, 1, 0, stream>>>(L, nm, n, a);
+}
+
+void eigen_GPU_check_FP(const int L, const int nm, const int n, const int m, float *a, float *w, float *z,
+                        const cudaStream_t stream)
+{
+  if (eigb::check_run<float>(L, nm, n, m, a, w, z, nullptr, nullptr, nullptr, reinterpret_cast<float *>(a),
+                             stream) == cudaSuccess)
+    eigb::k_check_print<float><<<1, 1, 0, stream>>>(L, nm, n, a);
+}
+
+cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents)
+{
+  if (events != nullptr && nevents < 4) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lk(eigb::g_mu);
+  eigb::g_trace = events;
+  eigb::g_ntrace = events ? nevents : 0;
+  return cudaSuccess;
+}
+
+cudaError_t eigen_GPU_check_ex_DP(const int L, const int nm, const int n, const int m, const double *a,
+                                  const double *w, const double *z, double *err1, double *err2, int *flags,
+                                  const cudaStream_t stream)
+{
+  return eigb::check_run<double>(L, nm, n, m, a, w, z, err1, err2, flags, nullptr, stream);
+}
+
+cudaError_t eigen_GPU_check_ex_FP(const int L, const int nm, const int n, const int m, const float *a,
+                                  const float *w, const float *z, double *err1, double *err2, int *flags,
+                                  const cudaStream_t stream)
+{
+  return eigb::check_run<float>(L, nm, n, m, a, w, z, err1, err2, flags, nullptr, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,209 @@
+"""Python host mirror of the B200 batched symmetric eigensolver.
+
+Thin ctypes binding of ``lib/libeigenGbatch.so`` (the C ABI declared in
+``include/eigen_GPU_batch.h`` and ``include/eigen_GPU_check.h``).  The names
+follow the reference's C/C++ interface (EigenG-Batched
+``eigen_GPU_batch.h:26-30``, ``eigen_GPU_batch.hpp:104-157``,
+``eigen_GPU_check.cu:183-197``); tensors are CUDA ``torch`` tensors and the
+stream defaults to torch's current stream.  PyTorch only supplies device
+memory and streams: every computation runs in the library's own kernels, and
+nothing here falls back to another implementation -- a missing library is
+an error.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libeigenGbatch.so")
+
+TQL2, IMTQL2, JACOBI = 0, 1, 2
+
+_lib = None
+
+
+class EigenGError(RuntimeError):
+    pass
+
+
+class Opts(ctypes.Structure):
+    """eigen_GPU_batch_opts of include/eigen_GPU_batch.h."""
+    _fields_ = [("method", ctypes.c_int), ("sort", ctypes.c_int), ("max_sweep", ctypes.c_int),
+                ("rec_cap", ctypes.c_int), ("chunk", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise EigenGError(f"{LIB_PATH} is missing: build it with `make -C eigeng-batched_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, SZ = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t
+        for s in ("DP", "FP"):
+            f = getattr(L, "eigen_GPU_batch_" + s)
+            f.argtypes = [I, I, I, I, P, P, P, P]
+            f.restype = None
+            f = getattr(L, "eigen_GPU_batch_BufferSize_" + s)
+            f.argtypes = [I, I, I, I, ctypes.POINTER(SZ)]
+            f.restype = I
+            f = getattr(L, "eigen_GPU_batch_ex_BufferSize_" + s)
+            f.argtypes = [I, I, I, I, ctypes.POINTER(Opts), ctypes.POINTER(SZ)]
+            f.restype = I
+            f = getattr(L, "eigen_GPU_batch_ex_" + s)
+            f.argtypes = [I, I, I, I, P, P, P, SZ, P, ctypes.POINTER(Opts), P]
+            f.restype = I
+            f = getattr(L, "eigen_GPU_check_" + s)
+            f.argtypes = [I, I, I, I, P, P, P, P]
+            f.restype = None
+            f = getattr(L, "eigen_GPU_check_ex_" + s)
+            f.argtypes = [I, I, I, I, P, P, P, P, P, P, P]
+            f.restype = I
+        L.eigen_GPU_batch_trace.argtypes = [P, I]
+        L.eigen_GPU_batch_trace.restype = I
+        _lib = L
+    return _lib
+
+
+class PhaseTrace:
+    """Context manager recording the per-phase events of eigen_GPU_batch_trace
+    for up to `chunks` chunks; `.ms()` returns [(p1, p2, p3) per chunk] in ms."""
+
+    def __init__(self, chunks=1):
+        self.events = [torch.cuda.Event(enable_timing=True) for _ in range(4 * chunks)]
+        self._arr = (ctypes.c_void_p * len(self.events))(*[ctypes.c_void_p(e.cuda_event) for e in self.events])
+
+    def __enter__(self):
+        st = lib().eigen_GPU_batch_trace(self._arr, len(self.events))
+        if st != 0:
+            raise EigenGError(f"eigen_GPU_batch_trace failed with cudaError {st}")
+        return self
+
+    def __exit__(self, *exc):
+        lib().eigen_GPU_batch_trace(None, 0)
+        return False
+
+    def ms(self):
+        torch.cuda.synchronize()
+        out = []
+        for c in range(len(self.events) // 4):
+            e = self.events[4 * c:4 * c + 4]
+            try:
+                out.append(tuple(e[i].elapsed_time(e[i + 1]) for i in range(3)))
+            except RuntimeError:
+                break
+        return out
+
+
+def exported_symbols():
+    return [
+        "eigen_GPU_batch_DP", "eigen_GPU_batch_FP",
+        "eigen_GPU_batch_BufferSize_DP", "eigen_GPU_batch_BufferSize_FP",
+        "eigen_GPU_batch_ex_DP", "eigen_GPU_batch_ex_FP",
+        "eigen_GPU_batch_ex_BufferSize_DP", "eigen_GPU_batch_ex_BufferSize_FP",
+        "eigen_GPU_check_DP", "eigen_GPU_check_FP",
+        "eigen_GPU_check_ex_DP", "eigen_GPU_check_ex_FP",
+        "eigen_GPU_batch_trace",
+    ]
+
+
+def _sfx(dtype):
+    if dtype == torch.float64:
+        return "DP"
+    if dtype == torch.float32:
+        return "FP"
+    raise TypeError(f"unsupported dtype {dtype}")
+
+
+def _ptr(t):
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def _dims(a, n, nm):
+    nm = n if nm is None else nm
+    if not a.is_cuda or not a.is_contiguous():
+        raise EigenGError("a must be a contiguous CUDA tensor")
+    if a.numel() % (nm * n):
+        raise EigenGError("a.numel() is not a multiple of nm*n")
+    return a.numel() // (nm * n), nm
+
+
+def buffer_size(L, nm, n, m=None, dtype=torch.float64, rec_cap=0, method=TQL2, chunk=0):
+    """eigen_GPU_batch_BufferSize<T>: workspace bytes (for the given options)."""
+    m = n if m is None else m
+    out = ctypes.c_size_t(0)
+    if rec_cap or chunk or method != TQL2:
+        o = Opts(method, 1, 100, rec_cap, chunk)
+        st = getattr(lib(), "eigen_GPU_batch_ex_BufferSize_" + _sfx(dtype))(L, nm, n, m, ctypes.byref(o),
+                                                                           ctypes.byref(out))
+    else:
+        st = getattr(lib(), "eigen_GPU_batch_BufferSize_" + _sfx(dtype))(L, nm, n, m, ctypes.byref(out))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_BufferSize failed with cudaError {st}")
+    return out.value
+
+
+def query_lwork(L, nm, n, m=None, dtype=torch.float64):
+    """The C size-query mode: wk == NULL writes the size through w (host)."""
+    m = n if m is None else m
+    out = ctypes.c_size_t(0xDEADBEEF)
+    getattr(lib(), "eigen_GPU_batch_" + _sfx(dtype))(L, nm, n, m, None, ctypes.byref(out), None, None)
+    return out.value
+
+
+def workspace(L, nm, n, dtype, device=None, rec_cap=0, chunk=0):
+    nb = buffer_size(L, nm, n, n, dtype, rec_cap, TQL2, chunk)
+    return torch.empty(max(nb, 16), dtype=torch.uint8, device=device or "cuda")
+
+
+def eigen_GPU_batch(a, w, wk, n, nm=None, m=None, stream=None):
+    """Drop-in call: eigenvectors overwrite ``a``, eigenvalues go to ``w``."""
+    L, nm = _dims(a, n, nm)
+    m = n if m is None else m
+    getattr(lib(), "eigen_GPU_batch_" + _sfx(a.dtype))(L, nm, n, m, _ptr(a), _ptr(w), _ptr(wk), _stream(stream))
+
+
+def eigen_GPU_batch_ex(a, w, wk, n, nm=None, m=None, info=None, method=TQL2, sort=True, max_sweep=100,
+                       stream=None, rec_cap=0, chunk=0):
+    """Extended call; returns the cudaError_t status (0 on success)."""
+    L, nm = _dims(a, n, nm)
+    m = n if m is None else m
+    o = Opts(method, 1 if sort else 0, max_sweep, rec_cap, chunk)
+    lw = 0 if wk is None else wk.numel() * wk.element_size()
+    return getattr(lib(), "eigen_GPU_batch_ex_" + _sfx(a.dtype))(
+        L, nm, n, m, _ptr(a), _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), _stream(stream))
+
+
+def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=None, rec_cap=0, chunk=0):
+    """Convenience wrapper: solves in place, returns (w, info)."""
+    L, nm = _dims(a, n, nm)
+    w = torch.empty((L, n), dtype=a.dtype, device=a.device)
+    info = torch.zeros(L, dtype=torch.int32, device=a.device)
+    if wk is None and method != JACOBI:
+        wk = workspace(L, nm, n, a.dtype, a.device, rec_cap, chunk)
+    st = eigen_GPU_batch_ex(a, w, wk, n, nm, n, info, method, sort, max_sweep, stream, rec_cap, chunk)
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
+    return w, info
+
+
+def check(a0, w, z, n, nm=None, stream=None):
+    """eigen_GPU_check_ex: per-matrix (err1, err2, flags) on the device."""
+    L, nm = _dims(a0, n, nm)
+    e1 = torch.empty(L, dtype=torch.float64, device=a0.device)
+    e2 = torch.empty(L, dtype=torch.float64, device=a0.device)
+    fl = torch.empty(L, dtype=torch.int32, device=a0.device)
+    st = getattr(lib(), "eigen_GPU_check_ex_" + _sfx(a0.dtype))(
+        L, nm, n, n, _ptr(a0), _ptr(w), _ptr(z), _ptr(e1), _ptr(e2), _ptr(fl), _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_check_ex failed with cudaError {st}")
+    return e1, e2, fl

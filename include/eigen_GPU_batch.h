@@ -1,0 +1,113 @@
+/*
+ * C ABI of the B200 batched symmetric eigensolver (libeigenGbatch).
+ *
+ * Computes all eigenvalues and eigenvectors of L real symmetric n x n
+ * matrices.  Matrix k is column-major at a + k*nm*n (only its upper
+ * triangle is read); on return a holds the eigenvectors column by column
+ * and w + k*n the eigenvalues (ascending by default).  All pointers except
+ * the size-query target are device pointers owned by the caller; every call
+ * is asynchronous on `stream` and allocates nothing.
+ *
+ * Drop-in replacement for RIKEN-RCCS/EigenG-Batched's eigen_GPU_batch.h.
+ */
+#ifndef EIGEN_GPU_BATCH_B200_H
+#define EIGEN_GPU_BATCH_B200_H
+
+#include <stddef.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/*
+ * Replaces eigen_GPU_batch_DP / eigen_GPU_batch_FP of the reference
+ * (eigen_GPU_batch.h:26-30, defined at eigen_GPU_batch.cu:327-359).
+ * Same arguments and behaviour: L matrices of order n (1 <= n <= nm,
+ * 1 <= m <= n; n <= 1024 here), eigenvectors in a, eigenvalues in w,
+ * workspace wk.
+ * Workspace query: when wk == NULL the required workspace size in bytes is
+ * written as a size_t through w, which must then be a HOST pointer
+ * (0 for n == 1), exactly as eigen_GPU_batch.cu:332-339.  The size differs
+ * from the reference's formula (eigen_GPU_batch.hpp:104-118), so callers
+ * must use this query or eigen_GPU_batch_BufferSize_*.
+ * Invalid arguments make the call a no-op (the reference discards the
+ * status too); use eigen_GPU_batch_ex_* to receive it.
+ */
+void eigen_GPU_batch_DP(const int L, const int nm, const int n, const int m, double *a, double *w, double *wk,
+                        const cudaStream_t stream);
+void eigen_GPU_batch_FP(const int L, const int nm, const int n, const int m, float *a, float *w, float *wk,
+                        const cudaStream_t stream);
+
+/*
+ * Workspace size in bytes for a call with these sizes on the current
+ * device.  Counterpart of the header-only template
+ * eigen_GPU_batch_BufferSize<T> (eigen_GPU_batch.hpp:104-118), exported so
+ * that C callers need not go through the size-query mode above.
+ */
+cudaError_t eigen_GPU_batch_BufferSize_DP(const int L, const int nm, const int n, const int m, size_t *lwork);
+cudaError_t eigen_GPU_batch_BufferSize_FP(const int L, const int nm, const int n, const int m, size_t *lwork);
+
+/* Eigenvalue method of the extended entry point.  TQL2 is the reference's
+ * default (USE_IMTQL 0, eigen_GPU_batch.cu:3); IMTQL2 its USE_IMTQL 1
+ * variant; JACOBI the cyclic Jacobi path for n <= 32 (jac_tiled.hpp). */
+#define EIGEN_GPU_BATCH_TQL2 0
+#define EIGEN_GPU_BATCH_IMTQL2 1
+#define EIGEN_GPU_BATCH_JACOBI 2
+
+typedef struct eigen_GPU_batch_opts {
+  int method;    /* EIGEN_GPU_BATCH_TQL2 (default), _IMTQL2 or _JACOBI */
+  int sort;      /* 1: ascending eigenvalues (reference DO_SORT 1), 0: as computed */
+  int max_sweep; /* QL sweeps per eigenvalue / Jacobi passes; <= 0 means 100 */
+  int rec_cap;   /* rotation records kept per matrix; <= 0: the default
+                    2n^2+4n+32.  A smaller value shrinks the workspace
+                    (eigen_GPU_batch_ex_BufferSize_*); a matrix whose QL
+                    rotations do not fit is finished by regenerating them
+                    inside the apply phase, with identical results. */
+  int chunk;     /* matrices per internal chunk; <= 0: automatic (workspace
+                    about 4 GiB or 512 matrices).  Bounds the workspace. */
+  int reserved[3];
+} eigen_GPU_batch_opts;
+
+/* Workspace bytes for eigen_GPU_batch_ex_* with these options (NULL:
+ * defaults, equal to eigen_GPU_batch_BufferSize_*). */
+cudaError_t eigen_GPU_batch_ex_BufferSize_DP(const int L, const int nm, const int n, const int m,
+                                             const eigen_GPU_batch_opts *opts, size_t *lwork);
+cudaError_t eigen_GPU_batch_ex_BufferSize_FP(const int L, const int nm, const int n, const int m,
+                                             const eigen_GPU_batch_opts *opts, size_t *lwork);
+
+/*
+ * Extended form of eigen_GPU_batch_DP/FP (no reference counterpart: the
+ * reference returns nothing and has no options).  lwork is the workspace
+ * size in bytes (0: not checked); info, when not NULL, is a device array of
+ * L ints that receives 0, or the 1-based index at which QL exceeded
+ * max_sweep, or n+1 when Jacobi did not converge within max_sweep passes.
+ * opts == NULL selects the reference defaults (tql2, sorted, 100 sweeps).
+ * The JACOBI method needs no workspace (wk may be NULL).
+ * Returns cudaErrorInvalidValue for bad sizes, a too small workspace or an
+ * unknown method, otherwise the launch status.
+ */
+cudaError_t eigen_GPU_batch_ex_DP(const int L, const int nm, const int n, const int m, double *a, double *w, void *wk,
+                                  const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                  const cudaStream_t stream);
+cudaError_t eigen_GPU_batch_ex_FP(const int L, const int nm, const int n, const int m, float *a, float *w, void *wk,
+                                  const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                  const cudaStream_t stream);
+
+/*
+ * Phase timing (counterpart of the reference's compile-time TIMER,
+ * eigen_GPU_batch.cu:157-244, which prints per-phase times from warp 0).
+ * When set, every later solve on the calling process records, for chunk c
+ * of the batch, events[4c] before phase 1 (tridiagonalization + Q),
+ * events[4c+1] after it, events[4c+2] after phase 2 (QL) and events[4c+3]
+ * after phase 3 (rotation apply + sort), on the call's stream, for the
+ * chunks whose four events fit in nevents.  events == NULL turns it off.
+ * The events are created and owned by the caller.
+ */
+cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,73 @@
+"""Generates tests/golden/ref_gpu_golden.npz: outputs of the reference's own
+GPU build (EigenG-Batched eigen_GPU_batch_DP/FP, default tql2 + DO_SORT,
+compiled for sm_100a by oracle/build_ref.sh into oracle/_ref/) on seeded
+inputs.  Run on a machine with a GPU:
+
+    python tests/golden/make_ref_golden.py [out.npz]
+
+The CPU oracle and the CUDA library are checked against these fixtures
+(tests/test_golden.py).  n == 2 is left out: the reference's n <= 32 path
+returns the input matrix unchanged for n == 2 (tred1_tiled.hpp:25-34,
+hhtr2sy_tiled.hpp:27-35).
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as O  # noqa: E402
+
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libeigenGbatch_ref.so")
+
+
+def ref_solve(lib, a0, n):
+    """Calls the reference exactly as its README does: size query, solve."""
+    L = a0.shape[0]
+    dt = a0.dtype
+    fn = lib.eigen_GPU_batch_DP if dt == np.float64 else lib.eigen_GPU_batch_FP
+    fn.restype = None
+    lw = ctypes.c_size_t(0)
+    fn(L, n, n, n, None, ctypes.byref(lw), None, None)
+    a = torch.from_numpy(a0.copy()).cuda()
+    w = torch.zeros((L, n), dtype=a.dtype, device="cuda")
+    wk = torch.zeros(max(lw.value, 16), dtype=torch.uint8, device="cuda")
+    fn(L, n, n, n, ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(w.data_ptr()), ctypes.c_void_p(wk.data_ptr()),
+       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    return w.cpu().numpy(), a.cpu().numpy()
+
+
+def cases():
+    for n in (3, 5, 8, 16, 17, 31, 32, 33, 48, 64, 100, 128):
+        L = 3 if n < 100 else 2
+        fams = {
+            "symu": O.sym_uniform(L, n, seed=500 + n),
+            "letkf": O.letkf_like(L, n, seed=600 + n),
+            "frank": O.ref_matrices(L, n, O.REF_FRANK),
+            "refrand": O.ref_matrices(L, n, O.REF_SYM_RAND),
+        }
+        for fam, a in fams.items():
+            for dt in (np.float64, np.float32):
+                yield f"{np.dtype(dt).name}_{fam}_{n}", n, np.ascontiguousarray(a.astype(dt))
+
+
+def main():
+    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden", "ref_gpu_golden.npz")
+    lib = ctypes.CDLL(REF_LIB)
+    res = {}
+    for key, n, a0 in cases():
+        w, z = ref_solve(lib, a0, n)
+        res[key + "__a"] = a0
+        res[key + "__w"] = w
+        res[key + "__z"] = z
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+    np.savez_compressed(out, **res)
+    print("wrote", out, len(res) // 3, "cases")
+
+
+if __name__ == "__main__":
+    main()
