@@ -24,20 +24,36 @@ template <> struct Num<float> {
 
 // 1/sqrt(x): CUDA's double rsqrt (1 ulp) and the correctly rounded float
 // intrinsic.
-__device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
-__device__ __forceinline__ float rsq(float x) { return __frsqrt_rn(x); }
-__device__ __forceinline__ double sqr_t(double x) { return sqrt(x); }
-__device__ __forceinline__ float sqr_t(float x) { return sqrtf(x); }
-__device__ __forceinline__ double fabs_t(double x) { return fabs(x); }
-__device__ __forceinline__ float fabs_t(float x) { return fabsf(x); }
-__device__ __forceinline__ double fmax_t(double x, double y) { return fmax(x, y); }
-__device__ __forceinline__ float fmax_t(float x, float y) { return fmaxf(x, y); }
-__device__ __forceinline__ double copysign_t(double x, double y) { return copysign(x, y); }
-__device__ __forceinline__ float copysign_t(float x, float y) { return copysignf(x, y); }
+// (host versions exist so that the scalar recurrences can be unit-tested on
+// the CPU; the host rsqrt is 1/sqrt)
+__host__ __device__ __forceinline__ double rsq(double x)
+{
+#ifdef __CUDA_ARCH__
+  return rsqrt(x);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
+__host__ __device__ __forceinline__ float rsq(float x)
+{
+#ifdef __CUDA_ARCH__
+  return __frsqrt_rn(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+__host__ __device__ __forceinline__ double sqr_t(double x) { return sqrt(x); }
+__host__ __device__ __forceinline__ float sqr_t(float x) { return sqrtf(x); }
+__host__ __device__ __forceinline__ double fabs_t(double x) { return fabs(x); }
+__host__ __device__ __forceinline__ float fabs_t(float x) { return fabsf(x); }
+__host__ __device__ __forceinline__ double fmax_t(double x, double y) { return fmax(x, y); }
+__host__ __device__ __forceinline__ float fmax_t(float x, float y) { return fmaxf(x, y); }
+__host__ __device__ __forceinline__ double copysign_t(double x, double y) { return copysign(x, y); }
+__host__ __device__ __forceinline__ float copysign_t(float x, float y) { return copysignf(x, y); }
 
 // Zero guard used wherever the reference divides by a possibly vanishing
 // product (misc_gpu.hpp:474-509 flip0to1).
-template <class T> __device__ __forceinline__ T flip0to1(T x) { return x == T(0) ? T(1) : x; }
+template <class T> __host__ __device__ __forceinline__ T flip0to1(T x) { return x == T(0) ? T(1) : x; }
 
 // Plane rotation for (a, b): r = hypot(a, b), c = a/r, s = b/r, with one
 // reciprocal square root instead of a square root and two divisions.  For
@@ -45,7 +61,7 @@ template <class T> __device__ __forceinline__ T flip0to1(T x) { return x == T(0)
 // reference's pythag (misc_gpu.hpp:533-548) the squares are formed
 // unscaled, so |a|,|b| must stay below sqrt(overflow threshold).
 template <class T>
-__device__ __forceinline__ void givens(T a, T b, T &c, T &s, T &r)
+__host__ __device__ __forceinline__ void givens(T a, T b, T &c, T &s, T &r)
 {
   const T sig = fma(a, a, b * b);
   if (sig > T(0)) {
@@ -63,7 +79,7 @@ __device__ __forceinline__ void givens(T a, T b, T &c, T &s, T &r)
 // sqrt(p*p + 1) without overflow for large |p| (the shift of tql2/imtql2,
 // reference pythag1, misc_gpu.hpp:514-530).
 template <class T>
-__device__ __forceinline__ T hypot1(T p)
+__host__ __device__ __forceinline__ T hypot1(T p)
 {
   const T ap = fabs_t(p);
   const T big = T(sizeof(T) == 8 ? 1e150 : 1e18);
@@ -77,24 +93,32 @@ __device__ __forceinline__ T hypot1(T p)
 // (tql2_tiled.hpp:116-121 chain order).
 template <class T> struct __align__(2 * sizeof(T)) Rec { T c, s; };
 
-__device__ __forceinline__ Rec<double> make_hdr(int i0, int cnt, double)
+union Bits64 { double d; long long i; };
+union Bits32 { float f; int i; };
+__host__ __device__ __forceinline__ Rec<double> make_hdr(int i0, int cnt, double)
 {
+  Bits64 a, b;
+  a.i = i0;
+  b.i = cnt;
   Rec<double> h;
-  h.c = __longlong_as_double((long long)i0);
-  h.s = __longlong_as_double((long long)cnt);
+  h.c = a.d;
+  h.s = b.d;
   return h;
 }
-__device__ __forceinline__ Rec<float> make_hdr(int i0, int cnt, float)
+__host__ __device__ __forceinline__ Rec<float> make_hdr(int i0, int cnt, float)
 {
+  Bits32 a, b;
+  a.i = i0;
+  b.i = cnt;
   Rec<float> h;
-  h.c = __int_as_float(i0);
-  h.s = __int_as_float(cnt);
+  h.c = a.f;
+  h.s = b.f;
   return h;
 }
-__device__ __forceinline__ int hdr_i0(const Rec<double> &h) { return (int)__double_as_longlong(h.c); }
-__device__ __forceinline__ int hdr_cnt(const Rec<double> &h) { return (int)__double_as_longlong(h.s); }
-__device__ __forceinline__ int hdr_i0(const Rec<float> &h) { return __float_as_int(h.c); }
-__device__ __forceinline__ int hdr_cnt(const Rec<float> &h) { return __float_as_int(h.s); }
+__host__ __device__ __forceinline__ int hdr_i0(const Rec<double> &h) { Bits64 a; a.d = h.c; return (int)a.i; }
+__host__ __device__ __forceinline__ int hdr_cnt(const Rec<double> &h) { Bits64 a; a.d = h.s; return (int)a.i; }
+__host__ __device__ __forceinline__ int hdr_i0(const Rec<float> &h) { Bits32 a; a.f = h.c; return a.i; }
+__host__ __device__ __forceinline__ int hdr_cnt(const Rec<float> &h) { Bits32 a; a.f = h.s; return a.i; }
 
 // Per-matrix status block in the workspace.
 struct Meta {

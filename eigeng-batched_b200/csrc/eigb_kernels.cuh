@@ -43,7 +43,7 @@ constexpr int K3W_NW = 4;       // warps per CTA in k3_warp
 constexpr int K3W_CH = 128;     // records staged per warp
 constexpr int K3C_CH = 512;     // records staged per CTA
 
-template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD * 32 + 32 + 32 + 64; }
+template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD * 32 + 32 + 32 + 72; }
 
 // ---------------------------------------------------------------- n == 1
 template <class T>
@@ -89,8 +89,8 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
   const int n = p.n, nm = p.nm, r = threadIdx.x;
   T *A = p.a + (size_t)k * nm * n;
   T *sm = reinterpret_cast<T *>(smem_raw);
-  T *red = sm;          // 64
-  T *beta_s = sm + 64;  // n
+  T *red = sm;          // 72
+  T *beta_s = sm + 72;  // n
   T *pv = beta_s + n;   // n
   T *S;
   int ld;

@@ -35,12 +35,12 @@ template <class T> struct QLGen {
 template <class T> struct DEView {
   T *d, *e;
   int st;
-  __device__ __forceinline__ T &D(int i) const { return d[(size_t)i * st]; }
-  __device__ __forceinline__ T &E(int i) const { return e[(size_t)i * st]; }
+  __host__ __device__ __forceinline__ T &D(int i) const { return d[(size_t)i * st]; }
+  __host__ __device__ __forceinline__ T &E(int i) const { return e[(size_t)i * st]; }
 };
 
 template <class T>
-__device__ __forceinline__ void ql_close_seg(QLGen<T> &g, Rec<T> *buf)
+__host__ __device__ __forceinline__ void ql_close_seg(QLGen<T> &g, Rec<T> *buf)
 {
   if (g.seg_pos >= 0) {
     buf[g.seg_pos] = make_hdr(g.seg_i0, g.seg_cnt, T(0));
@@ -52,7 +52,7 @@ __device__ __forceinline__ void ql_close_seg(QLGen<T> &g, Rec<T> *buf)
 // records written.  g.pc == PC_DONE when the iteration has finished; then
 // g.ierr is 0 or the failing index l (1-based, tql2_tiled.hpp:138).
 template <class T>
-__device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec<T> *buf, const int cap,
+__host__ __device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec<T> *buf, const int cap,
                        const int max_sweep)
 {
   const T tol = Num<T>::eps() * Num<T>::tolmul();
@@ -158,7 +158,7 @@ finish:
 }
 
 template <class T>
-__device__ int ql_imtql2(QLGen<T> &g, const DEView<T> v, const int n, Rec<T> *buf, const int cap,
+__host__ __device__ int ql_imtql2(QLGen<T> &g, const DEView<T> v, const int n, Rec<T> *buf, const int cap,
                          const int max_sweep)
 {
   const T tol = Num<T>::eps() * Num<T>::tolmul();
@@ -253,7 +253,7 @@ finish:
 }
 
 template <class T>
-__device__ __forceinline__ int ql_run(int method, QLGen<T> &g, const DEView<T> v, const int n,
+__host__ __device__ __forceinline__ int ql_run(int method, QLGen<T> &g, const DEView<T> v, const int n,
                                       Rec<T> *buf, const int cap, const int max_sweep)
 {
   return method == QL_IMTQL2 ? ql_imtql2(g, v, n, buf, cap, max_sweep)

@@ -28,9 +28,10 @@ namespace eigb {
 // d_out[0:n] = diagonal, e_out[0:n] = off-diagonal (e_out[k] couples k and
 // k+1, e_out[n-1] = 0, the reference's convention tred1_tiled.hpp:207-212)
 // and S holds M = Q^T with A = Q T Q^T.
-//   beta_s, pv: n-element scratch in shared memory; red: 64 slots.
+//   beta_s, pv: n-element scratch in shared memory; red: 72 slots (64 for
+//   team reductions, red[64] carries the reflector pivot to the team).
 template <class T, int R, class Team>
-__device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T *d_out, T *e_out,
+__host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T *d_out, T *e_out,
                            T *beta_s, T *pv, T *red)
 {
   const int nt = tm.size();
@@ -45,9 +46,12 @@ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T *d_out, 
       const int r = t + j * nt;
       ur[j] = (r < i) ? S[r + (size_t)i * ld] : T(0);
       ss = fma(ur[j], ur[j], ss);
+      // the owner of row i-1 publishes the pivot; the barrier in sum()
+      // orders it after the previous step's updates of that row
+      if (r == i - 1) red[64] = ur[j];
     }
-    const T ulast = S[(i - 1) + (size_t)i * ld];  // read before the barrier in sum()
     const T sig = tm.sum(ss, red);
+    const T ulast = red[64];
     const T anorm = -copysign_t(sqr_t(sig), ulast);
     const T ul = ulast - anorm;
     const T beta = T(1) / flip0to1(ul * anorm);

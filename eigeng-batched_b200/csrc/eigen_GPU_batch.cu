@@ -76,7 +76,7 @@ inline void trace(long chunk, int slot, cudaStream_t stream)
   if (ev && 4 * chunk + 3 < nev) cudaEventRecord(ev[i], stream);
 }
 
-template <class T> size_t k1c_smem_bytes(int n) { return sizeof(T) * (64 + 2 * (size_t)n + 1 + (size_t)n * (n | 1)); }
+template <class T> size_t k1c_smem_bytes(int n) { return sizeof(T) * (72 + 2 * (size_t)n + (size_t)n * (n | 1)); }
 template <class T> size_t k2_smem_per_thread(int n) { return sizeof(T) * 2 * (size_t)n; }
 
 // Layout of the workspace for one chunk of Lc matrices.
@@ -209,7 +209,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const size_t k1w_smem = sizeof(T) * k1w_slot<T>() * K1W_NW;
   const size_t k3w_smem = sizeof(K3WSlot<T>) * K3W_NW;
   const int cta = std::min(1024, ((n + 31) / 32) * 32);
-  const size_t k1c_smem = pl.sm ? k1c_smem_bytes<T>(n) : sizeof(T) * (64 + 2 * (size_t)n + 1);
+  const size_t k1c_smem = pl.sm ? k1c_smem_bytes<T>(n) : sizeof(T) * (72 + 2 * (size_t)n);
   const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.sm);
   int k2_tpb = 32;
   {

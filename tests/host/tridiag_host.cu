@@ -1,0 +1,55 @@
+// Host build of the library's phase-1 team code (csrc/eigb_tridiag.cuh:
+// tridiagonalization + explicit Q^T) for CPU unit tests.  The GPU team (a
+// warp or a CTA) is emulated by one std::thread per GPU thread, with
+// std::barrier standing in for __syncthreads and a shared array for the
+// team reductions, so the source's barrier placement is exercised too.
+#include <barrier>
+#include <thread>
+#include <vector>
+
+#include "../../eigeng-batched_b200/csrc/eigb_tridiag.cuh"
+
+template <class T> struct HostShared {
+  std::barrier<> bar;
+  std::vector<T> slots;  // 2 x nthr, alternating halves
+  explicit HostShared(int nthr) : bar(nthr), slots(2 * (size_t)nthr) {}
+};
+
+template <class T> struct HostTeam {
+  int rank, nthr, flip;
+  HostShared<T> *sh;
+  int size() const { return nthr; }
+  void sync() const { sh->bar.arrive_and_wait(); }
+  T sum(T x, T *)
+  {
+    T *buf = sh->slots.data() + (flip ? nthr : 0);
+    flip ^= 1;
+    buf[rank] = x;
+    sh->bar.arrive_and_wait();
+    T s = T(0);
+    for (int k = 0; k < nthr; k++) s += buf[k];  // same order in every thread
+    return s;
+  }
+};
+
+template <class T> static void run(int n, int nthr, T *S, int ld, T *d, T *e)
+{
+  HostShared<T> sh(nthr);
+  std::vector<T> beta(n + 1), pv(n + 1), red(72);
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthr; t++)
+    th.emplace_back([&, t]() {
+      HostTeam<T> tm{t, nthr, 0, &sh};
+      eigb::tridiag_qt<T, 1>(tm, S, ld, n, d, e, beta.data(), pv.data(), red.data());
+    });
+  for (auto &x : th) x.join();
+}
+
+extern "C" void host_tridiag_d(int n, int nthr, double *S, int ld, double *d, double *e)
+{
+  run<double>(n, nthr, S, ld, d, e);
+}
+extern "C" void host_tridiag_f(int n, int nthr, float *S, int ld, float *d, float *e)
+{
+  run<float>(n, nthr, S, ld, d, e);
+}
