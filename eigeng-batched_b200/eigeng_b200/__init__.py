@@ -74,6 +74,9 @@ class PhaseTrace:
 
     def __init__(self, chunks=1):
         self.events = [torch.cuda.Event(enable_timing=True) for _ in range(4 * chunks)]
+        for e in self.events:  # torch creates the CUDA event on first record
+            e.record()
+        torch.cuda.synchronize()
         self._arr = (ctypes.c_void_p * len(self.events))(*[ctypes.c_void_p(e.cuda_event) for e in self.events])
 
     def __enter__(self):

@@ -135,10 +135,15 @@ def test_jacobi_parity(oracle_mod, n, dtype):
         scale = np.abs(wo).max(axis=1, keepdims=True)
         ws, wos = np.sort(w, axis=1), np.sort(wo, axis=1)
         assert (np.abs(ws - wos) <= 64 * n * eps * scale).all()
-        e1, e2, fl = device_gate(a0, w, z, n)
-        assert (fl == 0).all()
         if sort:
+            # the reference gate scales by max(|w_1|, |w_n|), which assumes
+            # ascending eigenvalues (eigen_GPU_check.cu:65-70)
+            e1, e2, fl = device_gate(a0, w, z, n)
+            assert (fl == 0).all()
             assert_vectors_match(z, ao, wo, n, eps)
+        else:
+            res, orth = O.residuals(a0, w, z, n)
+            assert res.max() <= 100 * n * eps and orth.max() <= 100 * n * eps
 
 
 @pytest.mark.parametrize("n,nm", [(7, 8), (31, 32), (33, 34), (65, 70), (200, 201)])
