@@ -45,6 +45,9 @@ constexpr int K3C_CH = 512;     // records staged per CTA
 
 template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD * 32 + 32 + 32 + 72; }
 
+// threads per row in k1_cta (column ranges split across warps)
+__host__ __device__ constexpr int k1_split(int n) { return n <= 256 ? 4 : (n <= 512 ? 2 : 1); }
+
 // ---------------------------------------------------------------- n == 1
 template <class T>
 __global__ void k_n1(const long L, const int nm, T *a, T *w)
@@ -76,44 +79,61 @@ __global__ void __launch_bounds__(32 * K1W_NW) k1_warp(const KP<T> p)
   for (int c = 0; c < n; c++)
     if (r > c && r < n) S[r + c * K1W_LD] = S[c + r * K1W_LD];
   __syncwarp();
-  tridiag_qt<T, 1>(tm, S, K1W_LD, n, p.d + k * n, p.e + k * n, beta_s, pv, red);
+  tridiag_qt<T, 1>(tm, S, K1W_LD, n, p.d + k * n, p.e + k * n, beta_s, pv, pv, red);
   if (r < n)
     for (int c = 0; c < n; c++) A[r + (size_t)c * nm] = S[r + c * K1W_LD];
 }
 
-template <class T, bool SM>
+// Shared memory of k1_cta: red[72], beta[n], pv[n], part[nthreads], then S
+// (shared-memory variant) n x (n|1).
+template <class T> __host__ __device__ inline size_t k1c_smem_elems(int n, int nthreads, bool sm)
+{
+  return 72 + 2 * (size_t)n + (size_t)nthreads + (sm ? (size_t)n * (size_t)(n | 1) : 0);
+}
+
+template <class T, bool SM, int SPLIT>
 __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long k = blockIdx.x;
-  const int n = p.n, nm = p.nm, r = threadIdx.x;
+  const int n = p.n, nm = p.nm, t = threadIdx.x, nt = blockDim.x;
   T *A = p.a + (size_t)k * nm * n;
   T *sm = reinterpret_cast<T *>(smem_raw);
   T *red = sm;          // 72
   T *beta_s = sm + 72;  // n
   T *pv = beta_s + n;   // n
+  T *part = pv + n;     // nt
   T *S;
   int ld;
   if (SM) {
     ld = n | 1;
-    S = pv + n;
-    for (int c = 0; c < n; c++)
-      if (r <= c) S[r + (size_t)c * ld] = A[r + (size_t)c * nm];
+    S = part + nt;
+    for (int idx = t; idx < n * n; idx += nt) {  // upper triangle, coalesced
+      const int r = idx % n, c = idx / n;
+      if (r <= c) S[r + c * ld] = A[r + (size_t)c * nm];
+    }
     __syncthreads();
-    for (int c = 0; c < n; c++)
-      if (r > c && r < n) S[r + (size_t)c * ld] = S[c + (size_t)r * ld];
+    for (int idx = t; idx < n * n; idx += nt) {
+      const int r = idx % n, c = idx / n;
+      if (r > c) S[r + c * ld] = S[c + r * ld];
+    }
     __syncthreads();
   } else {
     ld = nm;
     S = A;
-    for (int c = 0; c < n; c++)
-      if (r > c && r < n) A[r + (size_t)c * nm] = A[c + (size_t)r * nm];
+    for (long idx = t; idx < (long)n * n; idx += nt) {
+      const int r = (int)(idx % n), c = (int)(idx / n);
+      if (r > c) A[r + (size_t)c * nm] = A[c + (size_t)r * nm];
+    }
     __syncthreads();
   }
   CtaTeam tm;
-  tridiag_qt<T, 1>(tm, S, ld, n, p.d + k * n, p.e + k * n, beta_s, pv, red);
-  if (SM && r < n)
-    for (int c = 0; c < n; c++) A[r + (size_t)c * nm] = S[r + (size_t)c * ld];
+  tridiag_qt<T, SPLIT>(tm, S, ld, n, p.d + k * n, p.e + k * n, beta_s, pv, part, red);
+  if (SM)
+    for (int idx = t; idx < n * n; idx += nt) {
+      const int r = idx % n, c = idx / n;
+      A[r + (size_t)c * nm] = S[r + c * ld];
+    }
 }
 
 // ---------------------------------------------------------------- phase 2
@@ -187,8 +207,8 @@ __device__ void select_sort_serial(const int n, T *dwork, int *pos)
   {                                                   \
     const Rec<T> rr = *rp++;                          \
     const T h0 = z[I], h1 = z[I + 1];                 \
-    z[I + 1] = fma(rr.s, h0, rr.c * h1);              \
-    z[I] = fma(rr.c, h0, -(rr.s * h1));               \
+    z[I + 1] = fma(rr.c, h1, rr.s * h0);              \
+    z[I] = fma(-rr.s, h1, rr.c * h0);                 \
     if (--mm == 0) break;                             \
   }
 
@@ -331,6 +351,43 @@ __global__ void __launch_bounds__(32 * K3W_NW) k3_warp(const KP<T> p)
 }
 
 // ---------------------------------------------------------------- phase 3, n > 32
+// One rotation on a row: z_{i+1} <- s z_i + c z_{i+1}, z_i <- c z_i - s z_{i+1}
+// with the incoming z_{i+1} (h1) carried in a register.  Only one FMA sits
+// on the loop-carried path (h1 -> h1); c*h0 and s*h0 do not depend on it.
+template <class T>
+__device__ __forceinline__ T rot_step(const Rec<T> &rr, const T h0, T &h1)
+{
+  const T o = fma(rr.c, h1, rr.s * h0);
+  h1 = fma(-rr.s, h1, rr.c * h0);
+  return o;
+}
+
+// Applies rotations cur, cur-1, ..., cur-m+1 (records rp[0..m)) to one row
+// whose column c is zr[c*CS]; h1 carries Z(row, cur+1).  Column values are
+// loaded eight at a time so their latency overlaps the chain.
+template <class T, int CS>
+__device__ __forceinline__ void apply_run(T *__restrict__ zr, const int cs_rt, const Rec<T> *__restrict__ rp,
+                                          int cur, int m, T &h1)
+{
+  const int cs = CS > 0 ? CS : cs_rt;
+  T *p = zr + cur * cs;
+  int j = 0;
+  for (; j + 8 <= m; j += 8, p -= 8 * cs) {
+    T h0[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) h0[u] = p[-u * cs];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const Rec<T> rr = rp[j + u];
+      p[(1 - u) * cs] = rot_step(rr, h0[u], h1);
+    }
+  }
+  for (; j < m; j++, p -= cs) {
+    const T h0 = p[0];
+    p[cs] = rot_step(rp[j], h0, h1);
+  }
+}
+
 template <class T> __host__ __device__ inline size_t k3c_smem_bytes(int n, bool sm)
 {
   size_t b = sizeof(Rec<T>) * K3C_CH + sizeof(T) * (3 * (size_t)n + 64) + sizeof(int) * (2 * (size_t)n + 8);
@@ -339,6 +396,11 @@ template <class T> __host__ __device__ inline size_t k3c_smem_bytes(int n, bool 
   return b;
 }
 
+// Z layout: in shared memory row-major, Z(r, c) at Z[r*ldz + c] with ldz
+// odd (each thread walks its own contiguous row; at a fixed column the warp
+// touches rows with an odd stride: conflict-free).  In the workspace
+// (large n) column-major, Z(r, c) at Z[r + c*n], so that a warp's accesses
+// at a fixed column are coalesced.
 template <class T, bool SM>
 __global__ void __launch_bounds__(1024) k3_cta(const KP<T> p)
 {
@@ -356,42 +418,48 @@ __global__ void __launch_bounds__(1024) k3_cta(const KP<T> p)
   size_t zoff = sizeof(Rec<T>) * K3C_CH + sizeof(T) * (3 * (size_t)n + 64) + sizeof(int) * (2 * (size_t)n + 8);
   zoff = (zoff + 15) & ~(size_t)15;
   T *Z;
-  int ldz;
+  int rs, cs;  // element (r, c) at Z[r*rs + c*cs]
   if (SM) {
     Z = reinterpret_cast<T *>(smem_raw + zoff);
-    ldz = n | 1;
+    rs = n | 1;
+    cs = 1;
   } else {
     Z = p.zs + (size_t)k * n * n;
-    ldz = n;
+    rs = 1;
+    cs = n;
   }
   T *A = p.a + (size_t)k * nm * n;
-  for (long idx = t; idx < (long)n * n; idx += nt) {
-    const int c = (int)(idx % n), rr = (int)(idx / n);
-    Z[rr + (size_t)c * ldz] = A[c + (size_t)rr * nm];
+  // Z = Q = M^T with M = Q^T in a: Z(r, c) = M(c, r) = a[c + r*nm]
+  for (int idx = t; idx < n * n; idx += nt) {
+    const int c = idx % n, rr = idx / n;
+    Z[rr * rs + c * cs] = A[c + (size_t)rr * nm];
   }
   __syncthreads();
 
   const Meta mt = p.meta[k];
-  const int row = t;
-  const bool own = row < n;
+  const bool own = t < n;
+  T *zr = Z + (own ? t : 0) * rs;
   int cur = 0, rem = 0;
   T h1 = T(0);
   auto apply = [&](const Rec<T> *b, int nr) {
-    for (int q = 0; q < nr; q++) {
-      const Rec<T> rr = b[q];
+    int q = 0;
+    while (q < nr) {
       if (rem == 0) {
-        cur = hdr_i0(rr);
-        rem = hdr_cnt(rr);
-        if (own) h1 = Z[row + (size_t)(cur + 1) * ldz];
+        const Rec<T> hd = b[q++];
+        cur = hdr_i0(hd);
+        rem = hdr_cnt(hd);
+        h1 = own ? zr[(cur + 1) * cs] : T(0);
         continue;
       }
+      const int m = min(rem, nr - q);
       if (own) {
-        const T h0 = Z[row + (size_t)cur * ldz];
-        Z[row + (size_t)(cur + 1) * ldz] = fma(rr.s, h0, rr.c * h1);
-        h1 = fma(rr.c, h0, -(rr.s * h1));
+        if (SM) apply_run<T, 1>(zr, 1, b + q, cur, m, h1);
+        else apply_run<T, 0>(zr, cs, b + q, cur, m, h1);
       }
-      cur--;
-      if (--rem == 0 && own) Z[row + (size_t)(cur + 1) * ldz] = h1;
+      q += m;
+      rem -= m;
+      cur -= m;
+      if (rem == 0 && own) zr[(cur + 1) * cs] = h1;
     }
   };
   if (!mt.overflow) {
@@ -453,10 +521,8 @@ __global__ void __launch_bounds__(1024) k3_cta(const KP<T> p)
     }
     __syncthreads();
   }
-  for (int c = 0; c < n; c++) {
-    const int dst = inv[c];
-    if (own) A[row + (size_t)dst * nm] = Z[row + (size_t)c * ldz];
-  }
+  if (own)
+    for (int c = 0; c < n; c++) A[t + (size_t)inv[c] * nm] = Z[t * rs + c * cs];
   for (int c = t; c < n; c += nt) p.w[k * n + inv[c]] = sd[c];
   if (p.info && t == 0) p.info[k] = ierr;
 }

@@ -14,164 +14,183 @@
 // gives the same eigenvectors Q * Z_T up to rounding.
 //
 // Thread mapping: the team (one warp, or the whole CTA) owns the rows of
-// the full symmetric n x n matrix S (column-major, leading dimension ld):
-// thread t owns rows t, t + size, ..., t + (R-1)*size.  Every access S[r +
-// k*ld] of a team at fixed k touches consecutive rows, i.e. consecutive
-// addresses in shared memory (conflict-free) or in global memory
-// (coalesced).
+// the full symmetric n x n matrix S (column-major, leading dimension ld).
+// The team's nt threads form SPLIT groups of nr = nt/SPLIT threads; thread
+// t owns row r = t % nr and, within every row operation, the h-th of SPLIT
+// contiguous column ranges, h = t / nr.  nr is a multiple of 32, so a warp
+// has one h and 32 consecutive rows: at fixed column k it touches
+// consecutive addresses (shared memory: conflict-free; global: coalesced).
 #pragma once
 #include "eigb_common.cuh"
 
 namespace eigb {
 
+// Column range [lo, hi) of part h of [0, len) split in SPLIT pieces.
+template <int SPLIT>
+__host__ __device__ __forceinline__ void split_range(int len, int h, int &lo, int &hi)
+{
+  if (SPLIT == 1) {
+    lo = 0;
+    hi = len;
+  } else {
+    const int q = (len + SPLIT - 1) / SPLIT;
+    lo = min(len, h * q);
+    hi = min(len, lo + q);
+  }
+}
+
+// sum_{k in [lo,hi)} S[r + k*ld] * v[k] with four independent accumulators
+template <class T>
+__host__ __device__ __forceinline__ T dot_col(const T *__restrict__ Sr, const int ld, const T *__restrict__ v,
+                                              int lo, const int hi)
+{
+  T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+  int off = lo * ld;
+  for (; lo + 4 <= hi; lo += 4, off += 4 * ld) {
+    a0 = fma(Sr[off], v[lo], a0);
+    a1 = fma(Sr[off + ld], v[lo + 1], a1);
+    a2 = fma(Sr[off + 2 * ld], v[lo + 2], a2);
+    a3 = fma(Sr[off + 3 * ld], v[lo + 3], a3);
+  }
+  for (; lo < hi; lo++, off += ld) a0 = fma(Sr[off], v[lo], a0);
+  return (a0 + a1) + (a2 + a3);
+}
+
 // On entry S holds the full symmetric matrix (both triangles).  On exit
 // d_out[0:n] = diagonal, e_out[0:n] = off-diagonal (e_out[k] couples k and
 // k+1, e_out[n-1] = 0, the reference's convention tred1_tiled.hpp:207-212)
 // and S holds M = Q^T with A = Q T Q^T.
-//   beta_s, pv: n-element scratch in shared memory; red: 72 slots (64 for
-//   team reductions, red[64] carries the reflector pivot to the team).
-template <class T, int R, class Team>
-__host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T *d_out, T *e_out,
-                           T *beta_s, T *pv, T *red)
+// Shared scratch: beta_s[n], pv[n], part[SPLIT*nr], red[72] (64 for team
+// reductions, red[64] carries the reflector pivot to the team).
+template <class T, int SPLIT, class Team>
+__host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T *d_out, T *e_out, T *beta_s,
+                                    T *pv, T *part, T *red)
 {
   const int nt = tm.size();
+  const int nr = nt / SPLIT;
   const int t = tm.rank;
+  const int r = t % nr;
+  const int h = t / nr;
+  T *Sr = S + r;  // row r: element (r, k) at Sr[k*ld]
 
   for (int i = n - 1; i >= 1; --i) {
-    // ---- reflector from column i (rows 0..i-1) ----
-    T ur[R];
-    T ss = T(0);
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-      const int r = t + j * nt;
-      ur[j] = (r < i) ? S[r + (size_t)i * ld] : T(0);
-      ss = fma(ur[j], ur[j], ss);
-      // the owner of row i-1 publishes the pivot; the barrier in sum()
-      // orders it after the previous step's updates of that row
-      if (r == i - 1) red[64] = ur[j];
-    }
-    const T sig = tm.sum(ss, red);
+    const T *ucol = S + i * ld;  // reflector: column i, rows 0..i-1
+    // ---- reflector ----
+    // Column i was last updated (previous step) by the threads whose column
+    // range held i; only they read it before the barrier.
+    const int hs = (SPLIT == 1) ? 0 : i / ((i + SPLIT) / SPLIT);
+    T ur = (r < i && h == hs) ? ucol[r] : T(0);
+    if (r == i - 1 && h == hs) red[64] = ur;  // pivot, ordered by the barrier in sum()
+    const T sig = tm.sum(ur * ur, red);
     const T ulast = red[64];
     const T anorm = -copysign_t(sqr_t(sig), ulast);
     const T ul = ulast - anorm;
     const T beta = T(1) / flip0to1(ul * anorm);
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-      const int r = t + j * nt;
-      if (r == i - 1) {
-        ur[j] = ul;
-        S[r + (size_t)i * ld] = ul;  // reflector pivot stored back
-      }
-    }
+    ur = (r < i - 1) ? ucol[r] : ((r == i - 1) ? ul : T(0));
+    if (r == i - 1 && h == 0) S[(i - 1) + i * ld] = ul;  // reflector pivot stored back
     if (t == 0) {
       e_out[i - 1] = anorm;
       beta_s[i] = beta;
     }
+    int lo, hi;
+    split_range<SPLIT>(i, h, lo, hi);
 
-    // ---- p = beta * A(0:i-1, 0:i-1) u ----
-    T p[R];
+    // ---- p = beta * A(0:i-1, 0:i-1) u (this thread's column range) ----
+    if (r < i) {
+      // column i-1 of u is the new pivot ul: ucol[i-1] is being rewritten
+      const int hi1 = min(hi, i - 1);
+      T pp = dot_col(Sr, ld, ucol, lo, hi1);
+      if (lo <= i - 1 && i - 1 < hi) pp = fma(Sr[(i - 1) * ld], ul, pp);
+      if (SPLIT > 1) part[h * nr + r] = pp;
+      else pv[r] = pp * beta;
+    }
+    if (SPLIT > 1) {
+      tm.sync();
+      if (r < i && h == 0) {
+        T pp = T(0);
 #pragma unroll
-    for (int j = 0; j < R; j++) p[j] = T(0);
-    {
-      const T *ucol = S + (size_t)i * ld;
-      for (int k = 0; k < i - 1; k++) {
-        const T uk = ucol[k];
-        const T *sk = S + (size_t)k * ld;
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-          const int r = t + j * nt;
-          if (r < i) p[j] = fma(sk[r], uk, p[j]);
-        }
-      }
-      const T *sk = S + (size_t)(i - 1) * ld;
-#pragma unroll
-      for (int j = 0; j < R; j++) {
-        const int r = t + j * nt;
-        if (r < i) {
-          p[j] = fma(sk[r], ul, p[j]);
-          p[j] *= beta;
-          pv[r] = p[j];
-        }
+        for (int q = 0; q < SPLIT; q++) pp += part[q * nr + r];
+        pv[r] = pp * beta;
       }
     }
-    T pu = T(0);
+    // p_r of this row (all SPLIT threads of the row hold the same value)
+    T pr = T(0);
+    if (r < i) {
+      if (SPLIT > 1) {
 #pragma unroll
-    for (int j = 0; j < R; j++) pu = fma(p[j], ur[j], pu);
-    const T alpha = tm.sum(pu, red) * (beta * T(0.5));
+        for (int q = 0; q < SPLIT; q++) pr += part[q * nr + r];
+        pr *= beta;
+      } else {
+        pr = pv[r];
+      }
+    }
+    const T alpha = tm.sum(h == 0 ? pr * ur : T(0), red) * (beta * T(0.5));
 
-    // ---- A += u w^T + w u^T, w = p + alpha u (both triangles) ----
-    {
-      T wr[R];
-#pragma unroll
-      for (int j = 0; j < R; j++) wr[j] = fma(alpha, ur[j], p[j]);
-      const T *ucol = S + (size_t)i * ld;
-      for (int k = 0; k < i; k++) {
+    // ---- A += u w^T + w u^T, w = p + alpha u (both triangles, own columns) ----
+    if (r < i) {
+      const T wr = fma(alpha, ur, pr);
+      int off = lo * ld;
+      for (int k = lo; k < hi; k++, off += ld) {
         const T uk = ucol[k];
         const T wk = fma(alpha, uk, pv[k]);
-        T *sk = S + (size_t)k * ld;
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-          const int r = t + j * nt;
-          if (r < i) sk[r] = fma(wk, ur[j], fma(uk, wr[j], sk[r]));
-        }
+        Sr[off] = fma(wk, ur, fma(uk, wr, Sr[off]));
       }
     }
     // the barrier in the next step's first sum() orders these updates
   }
   tm.sync();
-#pragma unroll
-  for (int j = 0; j < R; j++) {
-    const int r = t + j * nt;
-    if (r < n) d_out[r] = S[r + (size_t)r * ld];
-  }
+  if (r < n && h == 0) d_out[r] = Sr[r * ld];
   if (t == 0) e_out[n - 1] = T(0);
   tm.sync();
 
   // ---- M = H_1 H_2 ... H_{n-1}, built in the leading k x k block ----
-  if (t == 0) S[0] = T(1);
+  // Step k extends M_{k-1} by e_{k-1} (row and column k-1) and applies
+  // H_k from the right: M <- M + beta_k (M u) u^T, u = column k.  Every
+  // thread writes only the entries of its own row and column range, which
+  // are also the only entries it reads, so the extension needs no barrier.
   for (int k = 1; k < n; k++) {
     const T bk = beta_s[k];
-    const T *ucol = S + (size_t)k * ld;  // reflector k, rows 0..k-1
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-      const int r = t + j * nt;
-      // extend M_{k-1} by e_{k-1}: column k-1 (rows < k-1) and row k-1
-      if (r < k - 1) S[r + (size_t)(k - 1) * ld] = T(0);
-      if (r == k - 1)
-        for (int c = 0; c < k; c++) S[r + (size_t)c * ld] = (c == k - 1) ? T(1) : T(0);
-    }
-    // M <- M + beta (M u) u^T, row-local
-    T q[R];
-#pragma unroll
-    for (int j = 0; j < R; j++) q[j] = T(0);
-    for (int c = 0; c < k; c++) {
-      const T uc = ucol[c];
-      const T *sc = S + (size_t)c * ld;
-#pragma unroll
-      for (int j = 0; j < R; j++) {
-        const int r = t + j * nt;
-        if (r < k) q[j] = fma(sc[r], uc, q[j]);
+    const T *ucol = S + k * ld;
+    int lo, hi;
+    split_range<SPLIT>(k, h, lo, hi);
+    if (r < k) {
+      if (k == 1) {
+        if (h == 0) Sr[0] = T(1);  // M_0 = [1]
+      } else if (r < k - 1) {
+        if (lo <= k - 1 && k - 1 < hi) Sr[(k - 1) * ld] = T(0);
+      } else {  // r == k-1: row k-1 of the extension
+        for (int c = lo; c < hi; c++) Sr[c * ld] = (c == k - 1) ? T(1) : T(0);
+      }
+      T q = dot_col(Sr, ld, ucol, lo, hi);
+      if (SPLIT > 1) {
+        part[h * nr + r] = q;
+      } else {
+        q *= bk;
+        int off = lo * ld;
+        for (int c = lo; c < hi; c++, off += ld) Sr[off] = fma(q, ucol[c], Sr[off]);
       }
     }
+    if (SPLIT > 1) {
+      tm.sync();
+      if (r < k) {
+        T q = T(0);
 #pragma unroll
-    for (int j = 0; j < R; j++) q[j] *= bk;
-    for (int c = 0; c < k; c++) {
-      const T uc = ucol[c];
-      T *sc = S + (size_t)c * ld;
-#pragma unroll
-      for (int j = 0; j < R; j++) {
-        const int r = t + j * nt;
-        if (r < k) sc[r] = fma(q[j], uc, sc[r]);
+        for (int s = 0; s < SPLIT; s++) q += part[s * nr + r];
+        q *= bk;
+        int off = lo * ld;
+        for (int c = lo; c < hi; c++, off += ld) Sr[off] = fma(q, ucol[c], Sr[off]);
       }
     }
-    tm.sync();  // column k is overwritten by the next extension
+    tm.sync();  // column k is overwritten by the next extension; part is reused
   }
-#pragma unroll
-  for (int j = 0; j < R; j++) {
-    const int r = t + j * nt;
-    if (r < n - 1) S[r + (size_t)(n - 1) * ld] = T(0);
-    if (r == n - 1)
-      for (int c = 0; c < n; c++) S[r + (size_t)c * ld] = (c == n - 1) ? T(1) : T(0);
+  if (r < n) {
+    int lo, hi;
+    split_range<SPLIT>(n, h, lo, hi);
+    if (r < n - 1) {
+      if (lo <= n - 1 && n - 1 < hi) Sr[(n - 1) * ld] = T(0);
+    } else {
+      for (int c = lo; c < hi; c++) Sr[c * ld] = (c == n - 1) ? T(1) : T(0);
+    }
   }
   tm.sync();
 }

@@ -76,7 +76,8 @@ inline void trace(long chunk, int slot, cudaStream_t stream)
   if (ev && 4 * chunk + 3 < nev) cudaEventRecord(ev[i], stream);
 }
 
-template <class T> size_t k1c_smem_bytes(int n) { return sizeof(T) * (72 + 2 * (size_t)n + (size_t)n * (n | 1)); }
+inline int k1c_threads(int n) { return std::min(1024, ((n + 31) / 32) * 32 * k1_split(n)); }
+template <class T> size_t k1c_smem_bytes(int n) { return sizeof(T) * k1c_smem_elems<T>(n, k1c_threads(n), true); }
 template <class T> size_t k2_smem_per_thread(int n) { return sizeof(T) * 2 * (size_t)n; }
 
 // Layout of the workspace for one chunk of Lc matrices.
@@ -152,6 +153,33 @@ template <class K> cudaError_t set_smem(K kern, size_t bytes)
   return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+template <class T> cudaError_t set_k1_smem(int n, bool sm, size_t bytes)
+{
+  const int sp = k1_split(n);
+  if (sm) {
+    if (sp == 4) return set_smem(k1_cta<T, true, 4>, bytes);
+    if (sp == 2) return set_smem(k1_cta<T, true, 2>, bytes);
+    return set_smem(k1_cta<T, true, 1>, bytes);
+  }
+  if (sp == 4) return set_smem(k1_cta<T, false, 4>, bytes);
+  if (sp == 2) return set_smem(k1_cta<T, false, 2>, bytes);
+  return set_smem(k1_cta<T, false, 1>, bytes);
+}
+
+template <class T> void launch_k1(const KP<T> &p, bool sm, unsigned blocks, int nt, size_t smem, cudaStream_t st)
+{
+  const int sp = k1_split(p.n);
+  if (sm) {
+    if (sp == 4) k1_cta<T, true, 4><<<blocks, nt, smem, st>>>(p);
+    else if (sp == 2) k1_cta<T, true, 2><<<blocks, nt, smem, st>>>(p);
+    else k1_cta<T, true, 1><<<blocks, nt, smem, st>>>(p);
+  } else {
+    if (sp == 4) k1_cta<T, false, 4><<<blocks, nt, smem, st>>>(p);
+    else if (sp == 2) k1_cta<T, false, 2><<<blocks, nt, smem, st>>>(p);
+    else k1_cta<T, false, 1><<<blocks, nt, smem, st>>>(p);
+  }
+}
+
 template <class T>
 cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork, int *info,
                 const eigen_GPU_batch_opts *opts, cudaStream_t stream)
@@ -209,7 +237,8 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const size_t k1w_smem = sizeof(T) * k1w_slot<T>() * K1W_NW;
   const size_t k3w_smem = sizeof(K3WSlot<T>) * K3W_NW;
   const int cta = std::min(1024, ((n + 31) / 32) * 32);
-  const size_t k1c_smem = pl.sm ? k1c_smem_bytes<T>(n) : sizeof(T) * (72 + 2 * (size_t)n);
+  const int k1c_nt = k1c_threads(n);
+  const size_t k1c_smem = sizeof(T) * k1c_smem_elems<T>(n, k1c_nt, pl.sm);
   const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.sm);
   int k2_tpb = 32;
   {
@@ -222,12 +251,13 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   if (n <= 32) {
     if ((err = set_smem(k1_warp<T>, k1w_smem)) != cudaSuccess) return err;
     if ((err = set_smem(k3_warp<T>, k3w_smem)) != cudaSuccess) return err;
-  } else if (pl.sm) {
-    if ((err = set_smem(k1_cta<T, true>, k1c_smem)) != cudaSuccess) return err;
-    if ((err = set_smem(k3_cta<T, true>, k3c_smem)) != cudaSuccess) return err;
   } else {
-    if ((err = set_smem(k1_cta<T, false>, k1c_smem)) != cudaSuccess) return err;
-    if ((err = set_smem(k3_cta<T, false>, k3c_smem)) != cudaSuccess) return err;
+    if ((err = set_k1_smem<T>(n, pl.sm, k1c_smem)) != cudaSuccess) return err;
+    if (pl.sm) {
+      if ((err = set_smem(k3_cta<T, true>, k3c_smem)) != cudaSuccess) return err;
+    } else if ((err = set_smem(k3_cta<T, false>, k3c_smem)) != cudaSuccess) {
+      return err;
+    }
   }
   if ((err = set_smem(k2_ql<T>, k2_smem)) != cudaSuccess) return err;
 
@@ -242,10 +272,8 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     if (n <= 32) {
       const unsigned nb = (unsigned)((lc + K1W_NW - 1) / K1W_NW);
       k1_warp<T><<<nb, 32 * K1W_NW, k1w_smem, stream>>>(p);
-    } else if (pl.sm) {
-      k1_cta<T, true><<<(unsigned)lc, cta, k1c_smem, stream>>>(p);
     } else {
-      k1_cta<T, false><<<(unsigned)lc, cta, k1c_smem, stream>>>(p);
+      launch_k1<T>(p, pl.sm, (unsigned)lc, k1c_nt, k1c_smem, stream);
     }
     trace(chunk, 1, stream);
     k2_ql<T><<<(unsigned)((lc + k2_tpb - 1) / k2_tpb), k2_tpb, k2_smem, stream>>>(p);

@@ -32,24 +32,31 @@ template <class T> struct HostTeam {
   }
 };
 
-template <class T> static void run(int n, int nthr, T *S, int ld, T *d, T *e)
+template <class T, int SPLIT> static void run(int n, int nthr, T *S, int ld, T *d, T *e)
 {
   HostShared<T> sh(nthr);
-  std::vector<T> beta(n + 1), pv(n + 1), red(72);
+  std::vector<T> beta(n + 1), pv(n + 1), part(nthr), red(72);
   std::vector<std::thread> th;
   for (int t = 0; t < nthr; t++)
     th.emplace_back([&, t]() {
       HostTeam<T> tm{t, nthr, 0, &sh};
-      eigb::tridiag_qt<T, 1>(tm, S, ld, n, d, e, beta.data(), pv.data(), red.data());
+      eigb::tridiag_qt<T, SPLIT>(tm, S, ld, n, d, e, beta.data(), pv.data(), part.data(), red.data());
     });
   for (auto &x : th) x.join();
 }
 
-extern "C" void host_tridiag_d(int n, int nthr, double *S, int ld, double *d, double *e)
+template <class T> static void run_split(int n, int nthr, int split, T *S, int ld, T *d, T *e)
 {
-  run<double>(n, nthr, S, ld, d, e);
+  if (split == 4) run<T, 4>(n, nthr, S, ld, d, e);
+  else if (split == 2) run<T, 2>(n, nthr, S, ld, d, e);
+  else run<T, 1>(n, nthr, S, ld, d, e);
 }
-extern "C" void host_tridiag_f(int n, int nthr, float *S, int ld, float *d, float *e)
+
+extern "C" void host_tridiag_d(int n, int nthr, int split, double *S, int ld, double *d, double *e)
 {
-  run<float>(n, nthr, S, ld, d, e);
+  run_split<double>(n, nthr, split, S, ld, d, e);
+}
+extern "C" void host_tridiag_f(int n, int nthr, int split, float *S, int ld, float *d, float *e)
+{
+  run_split<float>(n, nthr, split, S, ld, d, e);
 }

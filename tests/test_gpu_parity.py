@@ -213,7 +213,7 @@ def test_reference_check_api_writes_flags():
     a0 = 0.5 * (b + b.transpose(0, 2, 1))
     w, z, _ = gpu_solve(a0, n)
     z_bad = z.copy()
-    z_bad[2, 3] *= 1.5  # break one eigenvector of matrix 2
+    z_bad[2, 3] += 0.5 * z_bad[2, 4]  # mix two eigenvectors of matrix 2
     ad = torch.from_numpy(a0.copy()).cuda()
     wd = torch.from_numpy(w).cuda()
     zd = torch.from_numpy(z_bad).cuda()

@@ -33,7 +33,7 @@ def hostlibs():
         f = getattr(libs["ql_host"], "host_ql" + s)
         f.argtypes = [I, P, P, I, I, I, I, P, P, P]
         f.restype = I
-        getattr(libs["tridiag_host"], "host_tridiag" + s).argtypes = [I, I, P, I, P, P]
+        getattr(libs["tridiag_host"], "host_tridiag" + s).argtypes = [I, I, I, P, I, P, P]
     return libs
 
 
@@ -128,10 +128,11 @@ def test_ql_sweep_limit_reports_index(oracle_mod, hostlibs):
     assert st == 0 and ierr == 1
 
 
-@pytest.mark.parametrize("n,nthr", [(2, 32), (3, 32), (8, 32), (32, 32), (33, 64), (64, 64), (100, 128),
-                                    (64, 96)])
+@pytest.mark.parametrize("n,nthr,split", [(2, 32, 1), (3, 32, 1), (8, 32, 1), (32, 32, 1), (33, 64, 1), (64, 64, 1),
+                                          (100, 128, 1), (64, 96, 1), (33, 256, 4), (64, 256, 4), (100, 512, 4),
+                                          (77, 192, 2), (128, 512, 4)])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, dtype):
+def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, split, dtype):
     O = oracle_mod
     a0 = O.sym_uniform(1, n, seed=n)[0].astype(dtype)
     ld = n | 1
@@ -140,15 +141,17 @@ def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, dtype):
     d = np.zeros(n, dtype)
     e = np.zeros(n, dtype)
     f = hostlibs["tridiag_host"].host_tridiag_d if dtype == np.float64 else hostlibs["tridiag_host"].host_tridiag_f
-    f(n, nthr, _p(S), ld, _p(d), _p(e))
-    do, eo = tred(O, a0, n)
+    f(n, nthr, split, _p(S), ld, _p(d), _p(e))
     eps = np.finfo(dtype).eps
     scale = np.abs(a0).max() * n
-    # same reduction, different summation order: agreement to rounding level
-    assert np.abs(d - do).max() <= 512 * eps * scale
-    assert np.abs(np.abs(e) - np.abs(eo)).max() <= 512 * eps * scale
     M = S[:, :n].T.astype(np.float64)     # M[r, c] with r = row
     Q = M.T
     T = np.diag(d.astype(np.float64)) + np.diag(e[:-1].astype(np.float64), 1) + np.diag(e[:-1].astype(np.float64), -1)
+    # backward stable: A = Q T Q^T with Q orthogonal, to rounding level
     assert np.abs(Q @ T @ Q.T - a0).max() <= 64 * eps * scale
     assert np.abs(Q.T @ Q - np.eye(n)).max() <= 64 * eps * n
+    # same spectrum as the oracle's tridiagonal (the reduction is the same up
+    # to rounding; summation order differs)
+    do, eo = tred(O, a0, n)
+    To = np.diag(do.astype(np.float64)) + np.diag(eo[:-1].astype(np.float64), 1) + np.diag(eo[:-1].astype(np.float64), -1)
+    assert np.abs(np.linalg.eigvalsh(T) - np.linalg.eigvalsh(To)).max() <= 64 * eps * scale
