@@ -16,6 +16,7 @@
 #include "eigb_common.cuh"
 #include "eigb_ql.cuh"
 #include "eigb_tridiag.cuh"
+#include "eigb_tridiag_reg.cuh"
 
 namespace eigb {
 
@@ -134,6 +135,18 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
       const int r = idx % n, c = idx / n;
       A[r + (size_t)c * nm] = S[r + c * ld];
     }
+}
+
+// Register-resident phase 1 for 32 < n <= 32*NB, one CTA of NB*NB warps
+// per matrix (eigb_tridiag_reg.cuh).
+template <class T, int NB>
+__global__ void __launch_bounds__(32 * NB * NB, 1) k1_reg(const KP<T> p)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long k = blockIdx.x;
+  CtaTeam tm;
+  tridiag_qt_reg<T, NB>(tm, p.a + (size_t)k * p.nm * p.n, p.nm, p.n, p.d + k * p.n, p.e + k * p.n,
+                        reinterpret_cast<T *>(smem_raw));
 }
 
 // ---------------------------------------------------------------- phase 2
@@ -373,14 +386,17 @@ __device__ __forceinline__ void apply_run(T *__restrict__ zr, const int cs_rt, c
   T *p = zr + cur * cs;
   int j = 0;
   for (; j + 8 <= m; j += 8, p -= 8 * cs) {
+    // all loads of the block before its stores (the compiler cannot prove
+    // that the record buffer and Z do not alias)
     T h0[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) h0[u] = p[-u * cs];
+    Rec<T> rr[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
-      const Rec<T> rr = rp[j + u];
-      p[(1 - u) * cs] = rot_step(rr, h0[u], h1);
+      h0[u] = p[-u * cs];
+      rr[u] = rp[j + u];
     }
+#pragma unroll
+    for (int u = 0; u < 8; u++) p[(1 - u) * cs] = rot_step(rr[u], h0[u], h1);
   }
   for (; j < m; j++, p -= cs) {
     const T h0 = p[0];
@@ -401,8 +417,8 @@ template <class T> __host__ __device__ inline size_t k3c_smem_bytes(int n, bool 
 // touches rows with an odd stride: conflict-free).  In the workspace
 // (large n) column-major, Z(r, c) at Z[r + c*n], so that a warp's accesses
 // at a fixed column are coalesced.
-template <class T, bool SM>
-__global__ void __launch_bounds__(1024) k3_cta(const KP<T> p)
+template <class T, bool SM, int RPT>
+__global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long k = blockIdx.x;
@@ -437,10 +453,17 @@ __global__ void __launch_bounds__(1024) k3_cta(const KP<T> p)
   __syncthreads();
 
   const Meta mt = p.meta[k];
-  const bool own = t < n;
-  T *zr = Z + (own ? t : 0) * rs;
+  // thread t owns rows t + j*nt, j < RPT
+  bool own[RPT];
+  T *zr[RPT];
+  T h1[RPT];
+#pragma unroll
+  for (int j = 0; j < RPT; j++) {
+    own[j] = t + j * nt < n;
+    zr[j] = Z + (own[j] ? t + j * nt : 0) * rs;
+    h1[j] = T(0);
+  }
   int cur = 0, rem = 0;
-  T h1 = T(0);
   auto apply = [&](const Rec<T> *b, int nr) {
     int q = 0;
     while (q < nr) {
@@ -448,18 +471,25 @@ __global__ void __launch_bounds__(1024) k3_cta(const KP<T> p)
         const Rec<T> hd = b[q++];
         cur = hdr_i0(hd);
         rem = hdr_cnt(hd);
-        h1 = own ? zr[(cur + 1) * cs] : T(0);
+#pragma unroll
+        for (int j = 0; j < RPT; j++) h1[j] = own[j] ? zr[j][(cur + 1) * cs] : T(0);
         continue;
       }
       const int m = min(rem, nr - q);
-      if (own) {
-        if (SM) apply_run<T, 1>(zr, 1, b + q, cur, m, h1);
-        else apply_run<T, 0>(zr, cs, b + q, cur, m, h1);
-      }
+#pragma unroll
+      for (int j = 0; j < RPT; j++)
+        if (own[j]) {
+          if (SM) apply_run<T, 1>(zr[j], 1, b + q, cur, m, h1[j]);
+          else apply_run<T, 0>(zr[j], cs, b + q, cur, m, h1[j]);
+        }
       q += m;
       rem -= m;
       cur -= m;
-      if (rem == 0 && own) zr[(cur + 1) * cs] = h1;
+      if (rem == 0) {
+#pragma unroll
+        for (int j = 0; j < RPT; j++)
+          if (own[j]) zr[j][(cur + 1) * cs] = h1[j];
+      }
     }
   };
   if (!mt.overflow) {
@@ -521,8 +551,12 @@ __global__ void __launch_bounds__(1024) k3_cta(const KP<T> p)
     }
     __syncthreads();
   }
-  if (own)
-    for (int c = 0; c < n; c++) A[t + (size_t)inv[c] * nm] = Z[t * rs + c * cs];
+#pragma unroll
+  for (int j = 0; j < RPT; j++)
+    if (own[j]) {
+      const int row = t + j * nt;
+      for (int c = 0; c < n; c++) A[row + (size_t)inv[c] * nm] = Z[row * rs + c * cs];
+    }
   for (int c = t; c < n; c += nt) p.w[k * n + inv[c]] = sd[c];
   if (p.info && t == 0) p.info[k] = ierr;
 }

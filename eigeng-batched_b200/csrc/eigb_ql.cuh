@@ -35,8 +35,8 @@ template <class T> struct QLGen {
 template <class T> struct DEView {
   T *d, *e;
   int st;
-  __host__ __device__ __forceinline__ T &D(int i) const { return d[(size_t)i * st]; }
-  __host__ __device__ __forceinline__ T &E(int i) const { return e[(size_t)i * st]; }
+  __host__ __device__ __forceinline__ T &D(int i) const { return d[i * st]; }
+  __host__ __device__ __forceinline__ T &E(int i) const { return e[i * st]; }
 };
 
 template <class T>
@@ -89,13 +89,16 @@ __host__ __device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec
           g.dl1 = el * psr;
           v.D(l) = dl;
           v.D(l + 1) = g.dl1;
-          const T delta = dl_old - dl;
-          for (int j = l + 2; j < n; j++) v.D(j) -= delta;
-          g.shift += delta;
+          g.delta = dl_old - dl;
+          // d(j) -= delta for j >= l+2 (tql2_tiled.hpp:77-80): the sweep below
+          // reads d(l+2..m) exactly once, before overwriting them, and
+          // subtracts delta on that read; only d(m+1..n-1) are updated here.
+          for (int j = g.m + 1; j < n; j++) v.D(j) -= g.delta;
+          g.shift += g.delta;
         }
         g.c = T(1); g.c2 = T(1); g.c3 = T(1);
         g.s = T(0); g.s2 = T(0);
-        g.p = v.D(g.m);
+        g.p = (g.m >= g.l + 2) ? v.D(g.m) - g.delta : v.D(g.m);
         g.el1 = v.E(g.l + 1);
         g.ei = T(0);
         for (g.i = g.m - 1; g.i >= g.l; g.i--) {
@@ -116,7 +119,7 @@ __host__ __device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec
             g.c2 = g.c;
             g.s2 = g.s;
             const T ei = v.E(i);
-            const T di = v.D(i);
+            const T di = (i >= g.l + 2) ? v.D(i) - g.delta : v.D(i);
             const T gg = g.c * ei;
             const T h = g.c * g.p;
             T c, s, r;

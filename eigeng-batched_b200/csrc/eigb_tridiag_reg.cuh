@@ -1,0 +1,178 @@
+// Phase 1, register-resident form for 32 < n <= 32*NB (NB <= 4).
+//
+// Same method as eigb_tridiag.cuh (bottom-up Householder reduction of the
+// reference, tred1_tiled.hpp:42-205, then M = Q^T = H_1 ... H_{n-1}), but
+// the matrix never lives in shared memory: a CTA of NB*NB warps tiles the
+// padded NR x NR matrix (NR = 32*NB) into 32 x 32 blocks, warp (rb, cb)
+// holding rows 32*rb.. and columns 32*cb.. with one row slice of 32 values
+// per lane in registers.  Shared memory only carries what every block
+// needs: the reflectors (kept, zero padded, for the Q formation), the
+// vector p, the per-block partial sums and the team reductions.  A step
+// touches only the blocks that intersect the active leading i x i part.
+#pragma once
+#include "eigb_common.cuh"
+
+namespace eigb {
+
+// v[i] for a warp-uniform (or per-lane) dynamic index, by selects, so that
+// the array stays in registers
+template <class T>
+__host__ __device__ __forceinline__ T get32(const T (&v)[32], const int i)
+{
+  T r = v[0];
+#pragma unroll
+  for (int c = 1; c < 32; c++) r = (i == c) ? v[c] : r;
+  return r;
+}
+
+template <int NB> struct RegLayout {
+  static constexpr int NR = 32 * NB;
+  static constexpr int NT = NR * NB;
+};
+
+// Shared-memory elements of tridiag_qt_reg: V (max(n*NR, n*(n|1)), also the
+// staging area of the input), part[2*NB*NR], pv[NR], beta[NR], red[72].
+template <int NB> __host__ __device__ inline size_t reg_smem_elems(int n)
+{
+  constexpr int NR = RegLayout<NB>::NR;
+  const size_t v = (size_t)n * NR > (size_t)n * (n | 1) ? (size_t)n * NR : (size_t)n * (n | 1);
+  return v + 2 * (size_t)NB * NR + 2 * (size_t)NR + 72;
+}
+
+// A: the input matrix (upper triangle used), overwritten with M = Q^T.
+template <class T, int NB, class Team>
+__host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int n, T *d_out, T *e_out, T *sm)
+{
+  constexpr int NR = RegLayout<NB>::NR;
+  const int t = tm.rank;
+  const int lane = t & 31, w = t >> 5;
+  const int rb = w % NB, cb = w / NB;
+  const int r = 32 * rb + lane;
+  const int c0 = 32 * cb;
+  const int lds = n | 1;
+  size_t voff = (size_t)n * NR > (size_t)n * lds ? (size_t)n * NR : (size_t)n * lds;
+  T *V = sm;
+  T *part = sm + voff;
+  T *pv = part + 2 * NB * NR;
+  T *beta_s = pv + NR;
+  T *red = beta_s + NR;
+
+  // ---- stage the upper triangle, then build the register slices ----
+  for (int idx = t; idx < n * n; idx += tm.size()) {
+    const int rr = idx % n, cc = idx / n;
+    if (rr <= cc) V[rr + cc * lds] = A[rr + (size_t)cc * nm];
+  }
+  tm.sync();
+  T S[32];
+#pragma unroll
+  for (int c = 0; c < 32; c++) {
+    const int kc = c0 + c;
+    S[c] = (r < n && kc < n) ? (r <= kc ? V[r + kc * lds] : V[kc + r * lds]) : T(0);
+  }
+  tm.sync();  // the staging area becomes the reflector store
+
+  // ---- reduction, i = n-1 .. 1 ----
+  for (int i = n - 1; i >= 1; --i) {
+    T *Vi = V + (size_t)i * NR;
+    const int cbi = i >> 5;
+    T u0 = T(0);
+    if (cb == cbi) {  // the warps holding column i publish it
+      const T col = get32(S, i & 31);
+      u0 = (r < i) ? col : T(0);
+      Vi[r] = u0;
+      if (r == i - 1) red[64] = u0;
+    }
+    const T sig = tm.sum(u0 * u0, red);
+    const T ulast = red[64];
+    const T anorm = -copysign_t(sqr_t(sig), ulast);
+    const T ul = ulast - anorm;
+    const T beta = T(1) / flip0to1(ul * anorm);
+    if (cb == cbi && r == i - 1) Vi[r] = ul;  // pivot (read by others after the next barrier)
+    if (t == 0) {
+      e_out[i - 1] = anorm;
+      beta_s[i] = beta;
+    }
+    const bool act = (c0 < i) && (32 * rb < i);
+    if (act) {  // partial p_r over this block's columns; u_{i-1} is ul
+      const int cp = (i - 1) - c0;
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll
+      for (int c = 0; c < 32; c += 4) {
+        const T v0 = (c + 0 == cp) ? ul : Vi[c0 + c + 0];
+        const T v1 = (c + 1 == cp) ? ul : Vi[c0 + c + 1];
+        const T v2 = (c + 2 == cp) ? ul : Vi[c0 + c + 2];
+        const T v3 = (c + 3 == cp) ? ul : Vi[c0 + c + 3];
+        a0 = fma(S[c + 0], v0, a0);
+        a1 = fma(S[c + 1], v1, a1);
+        a2 = fma(S[c + 2], v2, a2);
+        a3 = fma(S[c + 3], v3, a3);
+      }
+      part[cb * NR + r] = (r < i) ? (a0 + a1) + (a2 + a3) : T(0);
+    }
+    tm.sync();
+    const int nact = (i + 31) >> 5;
+    T pr = T(0);
+    if (r < i) {
+#pragma unroll
+      for (int q = 0; q < NB; q++)
+        if (q < nact) pr += part[q * NR + r];
+      pr *= beta;
+    }
+    if (cb == 0) pv[r] = pr;  // 0 for r >= i
+    const T ur = Vi[r];       // u_r with the pivot in place, 0 for r >= i
+    const T alpha = tm.sum(cb == 0 ? pr * ur : T(0), red) * (beta * T(0.5));
+    if (act) {  // A += u w^T + w u^T on this block
+      const T wr = fma(alpha, ur, pr);
+#pragma unroll
+      for (int c = 0; c < 32; c++) {
+        const T uk = Vi[c0 + c];
+        const T wk = fma(alpha, uk, pv[c0 + c]);
+        S[c] = fma(wk, ur, fma(uk, wr, S[c]));
+      }
+    }
+    // the barrier in the next step's first sum() orders pv/part reuse
+  }
+  tm.sync();
+  if (r < n && cb == rb) d_out[r] = get32(S, r - c0);
+  if (t == 0) e_out[n - 1] = T(0);
+
+  // ---- M = H_1 ... H_{n-1}: M <- M + beta_k (M u_k) u_k^T from M = I ----
+  T *Mr = S;
+#pragma unroll
+  for (int c = 0; c < 32; c++) Mr[c] = (c0 + c == r) ? T(1) : T(0);
+  for (int k = 1; k < n; k++) {
+    const T bk = beta_s[k];
+    const T *Vk = V + (size_t)k * NR;
+    T *pb = part + (k & 1) * NB * NR;  // double buffer: one barrier per step
+    const bool act = (c0 < k) && (32 * rb < k);
+    if (act) {
+      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll
+      for (int c = 0; c < 32; c += 4) {
+        a0 = fma(Mr[c + 0], Vk[c0 + c + 0], a0);
+        a1 = fma(Mr[c + 1], Vk[c0 + c + 1], a1);
+        a2 = fma(Mr[c + 2], Vk[c0 + c + 2], a2);
+        a3 = fma(Mr[c + 3], Vk[c0 + c + 3], a3);
+      }
+      pb[cb * NR + r] = (a0 + a1) + (a2 + a3);
+    }
+    tm.sync();
+    if (act) {
+      const int nact = (k + 31) >> 5;
+      T q = T(0);
+#pragma unroll
+      for (int s = 0; s < NB; s++)
+        if (s < nact) q += pb[s * NR + r];
+      q *= bk;
+#pragma unroll
+      for (int c = 0; c < 32; c++) Mr[c] = fma(q, Vk[c0 + c], Mr[c]);
+    }
+  }
+  if (r < n) {
+#pragma unroll
+    for (int c = 0; c < 32; c++)
+      if (c0 + c < n) A[r + (size_t)(c0 + c) * nm] = Mr[c];
+  }
+}
+
+}  // namespace eigb

@@ -153,6 +153,34 @@ template <class K> cudaError_t set_smem(K kern, size_t bytes)
   return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// phase 1 in registers for 32 < n <= 128 (NB = ceil(n/32) column blocks)
+inline int reg_nb(int n) { return (n > 32 && n <= 128) ? (n + 31) / 32 : 0; }
+template <class T> size_t k1r_smem_bytes(int n)
+{
+  switch (reg_nb(n)) {
+    case 2: return sizeof(T) * reg_smem_elems<2>(n);
+    case 3: return sizeof(T) * reg_smem_elems<3>(n);
+    case 4: return sizeof(T) * reg_smem_elems<4>(n);
+    default: return 0;
+  }
+}
+template <class T> cudaError_t set_k1r_smem(int n, size_t bytes)
+{
+  switch (reg_nb(n)) {
+    case 2: return set_smem(k1_reg<T, 2>, bytes);
+    case 3: return set_smem(k1_reg<T, 3>, bytes);
+    case 4: return set_smem(k1_reg<T, 4>, bytes);
+    default: return cudaErrorInvalidValue;
+  }
+}
+template <class T> void launch_k1r(const KP<T> &p, unsigned blocks, size_t smem, cudaStream_t st)
+{
+  const int nb = reg_nb(p.n);
+  if (nb == 2) k1_reg<T, 2><<<blocks, 32 * 4, smem, st>>>(p);
+  else if (nb == 3) k1_reg<T, 3><<<blocks, 32 * 9, smem, st>>>(p);
+  else k1_reg<T, 4><<<blocks, 32 * 16, smem, st>>>(p);
+}
+
 template <class T> cudaError_t set_k1_smem(int n, bool sm, size_t bytes)
 {
   const int sp = k1_split(n);
@@ -236,9 +264,11 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   // launch geometry
   const size_t k1w_smem = sizeof(T) * k1w_slot<T>() * K1W_NW;
   const size_t k3w_smem = sizeof(K3WSlot<T>) * K3W_NW;
-  const int cta = std::min(1024, ((n + 31) / 32) * 32);
+  // phase 3: one row per thread up to 512 rows, two above
+  const int k3_nt = n > 512 ? (((n + 1) / 2 + 31) / 32) * 32 : ((n + 31) / 32) * 32;
   const int k1c_nt = k1c_threads(n);
-  const size_t k1c_smem = sizeof(T) * k1c_smem_elems<T>(n, k1c_nt, pl.sm);
+  const bool k1_in_regs = reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin;
+  const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems<T>(n, k1c_nt, pl.sm);
   const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.sm);
   int k2_tpb = 32;
   {
@@ -252,10 +282,14 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     if ((err = set_smem(k1_warp<T>, k1w_smem)) != cudaSuccess) return err;
     if ((err = set_smem(k3_warp<T>, k3w_smem)) != cudaSuccess) return err;
   } else {
-    if ((err = set_k1_smem<T>(n, pl.sm, k1c_smem)) != cudaSuccess) return err;
+    if (k1_in_regs) {
+      if ((err = set_k1r_smem<T>(n, k1c_smem)) != cudaSuccess) return err;
+    } else if ((err = set_k1_smem<T>(n, pl.sm, k1c_smem)) != cudaSuccess) {
+      return err;
+    }
     if (pl.sm) {
-      if ((err = set_smem(k3_cta<T, true>, k3c_smem)) != cudaSuccess) return err;
-    } else if ((err = set_smem(k3_cta<T, false>, k3c_smem)) != cudaSuccess) {
+      if ((err = set_smem(k3_cta<T, true, 1>, k3c_smem)) != cudaSuccess) return err;
+    } else if ((err = set_smem(n > 512 ? k3_cta<T, false, 2> : k3_cta<T, false, 1>, k3c_smem)) != cudaSuccess) {
       return err;
     }
   }
@@ -272,6 +306,8 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     if (n <= 32) {
       const unsigned nb = (unsigned)((lc + K1W_NW - 1) / K1W_NW);
       k1_warp<T><<<nb, 32 * K1W_NW, k1w_smem, stream>>>(p);
+    } else if (k1_in_regs) {
+      launch_k1r<T>(p, (unsigned)lc, k1c_smem, stream);
     } else {
       launch_k1<T>(p, pl.sm, (unsigned)lc, k1c_nt, k1c_smem, stream);
     }
@@ -282,9 +318,11 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
       const unsigned nb = (unsigned)((lc + K3W_NW - 1) / K3W_NW);
       k3_warp<T><<<nb, 32 * K3W_NW, k3w_smem, stream>>>(p);
     } else if (pl.sm) {
-      k3_cta<T, true><<<(unsigned)lc, cta, k3c_smem, stream>>>(p);
+      k3_cta<T, true, 1><<<(unsigned)lc, k3_nt, k3c_smem, stream>>>(p);
+    } else if (n > 512) {
+      k3_cta<T, false, 2><<<(unsigned)lc, k3_nt, k3c_smem, stream>>>(p);
     } else {
-      k3_cta<T, false><<<(unsigned)lc, cta, k3c_smem, stream>>>(p);
+      k3_cta<T, false, 1><<<(unsigned)lc, k3_nt, k3c_smem, stream>>>(p);
     }
     trace(chunk, 3, stream);
     if ((err = cudaGetLastError()) != cudaSuccess) return err;

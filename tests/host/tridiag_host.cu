@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../eigeng-batched_b200/csrc/eigb_tridiag.cuh"
+#include "../../eigeng-batched_b200/csrc/eigb_tridiag_reg.cuh"
 
 template <class T> struct HostShared {
   std::barrier<> bar;
@@ -60,3 +61,29 @@ extern "C" void host_tridiag_f(int n, int nthr, int split, float *S, int ld, flo
 {
   run_split<float>(n, nthr, split, S, ld, d, e);
 }
+
+// register-resident variant: one "thread" per GPU thread of the CTA
+template <class T, int NB> static void run_reg(int n, T *A, int nm, T *d, T *e)
+{
+  const int nthr = 32 * NB * NB;
+  HostShared<T> sh(nthr);
+  std::vector<T> smem(eigb::reg_smem_elems<NB>(n));
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthr; t++)
+    th.emplace_back([&, t]() {
+      HostTeam<T> tm{t, nthr, 0, &sh};
+      eigb::tridiag_qt_reg<T, NB>(tm, A, nm, n, d, e, smem.data());
+    });
+  for (auto &x : th) x.join();
+}
+
+template <class T> static void run_reg_nb(int n, T *A, int nm, T *d, T *e)
+{
+  const int nb = (n + 31) / 32;
+  if (nb <= 2) run_reg<T, 2>(n, A, nm, d, e);
+  else if (nb == 3) run_reg<T, 3>(n, A, nm, d, e);
+  else run_reg<T, 4>(n, A, nm, d, e);
+}
+
+extern "C" void host_tridiag_reg_d(int n, double *A, int nm, double *d, double *e) { run_reg_nb<double>(n, A, nm, d, e); }
+extern "C" void host_tridiag_reg_f(int n, float *A, int nm, float *d, float *e) { run_reg_nb<float>(n, A, nm, d, e); }

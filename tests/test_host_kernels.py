@@ -34,6 +34,7 @@ def hostlibs():
         f.argtypes = [I, P, P, I, I, I, I, P, P, P]
         f.restype = I
         getattr(libs["tridiag_host"], "host_tridiag" + s).argtypes = [I, I, I, P, I, P, P]
+        getattr(libs["tridiag_host"], "host_tridiag_reg" + s).argtypes = [I, P, I, P, P]
     return libs
 
 
@@ -152,6 +153,34 @@ def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, split, dtype):
     assert np.abs(Q.T @ Q - np.eye(n)).max() <= 64 * eps * n
     # same spectrum as the oracle's tridiagonal (the reduction is the same up
     # to rounding; summation order differs)
+    do, eo = tred(O, a0, n)
+    To = np.diag(do.astype(np.float64)) + np.diag(eo[:-1].astype(np.float64), 1) + np.diag(eo[:-1].astype(np.float64), -1)
+    assert np.abs(np.linalg.eigvalsh(T) - np.linalg.eigvalsh(To)).max() <= 64 * eps * scale
+
+
+@pytest.mark.parametrize("n,nm", [(33, 33), (40, 41), (64, 64), (65, 66), (96, 96), (100, 101), (128, 128)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_tridiag_register_variant(oracle_mod, hostlibs, n, nm, dtype):
+    """The register-resident phase 1 (eigb_tridiag_reg.cuh): reads the upper
+    triangle of a (nm x n, column-major), leaves M = Q^T in its place."""
+    O = oracle_mod
+    a0 = O.sym_uniform(1, n, seed=n + 1)[0].astype(dtype)
+    A = np.full((n, nm), np.nan, dtype)  # A[c, r] = element (r, c)
+    A[:, :n] = a0
+    for c in range(n):
+        A[c, c + 1:n] = np.nan            # strict lower triangle is never read
+    d = np.zeros(n, dtype)
+    e = np.zeros(n, dtype)
+    f = hostlibs["tridiag_host"].host_tridiag_reg_d if dtype == np.float64 else hostlibs["tridiag_host"].host_tridiag_reg_f
+    f(n, _p(A), nm, _p(d), _p(e))
+    eps = np.finfo(dtype).eps
+    scale = np.abs(a0).max() * n
+    M = A[:, :n].T.astype(np.float64)
+    Q = M.T
+    T = np.diag(d.astype(np.float64)) + np.diag(e[:-1].astype(np.float64), 1) + np.diag(e[:-1].astype(np.float64), -1)
+    assert np.abs(Q @ T @ Q.T - a0).max() <= 64 * eps * scale
+    assert np.abs(Q.T @ Q - np.eye(n)).max() <= 64 * eps * n
+    assert np.isnan(A[:, n:]).all()     # padding rows untouched
     do, eo = tred(O, a0, n)
     To = np.diag(do.astype(np.float64)) + np.diag(eo[:-1].astype(np.float64), 1) + np.diag(eo[:-1].astype(np.float64), -1)
     assert np.abs(np.linalg.eigvalsh(T) - np.linalg.eigvalsh(To)).max() <= 64 * eps * scale
