@@ -13,6 +13,8 @@
 //   k_jacobi_warp  cyclic Jacobi for n <= 32 (jac_tiled.hpp:3-152)
 //   k_check        FP64 residual / orthogonality gate (eigen_GPU_check.cu)
 #pragma once
+#include <stdio.h>
+
 #include "eigb_common.cuh"
 #include "eigb_ql.cuh"
 #include "eigb_tridiag.cuh"
@@ -42,7 +44,6 @@ constexpr int K1W_NW = 4;       // warps (matrices) per CTA in k1_warp
 constexpr int K1W_LD = 33;      // padded leading dimension, odd
 constexpr int K3W_NW = 4;       // warps per CTA in k3_warp
 constexpr int K3W_CH = 128;     // records staged per warp
-constexpr int K3C_CH = 512;     // records staged per CTA
 
 template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD * 32 + 32 + 32 + 72; }
 
@@ -166,20 +167,19 @@ __global__ void k2_ql(const KP<T> p)
     dd[(size_t)i * st] = din[i];
     ee[(size_t)i * st] = ein[i];
   }
-  QLGen<T> g;
-  g.pc = PC_START;
-  DEView<T> v{dd, ee, st};
   Rec<T> *out = p.rec + (size_t)k * p.rcap;
-  const int nr = ql_run(p.method, g, v, n, out, p.rcap, p.max_sweep);
+  int ierr = 0;
+  const int nr = (p.method == QL_IMTQL2) ? ql_imtql2_fast(dd, ee, st, n, out, p.rcap, p.max_sweep, &ierr)
+                                         : ql_tql2_fast(dd, ee, st, n, out, p.rcap, p.max_sweep, &ierr);
   Meta mt;
-  mt.nrec = nr;
+  mt.nrec = nr < 0 ? 0 : nr;
   mt.pad = 0;
-  if (g.pc != PC_DONE) {
+  if (nr < 0) {
     mt.overflow = 1;
     mt.ierr = 0;
   } else {
     mt.overflow = 0;
-    mt.ierr = g.ierr;
+    mt.ierr = ierr;
     T *wo = p.w + k * n;
     for (int i = 0; i < n; i++) wo[i] = dd[(size_t)i * st];
   }
@@ -364,79 +364,134 @@ __global__ void __launch_bounds__(32 * K3W_NW) k3_warp(const KP<T> p)
 }
 
 // ---------------------------------------------------------------- phase 3, n > 32
-// One rotation on a row: z_{i+1} <- s z_i + c z_{i+1}, z_i <- c z_i - s z_{i+1}
-// with the incoming z_{i+1} (h1) carried in a register.  Only one FMA sits
-// on the loop-carried path (h1 -> h1); c*h0 and s*h0 do not depend on it.
-template <class T>
-__device__ __forceinline__ T rot_step(const Rec<T> &rr, const T h0, T &h1)
-{
-  const T o = fma(rr.c, h1, rr.s * h0);
-  h1 = fma(-rr.s, h1, rr.c * h0);
-  return o;
-}
+constexpr int K3_WAVE = 4;  // sweeps applied per pass in k3_cta
 
-// Applies rotations cur, cur-1, ..., cur-m+1 (records rp[0..m)) to one row
-// whose column c is zr[c*CS]; h1 carries Z(row, cur+1).  Column values are
-// loaded eight at a time so their latency overlaps the chain.
-template <class T, int CS>
-__device__ __forceinline__ void apply_run(T *__restrict__ zr, const int cs_rt, const Rec<T> *__restrict__ rp,
-                                          int cur, int m, T &h1)
+// Records staged per chunk in k3_cta: room for K3_WAVE whole segments.
+__host__ __device__ inline int k3c_chunk(int n) { return ((K3_WAVE * (n + 1) + 63) / 64) * 64; }
+
+template <class T> __host__ __device__ inline size_t k3c_fixed_bytes(int n)
 {
-  const int cs = CS > 0 ? CS : cs_rt;
-  T *p = zr + cur * cs;
-  int j = 0;
-  for (; j + 8 <= m; j += 8, p -= 8 * cs) {
-    // all loads of the block before its stores (the compiler cannot prove
-    // that the record buffer and Z do not alias)
-    T h0[8];
-    Rec<T> rr[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      h0[u] = p[-u * cs];
-      rr[u] = rp[j + u];
-    }
-#pragma unroll
-    for (int u = 0; u < 8; u++) p[(1 - u) * cs] = rot_step(rr[u], h0[u], h1);
-  }
-  for (; j < m; j++, p -= cs) {
-    const T h0 = p[0];
-    p[cs] = rot_step(rp[j], h0, h1);
-  }
+  size_t b = sizeof(Rec<T>) * (size_t)k3c_chunk(n) + sizeof(T) * (3 * (size_t)n + 64) +
+             sizeof(int) * (2 * (size_t)n + 8);
+  return (b + 15) & ~(size_t)15;
 }
 
 template <class T> __host__ __device__ inline size_t k3c_smem_bytes(int n, bool sm)
 {
-  size_t b = sizeof(Rec<T>) * K3C_CH + sizeof(T) * (3 * (size_t)n + 64) + sizeof(int) * (2 * (size_t)n + 8);
-  b = (b + 15) & ~(size_t)15;
+  size_t b = k3c_fixed_bytes<T>(n);
   if (sm) b += sizeof(T) * (size_t)n * (size_t)(n | 1);
   return b;
 }
 
-// Z layout: in shared memory row-major, Z(r, c) at Z[r*ldz + c] with ldz
-// odd (each thread walks its own contiguous row; at a fixed column the warp
-// touches rows with an odd stride: conflict-free).  In the workspace
-// (large n) column-major, Z(r, c) at Z[r + c*n], so that a warp's accesses
-// at a fixed column are coalesced.
+// Applies a group of ns <= K3_WAVE consecutive sweeps (segment s: rotations
+// i0[s], i0[s]-1, ..., i0[s]-len[s]+1, records rb[off[s]...]) to one row
+// whose column c is zr[c*cs].  Sweep s runs one column behind sweep s-1 as
+// stage s of a pipeline: at step j0 stage s handles column j0+s, taking the
+// column value just produced by stage s-1; outside its range a stage is an
+// identity rotation, i.e. a one-column delay.  The loop is skewed so that
+// the stages of one iteration are independent (stage s works on step
+// tau-s); every column is loaded once (stage 0) and stored once (last stage).
+template <class T, int CS>
+__host__ __device__ __forceinline__ void wave_apply(T *__restrict__ zr, const int cs_rt, const int n,
+                                           const Rec<T> *__restrict__ rb, const int (&i0)[K3_WAVE],
+                                           const int (&len)[K3_WAVE], const int (&off)[K3_WAVE], const int ns)
+{
+  const int cs = CS > 0 ? CS : cs_rt;
+  int jt = -0x3fffffff, jb = 0x3fffffff;
+#pragma unroll
+  for (int s = 0; s < K3_WAVE; s++)
+    if (s < ns) {
+      jt = max(jt, i0[s] - s);
+      jb = min(jb, i0[s] - len[s] + 1 - s);
+    }
+  const int nsteps = jt - (jb - ns) + 1;
+  T h1[K3_WAVE], x[K3_WAVE];
+#pragma unroll
+  for (int s = 0; s < K3_WAVE; s++) {
+    const int col = jt + s + 1;
+    h1[s] = (s < ns && col < n) ? zr[col * cs] : T(0);
+    x[s] = T(0);
+  }
+  for (int tau = 0; tau < nsteps + ns - 1; tau++) {
+    T y[K3_WAVE];
+#pragma unroll
+    for (int s = 0; s < K3_WAVE; s++) {
+      y[s] = T(0);
+      const int step = tau - s;
+      if (s < ns && step >= 0 && step < nsteps) {
+        const int j0 = jt - step;
+        const int col = j0 + s;
+        const T in = (s == 0) ? ((j0 >= 0) ? zr[j0 * cs] : T(0)) : x[s > 0 ? s - 1 : 0];
+        if (col <= i0[s] && col > i0[s] - len[s]) {
+          const Rec<T> rr = rb[off[s] + (i0[s] - col)];
+          y[s] = fma(rr.c, h1[s], rr.s * in);
+          h1[s] = fma(-rr.s, h1[s], rr.c * in);
+        } else {
+          y[s] = h1[s];
+          h1[s] = in;
+        }
+        if (s == ns - 1) {
+          const int oc = j0 + ns;
+          if (oc >= 0 && oc < n) zr[oc * cs] = y[s];
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < K3_WAVE; s++) x[s] = y[s];
+  }
+}
+
+// Reads up to K3_WAVE complete segments (header + rotations) from
+// rbuf[q..cnt); advances q past them; returns how many were read.
+template <class T>
+__host__ __device__ __forceinline__ int parse_group(const Rec<T> *rbuf, const int cnt, int &q, int (&i0)[K3_WAVE],
+                                                    int (&len)[K3_WAVE], int (&off)[K3_WAVE])
+{
+  int ns = 0;
+#pragma unroll
+  for (int s = 0; s < K3_WAVE; s++) {
+    i0[s] = 0;
+    len[s] = 0;
+    off[s] = 0;
+    if (ns == s && q < cnt) {
+      const Rec<T> hd = rbuf[q];
+      const int L = hdr_cnt(hd);
+      if (L >= 1 && q + 1 + L <= cnt) {
+        i0[s] = hdr_i0(hd);
+        len[s] = L;
+        off[s] = q + 1;
+        q += 1 + L;
+        ns++;
+      }
+    }
+  }
+  return ns;
+}
+
+// Z layout: in shared memory row-major, Z(r, c) at Z[r*(n|1) + c] (each
+// thread walks its own contiguous row; at a fixed column the warp touches
+// rows with an odd stride: conflict-free).  In the workspace (large n)
+// column-major, Z(r, c) at Z[r + c*n], so that a warp's accesses at a fixed
+// column are coalesced.
 template <class T, bool SM, int RPT>
 __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long k = blockIdx.x;
   const int n = p.n, nm = p.nm, t = threadIdx.x, nt = blockDim.x;
+  const int ch = k3c_chunk(n);
   Rec<T> *rbuf = reinterpret_cast<Rec<T> *>(smem_raw);
-  T *sd = reinterpret_cast<T *>(rbuf + K3C_CH);
+  T *sd = reinterpret_cast<T *>(rbuf + ch);
   T *se = sd + n;
   T *sdd = se + n;
   T *red = sdd + n;
   int *inv = reinterpret_cast<int *>(red + 64);
   int *pos = inv + n;
   int *sflag = pos + n;  // [0] nrec, [1] done, [2] ierr
-  size_t zoff = sizeof(Rec<T>) * K3C_CH + sizeof(T) * (3 * (size_t)n + 64) + sizeof(int) * (2 * (size_t)n + 8);
-  zoff = (zoff + 15) & ~(size_t)15;
   T *Z;
   int rs, cs;  // element (r, c) at Z[r*rs + c*cs]
   if (SM) {
-    Z = reinterpret_cast<T *>(smem_raw + zoff);
+    Z = reinterpret_cast<T *>(smem_raw + k3c_fixed_bytes<T>(n));
     rs = n | 1;
     cs = 1;
   } else {
@@ -453,57 +508,46 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
   __syncthreads();
 
   const Meta mt = p.meta[k];
-  // thread t owns rows t + j*nt, j < RPT
   bool own[RPT];
   T *zr[RPT];
-  T h1[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; j++) {
     own[j] = t + j * nt < n;
     zr[j] = Z + (own[j] ? t + j * nt : 0) * rs;
-    h1[j] = T(0);
   }
-  int cur = 0, rem = 0;
-  auto apply = [&](const Rec<T> *b, int nr) {
+  // applies the complete segments of rbuf[0..cnt) in groups of K3_WAVE;
+  // returns the index of the first incomplete segment
+  auto apply_chunk = [&](const int cnt) {
     int q = 0;
-    while (q < nr) {
-      if (rem == 0) {
-        const Rec<T> hd = b[q++];
-        cur = hdr_i0(hd);
-        rem = hdr_cnt(hd);
-#pragma unroll
-        for (int j = 0; j < RPT; j++) h1[j] = own[j] ? zr[j][(cur + 1) * cs] : T(0);
-        continue;
-      }
-      const int m = min(rem, nr - q);
+    while (true) {
+      int i0[K3_WAVE], len[K3_WAVE], off[K3_WAVE];
+      const int ns = parse_group(rbuf, cnt, q, i0, len, off);
+      if (ns == 0) break;
 #pragma unroll
       for (int j = 0; j < RPT; j++)
         if (own[j]) {
-          if (SM) apply_run<T, 1>(zr[j], 1, b + q, cur, m, h1[j]);
-          else apply_run<T, 0>(zr[j], cs, b + q, cur, m, h1[j]);
+          if (SM) wave_apply<T, 1>(zr[j], 1, n, rbuf, i0, len, off, ns);
+          else wave_apply<T, 0>(zr[j], cs, n, rbuf, i0, len, off, ns);
         }
-      q += m;
-      rem -= m;
-      cur -= m;
-      if (rem == 0) {
-#pragma unroll
-        for (int j = 0; j < RPT; j++)
-          if (own[j]) zr[j][(cur + 1) * cs] = h1[j];
-      }
     }
+    return q;
   };
   if (!mt.overflow) {
     const Rec<T> *src = p.rec + (size_t)k * p.rcap;
-    for (int base = 0; base < mt.nrec; base += K3C_CH) {
-      const int cnt = min(K3C_CH, mt.nrec - base);
+    int base = 0;
+    while (base < mt.nrec) {
+      const int cnt = min(ch, mt.nrec - base);
       for (int q = t; q < cnt; q += nt) rbuf[q] = src[base + q];
       __syncthreads();
-      apply(rbuf, cnt);
+      const int used = apply_chunk(cnt);
       __syncthreads();
+      base += used > 0 ? used : cnt;  // a segment is at most n records: used > 0
     }
     for (int c = t; c < n; c += nt) sd[c] = p.w[k * n + c];
     if (t == 0) sflag[2] = mt.ierr;
   } else {
+    // capacity exceeded in phase 2: regenerate in chunks (segments are
+    // closed at every chunk end, so each chunk is self-contained)
     for (int c = t; c < n; c += nt) {
       sd[c] = p.d[k * n + c];
       se[c] = p.e[k * n + c];
@@ -513,14 +557,14 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
     g.pc = PC_START;
     while (true) {
       if (t == 0) {
-        sflag[0] = ql_run(p.method, g, DEView<T>{sd, se, 1}, n, rbuf, K3C_CH, p.max_sweep);
+        sflag[0] = ql_run(p.method, g, DEView<T>{sd, se, 1}, n, rbuf, ch, p.max_sweep);
         sflag[1] = (g.pc == PC_DONE);
         sflag[2] = g.ierr;
       }
       __syncthreads();
       const int nr = sflag[0];
       const int done = sflag[1];
-      apply(rbuf, nr);
+      apply_chunk(nr);
       __syncthreads();
       if (done) break;
     }

@@ -255,6 +255,175 @@ finish:
   return nrec;
 }
 
+// ---------------------------------------------------------------------------
+// Fast single-call forms used by phase 2: the whole iteration in one call
+// with a fixed record capacity, no resume points, and the capacity checked
+// once per sweep.  Same arithmetic as ql_tql2 / ql_imtql2 (identical
+// rotations and eigenvalues).  Returns the record count, or -1 when the
+// capacity would be exceeded (phase 3 then regenerates with the resumable
+// form).  *ierr receives 0 or the failing 1-based index.
+template <class T>
+__host__ __device__ int ql_tql2_fast(T *__restrict__ d, T *__restrict__ e, const int st, const int n,
+                                     Rec<T> *__restrict__ out, const int cap, const int max_sweep, int *ierr)
+{
+  const T tol = Num<T>::eps() * Num<T>::tolmul();
+  int nrec = 0;
+  *ierr = 0;
+  if (n <= 1) return 0;
+  T shift = T(0), tst1 = T(0);
+  for (int l = 0; l < n; l++) {
+    T *dl_p = d + l * st;
+    T *el_p = e + l * st;
+    tst1 = fmax_t(tst1, (fabs_t(*dl_p) + fabs_t(*el_p)) * tol);
+    int m = l;
+    {
+      const T *ep = el_p;
+      while (m < n && !(fabs_t(*ep) <= tst1)) {
+        m++;
+        ep += st;
+      }
+    }
+    if (m >= n) {
+      *ierr = l + 1;
+      return nrec;
+    }
+    if (m != l) {
+      const int len = m - l;
+      int itr;
+      for (itr = 0; itr < max_sweep; itr++) {
+        if (nrec + 1 + len > cap) return -1;
+        const T dl_old = *dl_p;
+        const T el = *el_p;
+        const T pp = (dl_p[st] - dl_old) / (el + el);
+        const T rr = hypot1(pp);
+        const T psr = pp + copysign_t(rr, pp);
+        const T dl = el / psr;
+        const T dl1 = el * psr;
+        *dl_p = dl;
+        dl_p[st] = dl1;
+        const T delta = dl_old - dl;
+        for (int j = m + 1; j < n; j++) d[j * st] -= delta;  // d(l+2..m) are shifted on read
+        shift += delta;
+        T c = T(1), c2 = T(1), c3 = T(1), s = T(0), s2 = T(0);
+        T *dp = d + m * st;
+        T *ep = e + (m - 1) * st;
+        T p = (m >= l + 2) ? *dp - delta : *dp;
+        const T el1 = el_p[st];
+        T ei = T(0);
+        Rec<T> *o = out + nrec + 1;
+        for (int i = m - 1; i >= l; i--) {
+          c3 = c2;
+          c2 = c;
+          s2 = s;
+          ei = *ep;
+          const T dsi = dp[-st];
+          const T di = (i >= l + 2) ? dsi - delta : dsi;
+          const T gg = c * ei;
+          const T h = c * p;
+          T cn, sn, r;
+          givens(p, ei, cn, sn, r);
+          ep[st] = s * r;
+          p = cn * di - sn * gg;
+          *dp = h + sn * (cn * gg + sn * di);
+          c = cn;
+          s = sn;
+          Rec<T> rec;
+          rec.c = cn;
+          rec.s = sn;
+          *o++ = rec;
+          dp -= st;
+          ep -= st;
+        }
+        out[nrec] = make_hdr(m - 1, len, T(0));
+        nrec += 1 + len;
+        const T r = (-s * s2 * c3 * el1 * ei) / dl1;
+        *el_p = s * r;
+        *dl_p = c * r;
+        if (fabs_t(*el_p) <= tst1) break;
+      }
+      if (itr >= max_sweep) {
+        *ierr = l + 1;
+        return nrec;
+      }
+    }
+    *dl_p += shift;
+  }
+  return nrec;
+}
+
+template <class T>
+__host__ __device__ int ql_imtql2_fast(T *__restrict__ d, T *__restrict__ e, const int st, const int n,
+                                       Rec<T> *__restrict__ out, const int cap, const int max_sweep, int *ierr)
+{
+  const T tol = Num<T>::eps() * Num<T>::tolmul();
+  int nrec = 0;
+  *ierr = 0;
+  if (n <= 1) return 0;
+  for (int l = 0; l < n; l++) {
+    int itr;
+    for (itr = 0; itr <= max_sweep; itr++) {
+      int m = n - 1;
+      for (int mm = l; mm < n - 1; mm++) {
+        const T t1 = (fabs_t(d[mm * st]) + fabs_t(d[(mm + 1) * st])) * tol;
+        if (!(fabs_t(e[mm * st]) > t1)) {
+          m = mm;
+          break;
+        }
+      }
+      if (m == l) break;
+      if (nrec + 1 + (m - l) > cap) return -1;
+      const T dl = d[l * st], dl1 = d[(l + 1) * st], el = e[l * st];
+      const T f0 = (dl1 - dl) / (el + el);
+      const T g0 = hypot1(f0);
+      T di1 = d[m * st];
+      T r = (di1 - dl) + el / (f0 + copysign_t(g0, f0));
+      T s = T(1), c = T(1), delta = T(0);
+      Rec<T> *o = out + nrec + 1;
+      int i;
+      int cnt = 0;
+      for (i = m - 1; i >= l; i--) {
+        const T ei = e[i * st];
+        const T f = s * ei;
+        T cn, sn, rn;
+        givens(r, f, cn, sn, rn);
+        if (rn == T(0)) {
+          r = T(0);
+          break;
+        }
+        const T b = c * ei;
+        const T dix = di1 - delta;
+        di1 = d[i * st];
+        const T q = (di1 - dix) * sn + T(2) * cn * b;
+        const T dx1 = fma(sn, q, dix);
+        delta = dx1 - dix;
+        e[(i + 1) * st] = rn;
+        d[(i + 1) * st] = dx1;
+        r = cn * q - b;
+        c = cn;
+        s = sn;
+        Rec<T> rec;
+        rec.c = cn;
+        rec.s = sn;
+        *o++ = rec;
+        cnt++;
+      }
+      if (cnt > 0) {
+        out[nrec] = make_hdr(m - 1, cnt, T(0));
+        nrec += 1 + cnt;
+      }
+      const int j = (i + 1 > l) ? i + 1 : l;
+      d[j * st] -= delta;
+      e[j * st] = r;
+      e[m * st] = T(0);
+    }
+    if (itr > max_sweep) {
+      *ierr = l + 1;
+      return nrec;
+    }
+  }
+  return nrec;
+}
+
 template <class T>
 __host__ __device__ __forceinline__ int ql_run(int method, QLGen<T> &g, const DEView<T> v, const int n,
                                       Rec<T> *buf, const int cap, const int max_sweep)

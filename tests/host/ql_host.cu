@@ -42,3 +42,24 @@ extern "C" int host_ql_f(int n, float *d, float *e, int method, int max_sweep, i
 {
   return run<float>(n, d, e, method, max_sweep, cap, chunk, rec, nrec, ierr);
 }
+
+template <class T>
+static int run_fast(int n, T *d, T *e, int method, int max_sweep, int cap, T *rec_out, int *nrec_out, int *ierr)
+{
+  using namespace eigb;
+  Rec<T> *out = reinterpret_cast<Rec<T> *>(rec_out);
+  const int nr = method == QL_IMTQL2 ? ql_imtql2_fast(d, e, 1, n, out, cap, max_sweep, ierr)
+                                    : ql_tql2_fast(d, e, 1, n, out, cap, max_sweep, ierr);
+  *nrec_out = nr < 0 ? 0 : nr;
+  return nr < 0 ? 1 : 0;
+}
+extern "C" int host_ql_fast_d(int n, double *d, double *e, int method, int max_sweep, int cap, double *rec,
+                              int *nrec, int *ierr)
+{
+  return run_fast<double>(n, d, e, method, max_sweep, cap, rec, nrec, ierr);
+}
+extern "C" int host_ql_fast_f(int n, float *d, float *e, int method, int max_sweep, int cap, float *rec,
+                              int *nrec, int *ierr)
+{
+  return run_fast<float>(n, d, e, method, max_sweep, cap, rec, nrec, ierr);
+}

@@ -22,7 +22,7 @@ def hostlibs():
         pytest.skip("nvcc not available")
     td = tempfile.mkdtemp(prefix="eigb_host_")
     libs = {}
-    for name in ("ql_host", "tridiag_host"):
+    for name in ("ql_host", "tridiag_host", "apply_host"):
         out = os.path.join(td, f"lib{name}.so")
         subprocess.check_call([NVCC, "-O2", "-std=c++20", "-Xcompiler", "-fPIC", "-shared",
                                "-Wno-deprecated-gpu-targets", "-diag-suppress", "20014,20011",
@@ -33,8 +33,13 @@ def hostlibs():
         f = getattr(libs["ql_host"], "host_ql" + s)
         f.argtypes = [I, P, P, I, I, I, I, P, P, P]
         f.restype = I
+        f = getattr(libs["ql_host"], "host_ql_fast" + s)
+        f.argtypes = [I, P, P, I, I, I, P, P, P]
+        f.restype = I
         getattr(libs["tridiag_host"], "host_tridiag" + s).argtypes = [I, I, I, P, I, P, P]
         getattr(libs["tridiag_host"], "host_tridiag_reg" + s).argtypes = [I, P, I, P, P]
+        getattr(libs["apply_host"], "host_apply" + s).argtypes = [I, P, P, I, I]
+        getattr(libs["apply_host"], "host_apply" + s).restype = I
     return libs
 
 
@@ -184,3 +189,53 @@ def test_tridiag_register_variant(oracle_mod, hostlibs, n, nm, dtype):
     do, eo = tred(O, a0, n)
     To = np.diag(do.astype(np.float64)) + np.diag(eo[:-1].astype(np.float64), 1) + np.diag(eo[:-1].astype(np.float64), -1)
     assert np.abs(np.linalg.eigvalsh(T) - np.linalg.eigvalsh(To)).max() <= 64 * eps * scale
+
+
+@pytest.mark.parametrize("n", [2, 5, 16, 33, 64])
+@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_fast_generator_is_bit_identical(oracle_mod, hostlibs, n, method, dtype):
+    """Phase 2's single-call generator emits exactly the records and
+    eigenvalues of the resumable generator used by the fallback path."""
+    O = oracle_mod
+    a0 = O.sym_uniform(1, n, seed=3 * n)[0].astype(dtype)
+    d, e = tred(O, a0, n)
+    cap = 2 * n * n + 4 * n + 32
+    _, d1, r1, i1 = host_ql(hostlibs, d, e, method, cap)
+    d2, e2 = d.copy(), e.copy()
+    rec = np.zeros(2 * cap, dtype)
+    nrec = np.zeros(1, np.int32)
+    ierr = np.zeros(1, np.int32)
+    f = hostlibs["ql_host"].host_ql_fast_d if dtype == np.float64 else hostlibs["ql_host"].host_ql_fast_f
+    assert f(n, _p(d2), _p(e2), method, 100, cap, _p(rec), _p(nrec), _p(ierr)) == 0
+    assert int(ierr[0]) == i1
+    assert np.array_equal(d2, d1)
+    assert np.array_equal(rec[: 2 * int(nrec[0])].reshape(-1, 2).view(np.uint8), r1.view(np.uint8))
+    # too small a capacity is reported, not truncated
+    assert f(n, _p(d.copy()), _p(e.copy()), method, 100, 3, _p(rec), _p(nrec), _p(ierr)) == (1 if n > 2 else 0) or n <= 2
+
+
+@pytest.mark.parametrize("n", [3, 8, 17, 33, 64, 100])
+@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_wavefront_apply_matches_sequential(oracle_mod, hostlibs, n, method, dtype):
+    """Phase 3 applies groups of sweeps as a skewed pipeline (identity
+    outside each sweep's range); the result equals applying every rotation
+    in order, also when the stream is staged in small chunks."""
+    O = oracle_mod
+    a0 = O.sym_uniform(1, n, seed=7 * n + method)[0].astype(dtype)
+    d, e = tred(O, a0, n)
+    cap = 2 * n * n + 4 * n + 32
+    st, dq, rec, ierr = host_ql(hostlibs, d, e, method, cap)
+    assert st == 0
+    rng = np.random.default_rng(n)
+    q0 = rng.standard_normal((n, n)).astype(dtype)     # any start matrix, row-major
+    ref = q0.astype(np.float64) @ apply_records(rec, n, dtype)
+    f = hostlibs["apply_host"].host_apply_d if dtype == np.float64 else hostlibs["apply_host"].host_apply_f
+    flat = np.ascontiguousarray(rec)
+    eps = np.finfo(dtype).eps
+    for ch in (4 * (n + 1), n + 1, 10 ** 6):
+        z = np.ascontiguousarray(q0.copy())
+        groups = f(n, _p(z), _p(flat), flat.shape[0], ch)
+        assert groups > 0
+        assert np.abs(z - ref).max() <= 64 * n * eps * np.abs(ref).max()
