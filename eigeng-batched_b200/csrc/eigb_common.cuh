@@ -51,6 +51,26 @@ __host__ __device__ __forceinline__ float fmax_t(float x, float y) { return fmax
 __host__ __device__ __forceinline__ double copysign_t(double x, double y) { return copysign(x, y); }
 __host__ __device__ __forceinline__ float copysign_t(float x, float y) { return copysignf(x, y); }
 
+// Products that must not be fused into a neighbouring addition: the QL
+// recurrences are written with explicit fma() and these, so that every copy
+// of a recurrence rounds identically whatever the compiler's contraction.
+__host__ __device__ __forceinline__ double mul_rn(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+__host__ __device__ __forceinline__ float mul_rn(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+  return __fmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+
 // Zero guard used wherever the reference divides by a possibly vanishing
 // product (misc_gpu.hpp:474-509 flip0to1).
 template <class T> __host__ __device__ __forceinline__ T flip0to1(T x) { return x == T(0) ? T(1) : x; }
@@ -63,7 +83,7 @@ template <class T> __host__ __device__ __forceinline__ T flip0to1(T x) { return 
 template <class T>
 __host__ __device__ __forceinline__ void givens(T a, T b, T &c, T &s, T &r)
 {
-  const T sig = fma(a, a, b * b);
+  const T sig = fma(a, a, mul_rn(b, b));
   if (sig > T(0)) {
     const T y = rsq(sig);
     c = a * y;

@@ -388,58 +388,103 @@ template <class T> __host__ __device__ inline size_t k3c_smem_bytes(int n, bool 
 // whose column c is zr[c*cs].  Sweep s runs one column behind sweep s-1 as
 // stage s of a pipeline: at step j0 stage s handles column j0+s, taking the
 // column value just produced by stage s-1; outside its range a stage is an
-// identity rotation, i.e. a one-column delay.  The loop is skewed so that
-// the stages of one iteration are independent (stage s works on step
-// tau-s); every column is loaded once (stage 0) and stored once (last stage).
+// identity rotation, i.e. a one-column delay.  The loop is skewed: in
+// iteration tau stage s works on step tau-s, so the stages of an iteration
+// are independent (four rotation chains in flight per row).  Every column
+// is loaded once (stage 0) and stored once (last stage).  Iterations in
+// which every stage rotates run without any range check.
+#define EIGB_WSTAGE(S, IN)                                                     \
+  if (S < ns && tau >= S && tau - S < nsteps) {                              \
+    const T in_ = (IN);                                                      \
+    if (tau >= rs##S && tau <= re##S) {                                      \
+      const Rec<T> rr = rb[ro##S + (tau - rs##S)];                           \
+      y##S = fma(rr.c, h##S, rr.s * in_);                                    \
+      h##S = fma(-rr.s, h##S, rr.c * in_);                                   \
+    } else {                                                                 \
+      y##S = h##S;                                                           \
+      h##S = in_;                                                            \
+    }                                                                        \
+    if (S == ns - 1) {                                                       \
+      const int oc = jt - (tau - S) + ns;                                    \
+      if (oc >= 0 && oc < n) zr[oc * cs] = y##S;                             \
+    }                                                                        \
+  }
+
 template <class T, int CS>
 __host__ __device__ __forceinline__ void wave_apply(T *__restrict__ zr, const int cs_rt, const int n,
-                                           const Rec<T> *__restrict__ rb, const int (&i0)[K3_WAVE],
-                                           const int (&len)[K3_WAVE], const int (&off)[K3_WAVE], const int ns)
+                                                    const Rec<T> *__restrict__ rb, const int (&i0)[K3_WAVE],
+                                                    const int (&len)[K3_WAVE], const int (&off)[K3_WAVE],
+                                                    const int ns)
 {
+  static_assert(K3_WAVE == 4, "four stages are spelled out below");
   const int cs = CS > 0 ? CS : cs_rt;
-  int jt = -0x3fffffff, jb = 0x3fffffff;
-#pragma unroll
-  for (int s = 0; s < K3_WAVE; s++)
-    if (s < ns) {
-      jt = max(jt, i0[s] - s);
-      jb = min(jb, i0[s] - len[s] + 1 - s);
-    }
+  int jt = i0[0], jb = i0[0] - len[0] + 1;
+  if (ns > 1) { jt = max(jt, i0[1] - 1); jb = min(jb, i0[1] - len[1] + 1 - 1); }
+  if (ns > 2) { jt = max(jt, i0[2] - 2); jb = min(jb, i0[2] - len[2] + 1 - 2); }
+  if (ns > 3) { jt = max(jt, i0[3] - 3); jb = min(jb, i0[3] - len[3] + 1 - 3); }
   const int nsteps = jt - (jb - ns) + 1;
-  T h1[K3_WAVE], x[K3_WAVE];
-#pragma unroll
-  for (int s = 0; s < K3_WAVE; s++) {
-    const int col = jt + s + 1;
-    h1[s] = (s < ns && col < n) ? zr[col * cs] : T(0);
-    x[s] = T(0);
+  // stage s rotates in iterations [rs, re]; its records start at rb[ro]
+  const int rs0 = 0 + jt + 0 - i0[0], re0 = rs0 + len[0] - 1, ro0 = off[0];
+  const int rs1 = 1 + jt + 1 - i0[1], re1 = rs1 + len[1] - 1, ro1 = off[1];
+  const int rs2 = 2 + jt + 2 - i0[2], re2 = rs2 + len[2] - 1, ro2 = off[2];
+  const int rs3 = 3 + jt + 3 - i0[3], re3 = rs3 + len[3] - 1, ro3 = off[3];
+  T h0 = (jt + 1 < n) ? zr[(jt + 1) * cs] : T(0);
+  T h1 = (ns > 1 && jt + 2 < n) ? zr[(jt + 2) * cs] : T(0);
+  T h2 = (ns > 2 && jt + 3 < n) ? zr[(jt + 3) * cs] : T(0);
+  T h3 = (ns > 3 && jt + 4 < n) ? zr[(jt + 4) * cs] : T(0);
+  T x0 = T(0), x1 = T(0), x2 = T(0);
+  const int total = nsteps + ns - 1;
+  // steady range: all four stages rotating
+  int slo = total, shi = -1;
+  if (ns == 4) {
+    slo = max(max(rs0, rs1), max(rs2, rs3));
+    shi = min(min(re0, re1), min(re2, re3));
   }
-  for (int tau = 0; tau < nsteps + ns - 1; tau++) {
-    T y[K3_WAVE];
-#pragma unroll
-    for (int s = 0; s < K3_WAVE; s++) {
-      y[s] = T(0);
-      const int step = tau - s;
-      if (s < ns && step >= 0 && step < nsteps) {
-        const int j0 = jt - step;
-        const int col = j0 + s;
-        const T in = (s == 0) ? ((j0 >= 0) ? zr[j0 * cs] : T(0)) : x[s > 0 ? s - 1 : 0];
-        if (col <= i0[s] && col > i0[s] - len[s]) {
-          const Rec<T> rr = rb[off[s] + (i0[s] - col)];
-          y[s] = fma(rr.c, h1[s], rr.s * in);
-          h1[s] = fma(-rr.s, h1[s], rr.c * in);
-        } else {
-          y[s] = h1[s];
-          h1[s] = in;
-        }
-        if (s == ns - 1) {
-          const int oc = j0 + ns;
-          if (oc >= 0 && oc < n) zr[oc * cs] = y[s];
-        }
+  int tau = 0;
+  for (int phase = 0; phase < 2; phase++) {
+    // general iterations (range checks) up to the steady range, then after it
+    const int tend = (phase == 0 && slo <= shi) ? slo : total;
+    for (; tau < tend; tau++) {
+      T y0 = T(0), y1 = T(0), y2 = T(0), y3 = T(0);
+      EIGB_WSTAGE(0, (jt - tau >= 0) ? zr[(jt - tau) * cs] : T(0))
+      EIGB_WSTAGE(1, x0)
+      EIGB_WSTAGE(2, x1)
+      EIGB_WSTAGE(3, x2)
+      x0 = y0;
+      x1 = y1;
+      x2 = y2;
+    }
+    if (phase == 0 && slo <= shi) {
+      // steady state: no checks; stage 0 loads column jt-tau, stage 3
+      // stores column jt-tau+7 (= jt-(tau-3)+4), records advance by one
+      const Rec<T> *p0 = rb + ro0 + (tau - rs0);
+      const Rec<T> *p1 = rb + ro1 + (tau - rs1);
+      const Rec<T> *p2 = rb + ro2 + (tau - rs2);
+      const Rec<T> *p3 = rb + ro3 + (tau - rs3);
+      T *zin = zr + (jt - tau) * cs;
+      T *zout = zr + (jt - tau + 7) * cs;
+      for (; tau <= shi; tau++) {
+        const T in0 = *zin;
+        const Rec<T> r0 = *p0++, r1 = *p1++, r2 = *p2++, r3 = *p3++;
+        const T y0 = fma(r0.c, h0, r0.s * in0);
+        h0 = fma(-r0.s, h0, r0.c * in0);
+        const T y1 = fma(r1.c, h1, r1.s * x0);
+        h1 = fma(-r1.s, h1, r1.c * x0);
+        const T y2 = fma(r2.c, h2, r2.s * x1);
+        h2 = fma(-r2.s, h2, r2.c * x1);
+        const T y3 = fma(r3.c, h3, r3.s * x2);
+        h3 = fma(-r3.s, h3, r3.c * x2);
+        *zout = y3;  // stage 3 rotates a column <= n-2 here, so the output column is < n
+        x0 = y0;
+        x1 = y1;
+        x2 = y2;
+        zin -= cs;
+        zout -= cs;
       }
     }
-#pragma unroll
-    for (int s = 0; s < K3_WAVE; s++) x[s] = y[s];
   }
 }
+#undef EIGB_WSTAGE
 
 // Reads up to K3_WAVE complete segments (header + rotations) from
 // rbuf[q..cnt); advances q past them; returns how many were read.
@@ -466,6 +511,27 @@ __host__ __device__ __forceinline__ int parse_group(const Rec<T> *rbuf, const in
     }
   }
   return ns;
+}
+
+// Applies the complete segments of rbuf[0..cnt) in groups of K3_WAVE to the
+// rows this thread owns; returns the index of the first incomplete segment.
+template <class T, bool SM, int RPT>
+__device__ __forceinline__ int apply_chunk(const Rec<T> *rbuf, const int cnt, const int n, const int cs,
+                                           const bool (&own)[RPT], T *const (&zr)[RPT])
+{
+  int q = 0;
+  while (true) {
+    int i0[K3_WAVE], len[K3_WAVE], off[K3_WAVE];
+    const int ns = parse_group(rbuf, cnt, q, i0, len, off);
+    if (ns == 0) break;
+#pragma unroll
+    for (int j = 0; j < RPT; j++)
+      if (own[j]) {
+        if (SM) wave_apply<T, 1>(zr[j], 1, n, rbuf, i0, len, off, ns);
+        else wave_apply<T, 0>(zr[j], cs, n, rbuf, i0, len, off, ns);
+      }
+  }
+  return q;
 }
 
 // Z layout: in shared memory row-major, Z(r, c) at Z[r*(n|1) + c] (each
@@ -515,23 +581,6 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
     own[j] = t + j * nt < n;
     zr[j] = Z + (own[j] ? t + j * nt : 0) * rs;
   }
-  // applies the complete segments of rbuf[0..cnt) in groups of K3_WAVE;
-  // returns the index of the first incomplete segment
-  auto apply_chunk = [&](const int cnt) {
-    int q = 0;
-    while (true) {
-      int i0[K3_WAVE], len[K3_WAVE], off[K3_WAVE];
-      const int ns = parse_group(rbuf, cnt, q, i0, len, off);
-      if (ns == 0) break;
-#pragma unroll
-      for (int j = 0; j < RPT; j++)
-        if (own[j]) {
-          if (SM) wave_apply<T, 1>(zr[j], 1, n, rbuf, i0, len, off, ns);
-          else wave_apply<T, 0>(zr[j], cs, n, rbuf, i0, len, off, ns);
-        }
-    }
-    return q;
-  };
   if (!mt.overflow) {
     const Rec<T> *src = p.rec + (size_t)k * p.rcap;
     int base = 0;
@@ -539,7 +588,7 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
       const int cnt = min(ch, mt.nrec - base);
       for (int q = t; q < cnt; q += nt) rbuf[q] = src[base + q];
       __syncthreads();
-      const int used = apply_chunk(cnt);
+      const int used = apply_chunk<T, SM, RPT>(rbuf, cnt, n, cs, own, zr);
       __syncthreads();
       base += used > 0 ? used : cnt;  // a segment is at most n records: used > 0
     }
@@ -564,7 +613,7 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
       __syncthreads();
       const int nr = sflag[0];
       const int done = sflag[1];
-      apply_chunk(nr);
+      apply_chunk<T, SM, RPT>(rbuf, nr, n, cs, own, zr);
       __syncthreads();
       if (done) break;
     }

@@ -39,6 +39,69 @@ template <class T> struct DEView {
   __host__ __device__ __forceinline__ T &E(int i) const { return e[i * st]; }
 };
 
+// One tql2 chase step at index i (tql2_tiled.hpp:94-115): from the
+// previous (c, s, p) and (e_i, d_i) to the new rotation (cn, sn), the new p
+// and the values stored at i+1.  Shared by both generators.
+template <class T>
+__host__ __device__ __forceinline__ void tql2_step(const T c, const T s, const T p, const T ei, const T di, T &cn,
+                                                   T &sn, T &pn, T &ei1, T &di1)
+{
+  const T gg = mul_rn(c, ei);
+  const T h = mul_rn(c, p);
+  T r;
+  givens(p, ei, cn, sn, r);
+  ei1 = mul_rn(s, r);
+  pn = fma(cn, di, -mul_rn(sn, gg));
+  di1 = fma(sn, fma(cn, gg, mul_rn(sn, di)), h);
+}
+
+// Explicit shift of tql2 (tql2_tiled.hpp:64-75): new d(l), d(l+1).
+template <class T>
+__host__ __device__ __forceinline__ void tql2_shift(const T dl_old, const T dl1_old, const T el, T &dl, T &dl1)
+{
+  const T p = (dl1_old - dl_old) / (el + el);
+  const T r = hypot1(p);
+  const T psr = p + copysign_t(r, p);
+  dl = el / psr;
+  dl1 = mul_rn(el, psr);
+}
+
+// End of a tql2 sweep (tql2_tiled.hpp:126-130): new e(l), d(l).
+template <class T>
+__host__ __device__ __forceinline__ void tql2_close(const T c, const T s, const T s2, const T c3, const T el1,
+                                                    const T ei, const T dl1, T &el, T &dl)
+{
+  const T r = mul_rn(mul_rn(mul_rn(mul_rn(-s, s2), c3), el1), ei) / dl1;
+  el = mul_rn(s, r);
+  dl = mul_rn(c, r);
+}
+
+// One imtql2 chase step (imtql2_tiled.hpp:86-115) after the rotation
+// (cn, sn) has been formed: returns the new d(i+1) and updates di1, delta,
+// r.
+template <class T>
+__host__ __device__ __forceinline__ T imtql2_step(const T cn, const T sn, const T c_old, const T ei, const T di,
+                                                  T &di1, T &delta, T &r)
+{
+  const T b = mul_rn(c_old, ei);
+  const T dix = di1 - delta;
+  di1 = di;
+  const T q = fma(di - dix, sn, mul_rn(T(2) * cn, b));
+  const T dx1 = fma(sn, q, dix);
+  delta = dx1 - dix;
+  r = fma(cn, q, -b);
+  return dx1;
+}
+
+// Wilkinson-type shift of imtql2 (imtql2_tiled.hpp:67-75).
+template <class T>
+__host__ __device__ __forceinline__ T imtql2_shift(const T dl, const T dl1, const T el, const T dm)
+{
+  const T f = (dl1 - dl) / (el + el);
+  const T g = hypot1(f);
+  return (dm - dl) + el / (f + copysign_t(g, f));
+}
+
 template <class T>
 __host__ __device__ __forceinline__ void ql_close_seg(QLGen<T> &g, Rec<T> *buf)
 {
@@ -81,12 +144,8 @@ __host__ __device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec
         {  // explicit shift, tql2_tiled.hpp:64-80
           const int l = g.l;
           const T dl_old = v.D(l);
-          const T el = v.E(l);
-          const T p = (v.D(l + 1) - dl_old) / (el + el);
-          const T r = hypot1(p);
-          const T psr = p + copysign_t(r, p);
-          const T dl = el / psr;
-          g.dl1 = el * psr;
+          T dl;
+          tql2_shift(dl_old, v.D(l + 1), v.E(l), dl, g.dl1);
           v.D(l) = dl;
           v.D(l + 1) = g.dl1;
           g.delta = dl_old - dl;
@@ -120,13 +179,9 @@ __host__ __device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec
             g.s2 = g.s;
             const T ei = v.E(i);
             const T di = (i >= g.l + 2) ? v.D(i) - g.delta : v.D(i);
-            const T gg = g.c * ei;
-            const T h = g.c * g.p;
-            T c, s, r;
-            givens(g.p, ei, c, s, r);
-            const T ei1 = g.s * r;
-            g.p = c * di - s * gg;
-            const T di1 = h + s * (c * gg + s * di);
+            T c, s, pn, ei1, di1;
+            tql2_step(g.c, g.s, g.p, ei, di, c, s, pn, ei1, di1);
+            g.p = pn;
             v.E(i + 1) = ei1;
             v.D(i + 1) = di1;
             g.c = c;
@@ -141,9 +196,10 @@ __host__ __device__ int ql_tql2(QLGen<T> &g, const DEView<T> v, const int n, Rec
         }
         ql_close_seg(g, buf);
         {  // tql2_tiled.hpp:126-135
-          const T r = (-g.s * g.s2 * g.c3 * g.el1 * g.ei) / g.dl1;
-          v.E(g.l) = g.s * r;
-          v.D(g.l) = g.c * r;
+          T el, dl;
+          tql2_close(g.c, g.s, g.s2, g.c3, g.el1, g.ei, g.dl1, el, dl);
+          v.E(g.l) = el;
+          v.D(g.l) = dl;
         }
         if (fabs_t(v.E(g.l)) <= g.tst1) break;
       }
@@ -186,13 +242,9 @@ __host__ __device__ int ql_imtql2(QLGen<T> &g, const DEView<T> v, const int n, R
         g.m = m;
       }
       if (g.m == g.l) break;
-      {  // Wilkinson-type shift, imtql2_tiled.hpp:67-75
-        const T dl = v.D(g.l), dl1 = v.D(g.l + 1), el = v.E(g.l);
-        const T f = (dl1 - dl) / (el + el);
-        const T gg = hypot1(f);
-        g.di1 = v.D(g.m);
-        g.r = (g.di1 - dl) + el / (f + copysign_t(gg, f));
-      }
+      // Wilkinson-type shift, imtql2_tiled.hpp:67-75
+      g.di1 = v.D(g.m);
+      g.r = imtql2_shift(v.D(g.l), v.D(g.l + 1), v.E(g.l), g.di1);
       g.s = T(1);
       g.c = T(1);
       g.delta = T(0);
@@ -206,7 +258,7 @@ __host__ __device__ int ql_imtql2(QLGen<T> &g, const DEView<T> v, const int n, R
         {  // imtql2_tiled.hpp:86-115
           const int i = g.i;
           const T ei = v.E(i);
-          const T f = g.s * ei;
+          const T f = mul_rn(g.s, ei);
           T c, s, r;
           givens(g.r, f, c, s, r);
           if (r == T(0)) {
@@ -218,15 +270,9 @@ __host__ __device__ int ql_imtql2(QLGen<T> &g, const DEView<T> v, const int n, R
             g.seg_cnt = 0;
             g.seg_i0 = i;
           }
-          const T b = g.c * ei;
-          const T dix = g.di1 - g.delta;
-          g.di1 = v.D(i);
-          const T q = (g.di1 - dix) * s + T(2) * c * b;
-          const T dx1 = fma(s, q, dix);
-          g.delta = dx1 - dix;
+          const T dx1 = imtql2_step(c, s, g.c, ei, v.D(i), g.di1, g.delta, g.r);
           v.E(i + 1) = r;
           v.D(i + 1) = dx1;
-          g.r = c * q - b;
           g.c = c;
           g.s = s;
           Rec<T> rec;
@@ -293,12 +339,8 @@ __host__ __device__ int ql_tql2_fast(T *__restrict__ d, T *__restrict__ e, const
       for (itr = 0; itr < max_sweep; itr++) {
         if (nrec + 1 + len > cap) return -1;
         const T dl_old = *dl_p;
-        const T el = *el_p;
-        const T pp = (dl_p[st] - dl_old) / (el + el);
-        const T rr = hypot1(pp);
-        const T psr = pp + copysign_t(rr, pp);
-        const T dl = el / psr;
-        const T dl1 = el * psr;
+        T dl, dl1;
+        tql2_shift(dl_old, dl_p[st], *el_p, dl, dl1);
         *dl_p = dl;
         dl_p[st] = dl1;
         const T delta = dl_old - dl;
@@ -318,13 +360,11 @@ __host__ __device__ int ql_tql2_fast(T *__restrict__ d, T *__restrict__ e, const
           ei = *ep;
           const T dsi = dp[-st];
           const T di = (i >= l + 2) ? dsi - delta : dsi;
-          const T gg = c * ei;
-          const T h = c * p;
-          T cn, sn, r;
-          givens(p, ei, cn, sn, r);
-          ep[st] = s * r;
-          p = cn * di - sn * gg;
-          *dp = h + sn * (cn * gg + sn * di);
+          T cn, sn, pn, ei1, di1;
+          tql2_step(c, s, p, ei, di, cn, sn, pn, ei1, di1);
+          ep[st] = ei1;
+          p = pn;
+          *dp = di1;
           c = cn;
           s = sn;
           Rec<T> rec;
@@ -336,9 +376,10 @@ __host__ __device__ int ql_tql2_fast(T *__restrict__ d, T *__restrict__ e, const
         }
         out[nrec] = make_hdr(m - 1, len, T(0));
         nrec += 1 + len;
-        const T r = (-s * s2 * c3 * el1 * ei) / dl1;
-        *el_p = s * r;
-        *dl_p = c * r;
+        T eln, dln;
+        tql2_close(c, s, s2, c3, el1, ei, dl1, eln, dln);
+        *el_p = eln;
+        *dl_p = dln;
         if (fabs_t(*el_p) <= tst1) break;
       }
       if (itr >= max_sweep) {
@@ -372,33 +413,24 @@ __host__ __device__ int ql_imtql2_fast(T *__restrict__ d, T *__restrict__ e, con
       }
       if (m == l) break;
       if (nrec + 1 + (m - l) > cap) return -1;
-      const T dl = d[l * st], dl1 = d[(l + 1) * st], el = e[l * st];
-      const T f0 = (dl1 - dl) / (el + el);
-      const T g0 = hypot1(f0);
       T di1 = d[m * st];
-      T r = (di1 - dl) + el / (f0 + copysign_t(g0, f0));
+      T r = imtql2_shift(d[l * st], d[(l + 1) * st], e[l * st], di1);
       T s = T(1), c = T(1), delta = T(0);
       Rec<T> *o = out + nrec + 1;
       int i;
       int cnt = 0;
       for (i = m - 1; i >= l; i--) {
         const T ei = e[i * st];
-        const T f = s * ei;
+        const T f = mul_rn(s, ei);
         T cn, sn, rn;
         givens(r, f, cn, sn, rn);
         if (rn == T(0)) {
           r = T(0);
           break;
         }
-        const T b = c * ei;
-        const T dix = di1 - delta;
-        di1 = d[i * st];
-        const T q = (di1 - dix) * sn + T(2) * cn * b;
-        const T dx1 = fma(sn, q, dix);
-        delta = dx1 - dix;
+        const T dx1 = imtql2_step(cn, sn, c, ei, d[i * st], di1, delta, r);
         e[(i + 1) * st] = rn;
         d[(i + 1) * st] = dx1;
-        r = cn * q - b;
         c = cn;
         s = sn;
         Rec<T> rec;

@@ -10,6 +10,9 @@
 // vector p, the per-block partial sums and the team reductions.  A step
 // touches only the blocks that intersect the active leading i x i part.
 #pragma once
+#include <stdint.h>
+#include <stdlib.h>
+
 #include "eigb_common.cuh"
 
 namespace eigb {
@@ -25,6 +28,26 @@ __host__ __device__ __forceinline__ T get32(const T (&v)[32], const int i)
   return r;
 }
 
+// Two consecutive values from 2-element-aligned shared memory in one load.
+template <class T> struct Pair;
+template <> struct Pair<double> {
+  using V = double2;
+};
+template <> struct Pair<float> {
+  using V = float2;
+};
+template <class T>
+__host__ __device__ __forceinline__ void ld2(const T *p, T &a, T &b)
+{
+#ifndef __CUDA_ARCH__
+  // host builds (unit tests) check the alignment that the device load needs
+  if (reinterpret_cast<uintptr_t>(p) % sizeof(typename Pair<T>::V) != 0) abort();
+#endif
+  const typename Pair<T>::V v = *reinterpret_cast<const typename Pair<T>::V *>(p);
+  a = v.x;
+  b = v.y;
+}
+
 template <int NB> struct RegLayout {
   static constexpr int NR = 32 * NB;
   static constexpr int NT = NR * NB;
@@ -32,11 +55,18 @@ template <int NB> struct RegLayout {
 
 // Shared-memory elements of tridiag_qt_reg: V (max(n*NR, n*(n|1)), also the
 // staging area of the input), part[2*NB*NR], pv[NR], beta[NR], red[72].
-template <int NB> __host__ __device__ inline size_t reg_smem_elems(int n)
+// Offset of the arrays after V, rounded to 4 elements so that the paired
+// loads of V and pv stay aligned for every n.
+template <int NB> __host__ __device__ inline size_t reg_voff(int n)
 {
   constexpr int NR = RegLayout<NB>::NR;
   const size_t v = (size_t)n * NR > (size_t)n * (n | 1) ? (size_t)n * NR : (size_t)n * (n | 1);
-  return v + 2 * (size_t)NB * NR + 2 * (size_t)NR + 72;
+  return (v + 3) & ~(size_t)3;
+}
+template <int NB> __host__ __device__ inline size_t reg_smem_elems(int n)
+{
+  constexpr int NR = RegLayout<NB>::NR;
+  return reg_voff<NB>(n) + 2 * (size_t)NB * NR + 2 * (size_t)NR + 72;
 }
 
 // A: the input matrix (upper triangle used), overwritten with M = Q^T.
@@ -50,9 +80,8 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   const int r = 32 * rb + lane;
   const int c0 = 32 * cb;
   const int lds = n | 1;
-  size_t voff = (size_t)n * NR > (size_t)n * lds ? (size_t)n * NR : (size_t)n * lds;
   T *V = sm;
-  T *part = sm + voff;
+  T *part = sm + reg_voff<NB>(n);
   T *pv = part + 2 * NB * NR;
   T *beta_s = pv + NR;
   T *red = beta_s + NR;
@@ -98,10 +127,13 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
       T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
 #pragma unroll
       for (int c = 0; c < 32; c += 4) {
-        const T v0 = (c + 0 == cp) ? ul : Vi[c0 + c + 0];
-        const T v1 = (c + 1 == cp) ? ul : Vi[c0 + c + 1];
-        const T v2 = (c + 2 == cp) ? ul : Vi[c0 + c + 2];
-        const T v3 = (c + 3 == cp) ? ul : Vi[c0 + c + 3];
+        T v0, v1, v2, v3;
+        ld2(Vi + c0 + c, v0, v1);
+        ld2(Vi + c0 + c + 2, v2, v3);
+        v0 = (c + 0 == cp) ? ul : v0;
+        v1 = (c + 1 == cp) ? ul : v1;
+        v2 = (c + 2 == cp) ? ul : v2;
+        v3 = (c + 3 == cp) ? ul : v3;
         a0 = fma(S[c + 0], v0, a0);
         a1 = fma(S[c + 1], v1, a1);
         a2 = fma(S[c + 2], v2, a2);
@@ -121,13 +153,17 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
     if (cb == 0) pv[r] = pr;  // 0 for r >= i
     const T ur = Vi[r];       // u_r with the pivot in place, 0 for r >= i
     const T alpha = tm.sum(cb == 0 ? pr * ur : T(0), red) * (beta * T(0.5));
-    if (act) {  // A += u w^T + w u^T on this block
-      const T wr = fma(alpha, ur, pr);
+    if (act) {
+      // A += u w^T + w u^T with w = p + alpha u, i.e.
+      // a_rk += u_k (p_r + 2 alpha u_r) + p_k u_r
+      const T w2r = fma(alpha + alpha, ur, pr);
 #pragma unroll
-      for (int c = 0; c < 32; c++) {
-        const T uk = Vi[c0 + c];
-        const T wk = fma(alpha, uk, pv[c0 + c]);
-        S[c] = fma(wk, ur, fma(uk, wr, S[c]));
+      for (int c = 0; c < 32; c += 2) {
+        T u0, u1, p0, p1;
+        ld2(Vi + c0 + c, u0, u1);
+        ld2(pv + c0 + c, p0, p1);
+        S[c] = fma(p0, ur, fma(u0, w2r, S[c]));
+        S[c + 1] = fma(p1, ur, fma(u1, w2r, S[c + 1]));
       }
     }
     // the barrier in the next step's first sum() orders pv/part reuse
@@ -149,10 +185,13 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
       T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
 #pragma unroll
       for (int c = 0; c < 32; c += 4) {
-        a0 = fma(Mr[c + 0], Vk[c0 + c + 0], a0);
-        a1 = fma(Mr[c + 1], Vk[c0 + c + 1], a1);
-        a2 = fma(Mr[c + 2], Vk[c0 + c + 2], a2);
-        a3 = fma(Mr[c + 3], Vk[c0 + c + 3], a3);
+        T v0, v1, v2, v3;
+        ld2(Vk + c0 + c, v0, v1);
+        ld2(Vk + c0 + c + 2, v2, v3);
+        a0 = fma(Mr[c + 0], v0, a0);
+        a1 = fma(Mr[c + 1], v1, a1);
+        a2 = fma(Mr[c + 2], v2, a2);
+        a3 = fma(Mr[c + 3], v3, a3);
       }
       pb[cb * NR + r] = (a0 + a1) + (a2 + a3);
     }
@@ -165,7 +204,12 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
         if (s < nact) q += pb[s * NR + r];
       q *= bk;
 #pragma unroll
-      for (int c = 0; c < 32; c++) Mr[c] = fma(q, Vk[c0 + c], Mr[c]);
+      for (int c = 0; c < 32; c += 2) {
+        T v0, v1;
+        ld2(Vk + c0 + c, v0, v1);
+        Mr[c] = fma(q, v0, Mr[c]);
+        Mr[c + 1] = fma(q, v1, Mr[c + 1]);
+      }
     }
   }
   if (r < n) {

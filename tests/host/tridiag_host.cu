@@ -67,12 +67,13 @@ template <class T, int NB> static void run_reg(int n, T *A, int nm, T *d, T *e)
 {
   const int nthr = 32 * NB * NB;
   HostShared<T> sh(nthr);
-  std::vector<T> smem(eigb::reg_smem_elems<NB>(n));
+  std::vector<double2> smem_store((eigb::reg_smem_elems<NB>(n) * sizeof(T) + 15) / 16);
+  T *smem_p = reinterpret_cast<T *>(smem_store.data());
   std::vector<std::thread> th;
   for (int t = 0; t < nthr; t++)
     th.emplace_back([&, t]() {
       HostTeam<T> tm{t, nthr, 0, &sh};
-      eigb::tridiag_qt_reg<T, NB>(tm, A, nm, n, d, e, smem.data());
+      eigb::tridiag_qt_reg<T, NB>(tm, A, nm, n, d, e, smem_p);
     });
   for (auto &x : th) x.join();
 }
