@@ -463,9 +463,11 @@ __host__ __device__ __forceinline__ void wave_apply(T *__restrict__ zr, const in
       const Rec<T> *p3 = rb + ro3 + (tau - rs3);
       T *zin = zr + (jt - tau) * cs;
       T *zout = zr + (jt - tau + 7) * cs;
+      // operands of the next iteration are loaded before this iteration's
+      // store (they never alias: input column jt-tau-1, output jt-tau+7)
+      T in0 = *zin;
+      Rec<T> r0 = *p0, r1 = *p1, r2 = *p2, r3 = *p3;
       for (; tau <= shi; tau++) {
-        const T in0 = *zin;
-        const Rec<T> r0 = *p0++, r1 = *p1++, r2 = *p2++, r3 = *p3++;
         const T y0 = fma(r0.c, h0, r0.s * in0);
         h0 = fma(-r0.s, h0, r0.c * in0);
         const T y1 = fma(r1.c, h1, r1.s * x0);
@@ -474,12 +476,19 @@ __host__ __device__ __forceinline__ void wave_apply(T *__restrict__ zr, const in
         h2 = fma(-r2.s, h2, r2.c * x1);
         const T y3 = fma(r3.c, h3, r3.s * x2);
         h3 = fma(-r3.s, h3, r3.c * x2);
+        if (tau < shi) {
+          zin -= cs;
+          in0 = *zin;
+          r0 = *++p0;
+          r1 = *++p1;
+          r2 = *++p2;
+          r3 = *++p3;
+        }
         *zout = y3;  // stage 3 rotates a column <= n-2 here, so the output column is < n
+        zout -= cs;
         x0 = y0;
         x1 = y1;
         x2 = y2;
-        zin -= cs;
-        zout -= cs;
       }
     }
   }

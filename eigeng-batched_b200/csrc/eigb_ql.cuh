@@ -353,12 +353,19 @@ __host__ __device__ int ql_tql2_fast(T *__restrict__ d, T *__restrict__ e, const
         const T el1 = el_p[st];
         T ei = T(0);
         Rec<T> *o = out + nrec + 1;
+        // e(i), d(i) of the next step are loaded before this step's stores
+        // of e(i+1), d(i+1) (distinct addresses)
+        T ei_n = *ep, dsi_n = dp[-st];
         for (int i = m - 1; i >= l; i--) {
           c3 = c2;
           c2 = c;
           s2 = s;
-          ei = *ep;
-          const T dsi = dp[-st];
+          ei = ei_n;
+          const T dsi = dsi_n;
+          if (i > l) {
+            ei_n = ep[-st];
+            dsi_n = dp[-2 * st];
+          }
           const T di = (i >= l + 2) ? dsi - delta : dsi;
           T cn, sn, pn, ei1, di1;
           tql2_step(c, s, p, ei, di, cn, sn, pn, ei1, di1);
