@@ -344,6 +344,65 @@ void dropin(const int L, const int nm, const int n, const int m, T *a, T *w, T *
   run<T>(L, nm, n, m, a, w, wk, 0, nullptr, nullptr, stream);
 }
 
+// ---- solve without any allocation: workspace in a static device array ----
+//
+// Callers that may not allocate device memory (a plugin's enqueue that runs
+// under a framework-owned allocator, real-time loops that forbid
+// allocation) can still solve through
+// eigen_GPU_batch_noalloc_DP.  Its workspace is this file-scope array: every
+// GPU that loads the library holds it until the process exits.  Host code
+// only sees a stand-in for it, so its device address is taken with
+// cudaGetSymbolAddress, once per device, with that device current.
+constexpr size_t kNoallocScratchBytes = (size_t)64 << 20;  // 64 MiB per GPU
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+void *g_noalloc_ptr[kMaxDev];
+
+cudaError_t noalloc_scratch(void **out)
+{
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void *p = nullptr;
+    err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess) return err;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+template <class T>
+cudaError_t run_noalloc(long L, int nm, int n, int m, T *a, T *w, int *info, cudaStream_t stream)
+{
+  if (bad_args(L, nm, n, m) || a == nullptr || w == nullptr) return cudaErrorInvalidValue;
+  if (n == 1) return run<T>(L, nm, n, m, a, w, nullptr, 0, info, nullptr, stream);
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  // largest chunk of matrices whose workspace fits in the static array
+  eigen_GPU_batch_opts o{};
+  o.method = EIGEN_GPU_BATCH_TQL2;
+  o.sort = 1;
+  o.chunk = 1;
+  Plan<T> pl;
+  if ((err = make_plan<T>(L, nm, n, dp, pl, &o)) != cudaSuccess) return err;
+  if (pl.bytes > kNoallocScratchBytes) return cudaErrorInvalidValue;  // one matrix does not fit
+  long chunk = std::min<long>(L, (long)(kNoallocScratchBytes / pl.bytes));
+  while (chunk > 1) {
+    o.chunk = (int)chunk;
+    if ((err = make_plan<T>(L, nm, n, dp, pl, &o)) != cudaSuccess) return err;
+    if (pl.bytes <= kNoallocScratchBytes) break;
+    chunk--;
+  }
+  o.chunk = (int)chunk;
+  void *scratch = nullptr;
+  if ((err = noalloc_scratch(&scratch)) != cudaSuccess) return err;
+  return run<T>(L, nm, n, m, a, w, scratch, kNoallocScratchBytes, info, &o, stream);
+}
+
 template <class T>
 cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, const T *z, double *err1, double *err2,
                       int *flags, float *ref_flags, cudaStream_t stream)
@@ -421,6 +480,12 @@ void eigen_GPU_check_FP(const int L, const int nm, const int n, const int m, flo
   if (eigb::check_run<float>(L, nm, n, m, a, w, z, nullptr, nullptr, nullptr, reinterpret_cast<float *>(a),
                              stream) == cudaSuccess)
     eigb::k_check_print<float><<<1, 1, 0, stream>>>(L, nm, n, a);
+}
+
+cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, const int m, double *a, double *w,
+                                       int *info, const cudaStream_t stream)
+{
+  return eigb::run_noalloc<double>(L, nm, n, m, a, w, info, stream);
 }
 
 cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents)

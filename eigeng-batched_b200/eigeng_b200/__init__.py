@@ -62,6 +62,8 @@ def lib():
             f = getattr(L, "eigen_GPU_check_ex_" + s)
             f.argtypes = [I, I, I, I, P, P, P, P, P, P, P]
             f.restype = I
+        L.eigen_GPU_batch_noalloc_DP.argtypes = [I, I, I, I, P, P, P, P]
+        L.eigen_GPU_batch_noalloc_DP.restype = I
         L.eigen_GPU_batch_trace.argtypes = [P, I]
         L.eigen_GPU_batch_trace.restype = I
         _lib = L
@@ -109,7 +111,7 @@ def exported_symbols():
         "eigen_GPU_batch_ex_BufferSize_DP", "eigen_GPU_batch_ex_BufferSize_FP",
         "eigen_GPU_check_DP", "eigen_GPU_check_FP",
         "eigen_GPU_check_ex_DP", "eigen_GPU_check_ex_FP",
-        "eigen_GPU_batch_trace",
+        "eigen_GPU_batch_trace", "eigen_GPU_batch_noalloc_DP",
     ]
 
 
@@ -184,6 +186,16 @@ def eigen_GPU_batch_ex(a, w, wk, n, nm=None, m=None, info=None, method=TQL2, sor
     lw = 0 if wk is None else wk.numel() * wk.element_size()
     return getattr(lib(), "eigen_GPU_batch_ex_" + _sfx(a.dtype))(
         L, nm, n, m, _ptr(a), _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), _stream(stream))
+
+
+def eigen_GPU_batch_noalloc(a, w, n, nm=None, m=None, info=None, stream=None):
+    """eigen_GPU_batch_noalloc_DP: solve with the library's static device
+    workspace (FP64, tql2, sorted); returns the cudaError_t status."""
+    L, nm = _dims(a, n, nm)
+    m = n if m is None else m
+    if a.dtype != torch.float64:
+        raise TypeError("eigen_GPU_batch_noalloc_DP takes float64 matrices")
+    return lib().eigen_GPU_batch_noalloc_DP(L, nm, n, m, _ptr(a), _ptr(w), _ptr(info), _stream(stream))
 
 
 def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=None, rec_cap=0, chunk=0):

@@ -95,6 +95,32 @@ cudaError_t eigen_GPU_batch_ex_FP(const int L, const int nm, const int n, const 
                                   const cudaStream_t stream);
 
 /*
+ * Solve without allocating (no counterpart in the reference).  For callers
+ * that must not allocate device memory -- a plugin's enqueue that runs
+ * under an allocator owned by a framework, a real-time loop where
+ * allocation is not allowed -- and so cannot
+ * provide the workspace of eigen_GPU_batch_DP.  Arguments as there
+ * (tql2, sorted eigenvalues); info is an optional device array of L ints as
+ * in eigen_GPU_batch_ex_DP.
+ * The workspace is a fixed 64 MiB array in the library's device memory,
+ * present on every GPU that loads the library until the process exits.
+ * Large batches are processed in as many pieces as needed; a single matrix
+ * must fit, which holds for n <= 1024 (the size limit of every entry point).
+ * Limits and behaviour:
+ *  - the first call on a device looks the array's address up
+ *    (cudaGetSymbolAddress); make that first call before any stream capture;
+ *  - every call uses the same array: calls that may overlap on the GPU
+ *    (different streams, or different host threads without ordering) race
+ *    and corrupt each other's results -- serialize them;
+ *  - nothing in the array needs to start cleared; each call writes what it
+ *    reads;
+ *  - returns cudaErrorInvalidValue for invalid sizes, otherwise the launch
+ *    status.
+ */
+cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, const int m, double *a, double *w,
+                                       int *info, const cudaStream_t stream);
+
+/*
  * Phase timing (counterpart of the reference's compile-time TIMER,
  * eigen_GPU_batch.cu:157-244, which prints per-phase times from warp 0).
  * When set, every later solve on the calling process records, for chunk c
