@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 namespace eigb {
 
@@ -139,6 +140,31 @@ __host__ __device__ __forceinline__ int hdr_i0(const Rec<double> &h) { Bits64 a;
 __host__ __device__ __forceinline__ int hdr_cnt(const Rec<double> &h) { Bits64 a; a.d = h.s; return (int)a.i; }
 __host__ __device__ __forceinline__ int hdr_i0(const Rec<float> &h) { Bits32 a; a.f = h.c; return a.i; }
 __host__ __device__ __forceinline__ int hdr_cnt(const Rec<float> &h) { Bits32 a; a.f = h.s; return a.i; }
+
+// Asynchronous global -> shared copy of B bytes (B = 4, 8 or 16, both
+// addresses aligned to B), completed by cp_async_wait_all().  Host builds
+// (unit tests) copy at once.
+template <int B> __host__ __device__ __forceinline__ void cp_async(void *dst_smem, const void *src)
+{
+#ifdef __CUDA_ARCH__
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(B) : "memory");
+#else
+  memcpy(dst_smem, src, B);
+#endif
+}
+__host__ __device__ __forceinline__ void cp_async_commit()
+{
+#ifdef __CUDA_ARCH__
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+#endif
+}
+__host__ __device__ __forceinline__ void cp_async_wait_all()
+{
+#ifdef __CUDA_ARCH__
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+#endif
+}
 
 // Per-matrix status block in the workspace.
 struct Meta {

@@ -2,14 +2,18 @@
 //
 //   k_n1           n == 1 (eigen_GPU_batch.cu:36-54): w = a(1,1), a(1,1) = 1
 //   k1_warp        phase 1 for n <= 32: one warp per matrix, 4 per CTA
-//   k1_cta<SM>     phase 1 for n > 32: one CTA per matrix; the matrix is
-//                  staged in shared memory (SM) or, when it does not fit,
+//   k1_reg<NB>     phase 1 for 32 < n <= 128: one CTA per matrix, the matrix
+//                  in registers (eigb_tridiag_reg.cuh)
+//   k1_cta<SPLIT>  phase 1 for larger n: one CTA per matrix; the leading
+//                  block that fits is staged in shared memory, the rest is
 //                  reduced in place in global memory
 //   k2_ql          phase 2: QL on (d, e), one matrix per thread
 //   k3_warp        phase 3 for n <= 32: rotations applied to Q held in
 //                  registers (one row per lane), selection-sort emulation,
 //                  permuted write-back
-//   k3_cta<SM>     phase 3 for n > 32, Z in shared memory or workspace
+//   k3_cta<SM>     phase 3 for n > 32: rows of Z in shared memory (a
+//                  matrix's rows split over CTAs when needed) or, for the
+//                  largest FP64 sizes, Z in the workspace
 //   k_jacobi_warp  cyclic Jacobi for n <= 32 (jac_tiled.hpp:3-152)
 //   k_check        FP64 residual / orthogonality gate (eigen_GPU_check.cu)
 #pragma once
@@ -31,6 +35,9 @@ template <class T> struct KP {
   Rec<T> *rec;   // workspace: rotation records, rcap per matrix
   Meta *meta;    // workspace: per-matrix status
   T *zs;         // workspace: n*n per matrix when Z does not fit in shared memory
+  int k1b;       // phase 1 (CTA form): leading block kept in shared memory
+  int zrows;     // phase 3 with Z in shared memory: rows per CTA ...
+  int zsplit;    // ... and CTAs per matrix
   int *info;     // optional per-matrix status for the caller (may be null)
   long Lc;       // matrices in this chunk
   int n, nm;
@@ -81,61 +88,69 @@ __global__ void __launch_bounds__(32 * K1W_NW) k1_warp(const KP<T> p)
   for (int c = 0; c < n; c++)
     if (r > c && r < n) S[r + c * K1W_LD] = S[c + r * K1W_LD];
   __syncwarp();
-  tridiag_qt<T, 1>(tm, S, K1W_LD, n, p.d + k * n, p.e + k * n, beta_s, pv, pv, red);
+  tridiag_qt<T, 1>(tm, S, K1W_LD, S, K1W_LD, n, n, p.d + k * n, p.e + k * n, beta_s, pv, pv, red);
   if (r < n)
     for (int c = 0; c < n; c++) A[r + (size_t)c * nm] = S[r + c * K1W_LD];
 }
 
 // Shared memory of k1_cta: red[72], beta[n], pv[n], part[nthreads], then S
 // (shared-memory variant) n x (n|1).
-template <class T> __host__ __device__ inline size_t k1c_smem_elems(int n, int nthreads, bool sm)
+// Shared-memory elements of k1_cta: red[72], beta[n], pv[n], part[nthreads]
+// and the leading B x B block of the matrix (leading dimension B|1).
+__host__ __device__ inline size_t k1c_smem_elems(int n, int nthreads, int B)
 {
-  return 72 + 2 * (size_t)n + (size_t)nthreads + (sm ? (size_t)n * (size_t)(n | 1) : 0);
+  return 72 + 2 * (size_t)n + (size_t)nthreads + (size_t)B * (size_t)(B | 1);
 }
 
-template <class T, bool SM, int SPLIT>
+// One CTA per matrix; the leading p.k1b x p.k1b block of the matrix is
+// worked on in shared memory and the rest in place in a (all of it in
+// shared memory when p.k1b = n).  On exit a holds Q (A = Q T Q^T): its rows
+// are what phase 3 rotates.
+template <class T, int SPLIT>
 __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long k = blockIdx.x;
   const int n = p.n, nm = p.nm, t = threadIdx.x, nt = blockDim.x;
+  const int B = p.k1b, ld = B | 1;
   T *A = p.a + (size_t)k * nm * n;
   T *sm = reinterpret_cast<T *>(smem_raw);
   T *red = sm;          // 72
   T *beta_s = sm + 72;  // n
   T *pv = beta_s + n;   // n
   T *part = pv + n;     // nt
-  T *S;
-  int ld;
-  if (SM) {
-    ld = n | 1;
-    S = part + nt;
-    for (int idx = t; idx < n * n; idx += nt) {  // upper triangle, coalesced
-      const int r = idx % n, c = idx / n;
-      if (r <= c) S[r + c * ld] = A[r + (size_t)c * nm];
-    }
-    __syncthreads();
-    for (int idx = t; idx < n * n; idx += nt) {
-      const int r = idx % n, c = idx / n;
-      if (r > c) S[r + c * ld] = S[c + r * ld];
-    }
-    __syncthreads();
-  } else {
-    ld = nm;
-    S = A;
-    for (long idx = t; idx < (long)n * n; idx += nt) {
-      const int r = (int)(idx % n), c = (int)(idx / n);
-      if (r > c) A[r + (size_t)c * nm] = A[c + (size_t)r * nm];
-    }
-    __syncthreads();
+  T *S = part + nt;     // B x B
+  // full symmetric matrix from the upper triangle: the leading block in S
+  // (coalesced reads), the outer band mirrored in place
+  for (int idx = t; idx < B * B; idx += nt) {
+    const int r = idx % B, c = idx / B;
+    if (r <= c) S[r + c * ld] = A[r + (size_t)c * nm];
   }
+  for (long idx = t; idx < (long)n * n; idx += nt) {
+    const int r = (int)(idx % n), c = (int)(idx / n);
+    if (r > c && r >= B) A[r + (size_t)c * nm] = A[c + (size_t)r * nm];
+  }
+  __syncthreads();
+  for (int idx = t; idx < B * B; idx += nt) {
+    const int r = idx % B, c = idx / B;
+    if (r > c) S[r + c * ld] = S[c + r * ld];
+  }
+  __syncthreads();
   CtaTeam tm;
-  tridiag_qt<T, SPLIT>(tm, S, ld, n, p.d + k * n, p.e + k * n, beta_s, pv, part, red);
-  if (SM)
-    for (int idx = t; idx < n * n; idx += nt) {
-      const int r = idx % n, c = idx / n;
-      A[r + (size_t)c * nm] = S[r + c * ld];
+  tridiag_qt<T, SPLIT>(tm, S, ld, A, nm, B, n, p.d + k * n, p.e + k * n, beta_s, pv, part, red);
+  // the storage holds M = Q^T; a receives Q: the leading block transposed
+  // out of S, the outer band transposed in place (pairs (r, c), (c, r)
+  // both lie outside the block)
+  for (long idx = t; idx < (long)n * n; idx += nt) {
+    const int r = (int)(idx % n), c = (int)(idx / n);
+    if (r < B && c < B) {
+      A[r + (size_t)c * nm] = S[c + r * ld];
+    } else if (r < c) {
+      const T x = A[r + (size_t)c * nm];
+      A[r + (size_t)c * nm] = A[c + (size_t)r * nm];
+      A[c + (size_t)r * nm] = x;
     }
+  }
 }
 
 // Register-resident phase 1 for 32 < n <= 32*NB, one CTA of NB*NB warps
@@ -180,7 +195,9 @@ __global__ void k2_ql(const KP<T> p)
   } else {
     mt.overflow = 0;
     mt.ierr = ierr;
-    T *wo = p.w + k * n;
+    // unsorted eigenvalues over e (no longer needed): phase 3 reads them
+    // from there in every CTA of the matrix, and writes w sorted
+    T *wo = p.e + k * n;
     for (int i = 0; i < n; i++) wo[i] = dd[(size_t)i * st];
   }
   p.meta[k] = mt;
@@ -333,7 +350,7 @@ __global__ void __launch_bounds__(32 * K3W_NW) k3_warp(const KP<T> p)
       apply(sl.rbuf, cnt);
       __syncwarp();
     }
-    dr = (r < n) ? p.w[k * n + r] : T(0);
+    dr = (r < n) ? p.e[k * n + r] : T(0);
     ierr = mt.ierr;
   } else {
     // capacity exceeded in phase 2: regenerate the rotations in small chunks
@@ -364,185 +381,122 @@ __global__ void __launch_bounds__(32 * K3W_NW) k3_warp(const KP<T> p)
 }
 
 // ---------------------------------------------------------------- phase 3, n > 32
-constexpr int K3_WAVE = 4;  // sweeps applied per pass in k3_cta
-
-// Records staged per chunk in k3_cta: room for K3_WAVE whole segments.
-__host__ __device__ inline int k3c_chunk(int n) { return ((K3_WAVE * (n + 1) + 63) / 64) * 64; }
+// Records staged per buffer in k3_cta (two buffers, one being filled while
+// the other is applied): room for two whole segments.
+__host__ __device__ inline int k3c_chunk(int n) { return ((2 * (n + 1) + 63) / 64) * 64; }
 
 template <class T> __host__ __device__ inline size_t k3c_fixed_bytes(int n)
 {
-  size_t b = sizeof(Rec<T>) * (size_t)k3c_chunk(n) + sizeof(T) * (3 * (size_t)n + 64) +
+  size_t b = sizeof(Rec<T>) * 2 * (size_t)k3c_chunk(n) + sizeof(T) * (3 * (size_t)n + 64) +
              sizeof(int) * (2 * (size_t)n + 8);
   return (b + 15) & ~(size_t)15;
 }
 
-template <class T> __host__ __device__ inline size_t k3c_smem_bytes(int n, bool sm)
+// rows: rows of Z held in shared memory by one CTA (0: Z in the workspace)
+template <class T> __host__ __device__ inline size_t k3c_smem_bytes(int n, int rows)
 {
-  size_t b = k3c_fixed_bytes<T>(n);
-  if (sm) b += sizeof(T) * (size_t)n * (size_t)(n | 1);
-  return b;
+  return k3c_fixed_bytes<T>(n) + sizeof(T) * (size_t)rows * (size_t)(n | 1);
 }
 
-// Applies a group of ns <= K3_WAVE consecutive sweeps (segment s: rotations
-// i0[s], i0[s]-1, ..., i0[s]-len[s]+1, records rb[off[s]...]) to one row
-// whose column c is zr[c*cs].  Sweep s runs one column behind sweep s-1 as
-// stage s of a pipeline: at step j0 stage s handles column j0+s, taking the
-// column value just produced by stage s-1; outside its range a stage is an
-// identity rotation, i.e. a one-column delay.  The loop is skewed: in
-// iteration tau stage s works on step tau-s, so the stages of an iteration
-// are independent (four rotation chains in flight per row).  Every column
-// is loaded once (stage 0) and stored once (last stage).  Iterations in
-// which every stage rotates run without any range check.
-#define EIGB_WSTAGE(S, IN)                                                     \
-  if (S < ns && tau >= S && tau - S < nsteps) {                              \
-    const T in_ = (IN);                                                      \
-    if (tau >= rs##S && tau <= re##S) {                                      \
-      const Rec<T> rr = rb[ro##S + (tau - rs##S)];                           \
-      y##S = fma(rr.c, h##S, rr.s * in_);                                    \
-      h##S = fma(-rr.s, h##S, rr.c * in_);                                   \
-    } else {                                                                 \
-      y##S = h##S;                                                           \
-      h##S = in_;                                                            \
-    }                                                                        \
-    if (S == ns - 1) {                                                       \
-      const int oc = jt - (tau - S) + ns;                                    \
-      if (oc >= 0 && oc < n) zr[oc * cs] = y##S;                             \
-    }                                                                        \
+// Rotations K3_U at a time: the columns and records of the next block are
+// loaded before the stores of the current one, so their latency overlaps
+// the rotation chain (which only waits for one fma per rotation).
+constexpr int K3_U = 8;
+
+#define EIGB_CHAIN(R, Z, OUT)                     \
+  {                                               \
+    const T y_ = fma((R).c, h, (R).s * (Z));      \
+    h = fma(-(R).s, h, (R).c * (Z));              \
+    OUT = y_;                                     \
   }
 
+// One segment: rotations i0, i0-1, ..., i0-len+1 (records rp[0..len)) on a
+// row whose column c is zr[c*cs].  Rotation i replaces (z_i, z_{i+1}) by
+// (c z_i - s z_{i+1}, s z_i + c z_{i+1}); z_{i+1} is carried in h, which
+// enters as column i0+1 and leaves as column i0-len+1.
 template <class T, int CS>
-__host__ __device__ __forceinline__ void wave_apply(T *__restrict__ zr, const int cs_rt, const int n,
-                                                    const Rec<T> *__restrict__ rb, const int (&i0)[K3_WAVE],
-                                                    const int (&len)[K3_WAVE], const int (&off)[K3_WAVE],
-                                                    const int ns)
+__host__ __device__ __forceinline__ void seg_apply(T *__restrict__ zr, const int cs_rt,
+                                                   const Rec<T> *__restrict__ rp, const int i0, const int len)
 {
-  static_assert(K3_WAVE == 4, "four stages are spelled out below");
   const int cs = CS > 0 ? CS : cs_rt;
-  int jt = i0[0], jb = i0[0] - len[0] + 1;
-  if (ns > 1) { jt = max(jt, i0[1] - 1); jb = min(jb, i0[1] - len[1] + 1 - 1); }
-  if (ns > 2) { jt = max(jt, i0[2] - 2); jb = min(jb, i0[2] - len[2] + 1 - 2); }
-  if (ns > 3) { jt = max(jt, i0[3] - 3); jb = min(jb, i0[3] - len[3] + 1 - 3); }
-  const int nsteps = jt - (jb - ns) + 1;
-  // stage s rotates in iterations [rs, re]; its records start at rb[ro]
-  const int rs0 = 0 + jt + 0 - i0[0], re0 = rs0 + len[0] - 1, ro0 = off[0];
-  const int rs1 = 1 + jt + 1 - i0[1], re1 = rs1 + len[1] - 1, ro1 = off[1];
-  const int rs2 = 2 + jt + 2 - i0[2], re2 = rs2 + len[2] - 1, ro2 = off[2];
-  const int rs3 = 3 + jt + 3 - i0[3], re3 = rs3 + len[3] - 1, ro3 = off[3];
-  T h0 = (jt + 1 < n) ? zr[(jt + 1) * cs] : T(0);
-  T h1 = (ns > 1 && jt + 2 < n) ? zr[(jt + 2) * cs] : T(0);
-  T h2 = (ns > 2 && jt + 3 < n) ? zr[(jt + 3) * cs] : T(0);
-  T h3 = (ns > 3 && jt + 4 < n) ? zr[(jt + 4) * cs] : T(0);
-  T x0 = T(0), x1 = T(0), x2 = T(0);
-  const int total = nsteps + ns - 1;
-  // steady range: all four stages rotating
-  int slo = total, shi = -1;
-  if (ns == 4) {
-    slo = max(max(rs0, rs1), max(rs2, rs3));
-    shi = min(min(re0, re1), min(re2, re3));
-  }
-  int tau = 0;
-  for (int phase = 0; phase < 2; phase++) {
-    // general iterations (range checks) up to the steady range, then after it
-    const int tend = (phase == 0 && slo <= shi) ? slo : total;
-    for (; tau < tend; tau++) {
-      T y0 = T(0), y1 = T(0), y2 = T(0), y3 = T(0);
-      EIGB_WSTAGE(0, (jt - tau >= 0) ? zr[(jt - tau) * cs] : T(0))
-      EIGB_WSTAGE(1, x0)
-      EIGB_WSTAGE(2, x1)
-      EIGB_WSTAGE(3, x2)
-      x0 = y0;
-      x1 = y1;
-      x2 = y2;
-    }
-    if (phase == 0 && slo <= shi) {
-      // steady state: no checks; stage 0 loads column jt-tau, stage 3
-      // stores column jt-tau+7 (= jt-(tau-3)+4), records advance by one
-      const Rec<T> *p0 = rb + ro0 + (tau - rs0);
-      const Rec<T> *p1 = rb + ro1 + (tau - rs1);
-      const Rec<T> *p2 = rb + ro2 + (tau - rs2);
-      const Rec<T> *p3 = rb + ro3 + (tau - rs3);
-      T *zin = zr + (jt - tau) * cs;
-      T *zout = zr + (jt - tau + 7) * cs;
-      // operands of the next iteration are loaded before this iteration's
-      // store (they never alias: input column jt-tau-1, output jt-tau+7)
-      T in0 = *zin;
-      Rec<T> r0 = *p0, r1 = *p1, r2 = *p2, r3 = *p3;
-      for (; tau <= shi; tau++) {
-        const T y0 = fma(r0.c, h0, r0.s * in0);
-        h0 = fma(-r0.s, h0, r0.c * in0);
-        const T y1 = fma(r1.c, h1, r1.s * x0);
-        h1 = fma(-r1.s, h1, r1.c * x0);
-        const T y2 = fma(r2.c, h2, r2.s * x1);
-        h2 = fma(-r2.s, h2, r2.c * x1);
-        const T y3 = fma(r3.c, h3, r3.s * x2);
-        h3 = fma(-r3.s, h3, r3.c * x2);
-        if (tau < shi) {
-          zin -= cs;
-          in0 = *zin;
-          r0 = *++p0;
-          r1 = *++p1;
-          r2 = *++p2;
-          r3 = *++p3;
-        }
-        *zout = y3;  // stage 3 rotates a column <= n-2 here, so the output column is < n
-        zout -= cs;
-        x0 = y0;
-        x1 = y1;
-        x2 = y2;
-      }
-    }
-  }
-}
-#undef EIGB_WSTAGE
-
-// Reads up to K3_WAVE complete segments (header + rotations) from
-// rbuf[q..cnt); advances q past them; returns how many were read.
-template <class T>
-__host__ __device__ __forceinline__ int parse_group(const Rec<T> *rbuf, const int cnt, int &q, int (&i0)[K3_WAVE],
-                                                    int (&len)[K3_WAVE], int (&off)[K3_WAVE])
-{
-  int ns = 0;
+  T *p = zr + i0 * cs;  // column of the next rotation's z_i
+  T h = p[cs];
+  int j = 0;
+  if (len >= 2 * K3_U) {
+    T z[K3_U];
+    Rec<T> r[K3_U];
 #pragma unroll
-  for (int s = 0; s < K3_WAVE; s++) {
-    i0[s] = 0;
-    len[s] = 0;
-    off[s] = 0;
-    if (ns == s && q < cnt) {
-      const Rec<T> hd = rbuf[q];
-      const int L = hdr_cnt(hd);
-      if (L >= 1 && q + 1 + L <= cnt) {
-        i0[s] = hdr_i0(hd);
-        len[s] = L;
-        off[s] = q + 1;
-        q += 1 + L;
-        ns++;
+    for (int u = 0; u < K3_U; u++) {
+      z[u] = p[-u * cs];
+      r[u] = rp[u];
+    }
+    for (; j + 2 * K3_U <= len; j += K3_U) {
+      T zn[K3_U];
+      Rec<T> rn[K3_U];
+#pragma unroll
+      for (int u = 0; u < K3_U; u++) {
+        zn[u] = p[-(K3_U + u) * cs];  // columns below every store of this block
+        rn[u] = rp[j + K3_U + u];
+      }
+#pragma unroll
+      for (int u = 0; u < K3_U; u++) EIGB_CHAIN(r[u], z[u], p[(1 - u) * cs])
+      p -= K3_U * cs;
+#pragma unroll
+      for (int u = 0; u < K3_U; u++) {
+        z[u] = zn[u];
+        r[u] = rn[u];
       }
     }
+    // j + K3_U <= len: the block in registers is still inside the segment
+#pragma unroll
+    for (int u = 0; u < K3_U; u++) EIGB_CHAIN(r[u], z[u], p[(1 - u) * cs])
+    p -= K3_U * cs;
+    j += K3_U;
   }
-  return ns;
+  for (; j < len; j++, p -= cs) {
+    const T z0 = p[0];
+    EIGB_CHAIN(rp[j], z0, p[cs])
+  }
+  p[cs] = h;
 }
+#undef EIGB_CHAIN
 
-// Applies the complete segments of rbuf[0..cnt) in groups of K3_WAVE to the
-// rows this thread owns; returns the index of the first incomplete segment.
-template <class T, bool SM, int RPT>
-__device__ __forceinline__ int apply_chunk(const Rec<T> *rbuf, const int cnt, const int n, const int cs,
-                                           const bool (&own)[RPT], T *const (&zr)[RPT])
+// End of the last complete segment (header + rotations) in rbuf[0..cnt).
+template <class T> __host__ __device__ __forceinline__ int seg_walk(const Rec<T> *rbuf, const int cnt)
 {
   int q = 0;
-  while (true) {
-    int i0[K3_WAVE], len[K3_WAVE], off[K3_WAVE];
-    const int ns = parse_group(rbuf, cnt, q, i0, len, off);
-    if (ns == 0) break;
-#pragma unroll
-    for (int j = 0; j < RPT; j++)
-      if (own[j]) {
-        if (SM) wave_apply<T, 1>(zr[j], 1, n, rbuf, i0, len, off, ns);
-        else wave_apply<T, 0>(zr[j], cs, n, rbuf, i0, len, off, ns);
-      }
+  while (q < cnt) {
+    const int L = hdr_cnt(rbuf[q]);
+    if (L < 0 || q + 1 + L > cnt) break;
+    q += 1 + L;
   }
   return q;
 }
 
+// Applies the segments of rbuf[0..used) (complete, as found by seg_walk) to
+// the rows this thread owns.
+template <class T, bool SM, int RPT>
+__device__ __forceinline__ void apply_chunk(const Rec<T> *rbuf, const int used, const int cs, const bool (&own)[RPT],
+                                            T *const (&zr)[RPT])
+{
+  int q = 0;
+  while (q < used) {
+    const Rec<T> hd = rbuf[q];
+    const int L = hdr_cnt(hd), i0 = hdr_i0(hd);
+#pragma unroll
+    for (int j = 0; j < RPT; j++)
+      if (own[j]) {
+        if (SM) seg_apply<T, 1>(zr[j], 1, rbuf + q + 1, i0, L);
+        else seg_apply<T, 0>(zr[j], cs, rbuf + q + 1, i0, L);
+      }
+    q += 1 + L;
+  }
+}
+
+// Phase 1 leaves Q in a; rotations act on the rows of Q independently, so
+// with Z in shared memory a matrix's rows are split over p.zsplit CTAs of
+// p.zrows rows each (every CTA reads all records and only its own rows of
+// a, and writes only those rows back).
 // Z layout: in shared memory row-major, Z(r, c) at Z[r*(n|1) + c] (each
 // thread walks its own contiguous row; at a fixed column the warp touches
 // rows with an odd stride: conflict-free).  In the workspace (large n)
@@ -552,8 +506,11 @@ template <class T, bool SM, int RPT>
 __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const long k = blockIdx.x;
+  const int zsplit = SM ? p.zsplit : 1;
+  const long k = blockIdx.x / zsplit;
   const int n = p.n, nm = p.nm, t = threadIdx.x, nt = blockDim.x;
+  const int r0 = SM ? (int)(blockIdx.x % zsplit) * p.zrows : 0;
+  const int nrow = SM ? min(p.zrows, n - r0) : n;
   const int ch = k3c_chunk(n);
   Rec<T> *rbuf = reinterpret_cast<Rec<T> *>(smem_raw);
   T *sd = reinterpret_cast<T *>(rbuf + ch);
@@ -575,33 +532,50 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
     cs = n;
   }
   T *A = p.a + (size_t)k * nm * n;
-  // Z = Q = M^T with M = Q^T in a: Z(r, c) = M(c, r) = a[c + r*nm]
-  for (int idx = t; idx < n * n; idx += nt) {
-    const int c = idx % n, rr = idx / n;
-    Z[rr * rs + c * cs] = A[c + (size_t)rr * nm];
+  const Meta mt = p.meta[k];
+  if (!mt.overflow) {  // first chunk of records, copied while Z is loaded
+    const Rec<T> *src = p.rec + (size_t)k * p.rcap;
+    const int cnt = min(ch, mt.nrec);
+    for (int q = t; q < cnt; q += nt) cp_async<sizeof(Rec<T>)>(rbuf + q, src + q);
+    cp_async_commit();
   }
+  // Z = rows r0 .. r0+nrow-1 of Q
+  for (int idx = t; idx < nrow * n; idx += nt) {
+    const int rr = idx % nrow, c = idx / nrow;
+    Z[rr * rs + c * cs] = A[r0 + rr + (size_t)c * nm];
+  }
+  cp_async_wait_all();
   __syncthreads();
 
-  const Meta mt = p.meta[k];
   bool own[RPT];
   T *zr[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; j++) {
-    own[j] = t + j * nt < n;
+    own[j] = t + j * nt < nrow;
     zr[j] = Z + (own[j] ? t + j * nt : 0) * rs;
   }
   if (!mt.overflow) {
+    // double buffer: the next chunk is copied in while this one is applied
     const Rec<T> *src = p.rec + (size_t)k * p.rcap;
-    int base = 0;
+    int base = 0, cur = 0;
     while (base < mt.nrec) {
+      Rec<T> *rb = rbuf + cur * ch;
       const int cnt = min(ch, mt.nrec - base);
-      for (int q = t; q < cnt; q += nt) rbuf[q] = src[base + q];
+      const int used = seg_walk(rb, cnt);
+      const int nb = base + (used > 0 ? used : cnt);  // a segment is at most n records: used > 0
+      if (nb < mt.nrec) {
+        Rec<T> *nx = rbuf + (cur ^ 1) * ch;
+        const int ncnt = min(ch, mt.nrec - nb);
+        for (int q = t; q < ncnt; q += nt) cp_async<sizeof(Rec<T>)>(nx + q, src + nb + q);
+        cp_async_commit();
+      }
+      apply_chunk<T, SM, RPT>(rb, used, cs, own, zr);
+      cp_async_wait_all();
       __syncthreads();
-      const int used = apply_chunk<T, SM, RPT>(rbuf, cnt, n, cs, own, zr);
-      __syncthreads();
-      base += used > 0 ? used : cnt;  // a segment is at most n records: used > 0
+      base = nb;
+      cur ^= 1;
     }
-    for (int c = t; c < n; c += nt) sd[c] = p.w[k * n + c];
+    for (int c = t; c < n; c += nt) sd[c] = p.e[k * n + c];
     if (t == 0) sflag[2] = mt.ierr;
   } else {
     // capacity exceeded in phase 2: regenerate in chunks (segments are
@@ -622,7 +596,7 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
       __syncthreads();
       const int nr = sflag[0];
       const int done = sflag[1];
-      apply_chunk<T, SM, RPT>(rbuf, nr, n, cs, own, zr);
+      apply_chunk<T, SM, RPT>(rbuf, nr, cs, own, zr);
       __syncthreads();
       if (done) break;
     }
@@ -657,10 +631,12 @@ __global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
   for (int j = 0; j < RPT; j++)
     if (own[j]) {
       const int row = t + j * nt;
-      for (int c = 0; c < n; c++) A[row + (size_t)inv[c] * nm] = Z[row * rs + c * cs];
+      for (int c = 0; c < n; c++) A[r0 + row + (size_t)inv[c] * nm] = Z[row * rs + c * cs];
     }
-  for (int c = t; c < n; c += nt) p.w[k * n + inv[c]] = sd[c];
-  if (p.info && t == 0) p.info[k] = ierr;
+  if (r0 == 0) {
+    for (int c = t; c < n; c += nt) p.w[k * n + inv[c]] = sd[c];
+    if (p.info && t == 0) p.info[k] = ierr;
+  }
 }
 
 // ---------------------------------------------------------------- Jacobi, n <= 32

@@ -56,25 +56,45 @@ __host__ __device__ __forceinline__ T dot_col(const T *__restrict__ Sr, const in
   return (a0 + a1) + (a2 + a3);
 }
 
-// On entry S holds the full symmetric matrix (both triangles).  On exit
-// d_out[0:n] = diagonal, e_out[0:n] = off-diagonal (e_out[k] couples k and
-// k+1, e_out[n-1] = 0, the reference's convention tred1_tiled.hpp:207-212)
-// and S holds M = Q^T with A = Q T Q^T.
+// Storage of tridiag_qt: element (r, c) is S[r + c*ld] (shared memory) when
+// r < B and c < B, else G[r + c*ldg] (global memory).  B = n keeps the whole
+// matrix in shared memory, B = 0 none of it; in between, the leading B x B
+// block (where the bottom-up reduction spends its last steps, and the
+// formation of M its first) is on chip and only the outer band goes to
+// memory.  Column i < B lies entirely in S (its rows are < i), column
+// i >= B entirely in G.
+template <class T> struct HybridRow {
+  T *s;    // row r in S: element (r, k) at s[k*ld] for k < lim
+  T *g;    // row r in G: element (r, k) at g[k*ldg] for k >= lim
+  int ld, ldg, lim;
+  __host__ __device__ __forceinline__ T &at(int k) const
+  {
+    return (k < lim) ? s[(size_t)k * ld] : g[(size_t)k * ldg];
+  }
+};
+
+// On entry the storage holds the full symmetric matrix (both triangles).
+// On exit d_out[0:n] = diagonal, e_out[0:n] = off-diagonal (e_out[k]
+// couples k and k+1, e_out[n-1] = 0, the reference's convention
+// tred1_tiled.hpp:207-212) and the storage holds M = Q^T with A = Q T Q^T.
 // Shared scratch: beta_s[n], pv[n], part[SPLIT*nr], red[72] (64 for team
 // reductions, red[64] carries the reflector pivot to the team).
 template <class T, int SPLIT, class Team>
-__host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T *d_out, T *e_out, T *beta_s,
-                                    T *pv, T *part, T *red)
+__host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, T *G, const int ldg, const int B, const int n,
+                                    T *d_out, T *e_out, T *beta_s, T *pv, T *part, T *red)
 {
   const int nt = tm.size();
   const int nr = nt / SPLIT;
   const int t = tm.rank;
   const int r = t % nr;
   const int h = t / nr;
-  T *Sr = S + r;  // row r: element (r, k) at Sr[k*ld]
+  const HybridRow<T> row{S + r, G + r, ld, ldg, (r < B) ? B : 0};
+  T *Sr = row.s;
+  T *Gr = row.g;
+  const int Br = row.lim;  // first column of row r held in G
 
   for (int i = n - 1; i >= 1; --i) {
-    const T *ucol = S + i * ld;  // reflector: column i, rows 0..i-1
+    T *ucol = (i < B) ? S + (size_t)i * ld : G + (size_t)i * ldg;  // reflector: column i, rows 0..i-1
     // ---- reflector ----
     // Column i was last updated (previous step) by the threads whose column
     // range held i; only they read it before the barrier.
@@ -87,7 +107,7 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T
     const T ul = ulast - anorm;
     const T beta = T(1) / flip0to1(ul * anorm);
     ur = (r < i - 1) ? ucol[r] : ((r == i - 1) ? ul : T(0));
-    if (r == i - 1 && h == 0) S[(i - 1) + i * ld] = ul;  // reflector pivot stored back
+    if (r == i - 1 && h == 0) ucol[i - 1] = ul;  // reflector pivot stored back
     if (t == 0) {
       e_out[i - 1] = anorm;
       beta_s[i] = beta;
@@ -99,8 +119,8 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T
     if (r < i) {
       // column i-1 of u is the new pivot ul: ucol[i-1] is being rewritten
       const int hi1 = min(hi, i - 1);
-      T pp = dot_col(Sr, ld, ucol, lo, hi1);
-      if (lo <= i - 1 && i - 1 < hi) pp = fma(Sr[(i - 1) * ld], ul, pp);
+      T pp = dot_col(Sr, ld, ucol, lo, min(hi1, Br)) + dot_col(Gr, ldg, ucol, max(lo, Br), hi1);
+      if (lo <= i - 1 && i - 1 < hi) pp = fma(row.at(i - 1), ul, pp);
       if (SPLIT > 1) part[h * nr + r] = pp;
       else pv[r] = pp * beta;
     }
@@ -129,17 +149,24 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T
     // ---- A += u w^T + w u^T, w = p + alpha u (both triangles, own columns) ----
     if (r < i) {
       const T wr = fma(alpha, ur, pr);
-      int off = lo * ld;
-      for (int k = lo; k < hi; k++, off += ld) {
+      const int mid = max(lo, min(hi, Br));
+      size_t off = (size_t)lo * ld;
+      for (int k = lo; k < mid; k++, off += ld) {
         const T uk = ucol[k];
         const T wk = fma(alpha, uk, pv[k]);
         Sr[off] = fma(wk, ur, fma(uk, wr, Sr[off]));
+      }
+      off = (size_t)mid * ldg;
+      for (int k = mid; k < hi; k++, off += ldg) {
+        const T uk = ucol[k];
+        const T wk = fma(alpha, uk, pv[k]);
+        Gr[off] = fma(wk, ur, fma(uk, wr, Gr[off]));
       }
     }
     // the barrier in the next step's first sum() orders these updates
   }
   tm.sync();
-  if (r < n && h == 0) d_out[r] = Sr[r * ld];
+  if (r < n && h == 0) d_out[r] = row.at(r);
   if (t == 0) e_out[n - 1] = T(0);
   tm.sync();
 
@@ -150,24 +177,25 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T
   // are also the only entries it reads, so the extension needs no barrier.
   for (int k = 1; k < n; k++) {
     const T bk = beta_s[k];
-    const T *ucol = S + k * ld;
+    const T *ucol = (k < B) ? S + (size_t)k * ld : G + (size_t)k * ldg;
     int lo, hi;
     split_range<SPLIT>(k, h, lo, hi);
+    const int mid = max(lo, min(hi, Br));
     if (r < k) {
       if (k == 1) {
-        if (h == 0) Sr[0] = T(1);  // M_0 = [1]
+        if (h == 0) row.at(0) = T(1);  // M_0 = [1]
       } else if (r < k - 1) {
-        if (lo <= k - 1 && k - 1 < hi) Sr[(k - 1) * ld] = T(0);
+        if (lo <= k - 1 && k - 1 < hi) row.at(k - 1) = T(0);
       } else {  // r == k-1: row k-1 of the extension
-        for (int c = lo; c < hi; c++) Sr[c * ld] = (c == k - 1) ? T(1) : T(0);
+        for (int c = lo; c < hi; c++) row.at(c) = (c == k - 1) ? T(1) : T(0);
       }
-      T q = dot_col(Sr, ld, ucol, lo, hi);
+      T q = dot_col(Sr, ld, ucol, lo, mid) + dot_col(Gr, ldg, ucol, mid, hi);
       if (SPLIT > 1) {
         part[h * nr + r] = q;
       } else {
         q *= bk;
-        int off = lo * ld;
-        for (int c = lo; c < hi; c++, off += ld) Sr[off] = fma(q, ucol[c], Sr[off]);
+        for (int c = lo; c < mid; c++) Sr[(size_t)c * ld] = fma(q, ucol[c], Sr[(size_t)c * ld]);
+        for (int c = mid; c < hi; c++) Gr[(size_t)c * ldg] = fma(q, ucol[c], Gr[(size_t)c * ldg]);
       }
     }
     if (SPLIT > 1) {
@@ -177,8 +205,8 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T
 #pragma unroll
         for (int s = 0; s < SPLIT; s++) q += part[s * nr + r];
         q *= bk;
-        int off = lo * ld;
-        for (int c = lo; c < hi; c++, off += ld) Sr[off] = fma(q, ucol[c], Sr[off]);
+        for (int c = lo; c < mid; c++) Sr[(size_t)c * ld] = fma(q, ucol[c], Sr[(size_t)c * ld]);
+        for (int c = mid; c < hi; c++) Gr[(size_t)c * ldg] = fma(q, ucol[c], Gr[(size_t)c * ldg]);
       }
     }
     tm.sync();  // column k is overwritten by the next extension; part is reused
@@ -187,9 +215,9 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, const int n, T
     int lo, hi;
     split_range<SPLIT>(n, h, lo, hi);
     if (r < n - 1) {
-      if (lo <= n - 1 && n - 1 < hi) Sr[(n - 1) * ld] = T(0);
+      if (lo <= n - 1 && n - 1 < hi) row.at(n - 1) = T(0);
     } else {
-      for (int c = lo; c < hi; c++) Sr[c * ld] = (c == n - 1) ? T(1) : T(0);
+      for (int c = lo; c < hi; c++) row.at(c) = (c == n - 1) ? T(1) : T(0);
     }
   }
   tm.sync();

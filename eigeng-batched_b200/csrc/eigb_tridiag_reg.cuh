@@ -54,7 +54,7 @@ template <int NB> struct RegLayout {
 };
 
 // Shared-memory elements of tridiag_qt_reg: V (max(n*NR, n*(n|1)), also the
-// staging area of the input), part[2*NB*NR], pv[NR], beta[NR], red[72].
+// staging area of the input and of the output), part[2*NB*NR], pv[NR], beta[NR], red[72].
 // Offset of the arrays after V, rounded to 4 elements so that the paired
 // loads of V and pv stay aligned for every n.
 template <int NB> __host__ __device__ inline size_t reg_voff(int n)
@@ -69,7 +69,7 @@ template <int NB> __host__ __device__ inline size_t reg_smem_elems(int n)
   return reg_voff<NB>(n) + 2 * (size_t)NB * NR + 2 * (size_t)NR + 72;
 }
 
-// A: the input matrix (upper triangle used), overwritten with M = Q^T.
+// A: the input matrix (upper triangle used), overwritten with Q (A = Q T Q^T).
 template <class T, int NB, class Team>
 __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int n, T *d_out, T *e_out, T *sm)
 {
@@ -212,10 +212,19 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
       }
     }
   }
+  // Q = M^T, written through the (now free) reflector store so that both
+  // the shared-memory and the global accesses stay unit-stride:
+  // W[x + y*lds] = M(x, y), then A(i, j) = M(j, i) = W[j + i*lds]
+  tm.sync();
   if (r < n) {
 #pragma unroll
     for (int c = 0; c < 32; c++)
-      if (c0 + c < n) A[r + (size_t)(c0 + c) * nm] = Mr[c];
+      if (c0 + c < n) V[r + (c0 + c) * lds] = Mr[c];
+  }
+  tm.sync();
+  for (int idx = t; idx < n * n; idx += tm.size()) {
+    const int i = idx % n, j = idx / n;
+    A[i + (size_t)j * nm] = V[j + i * lds];
   }
 }
 

@@ -77,7 +77,16 @@ inline void trace(long chunk, int slot, cudaStream_t stream)
 }
 
 inline int k1c_threads(int n) { return std::min(1024, ((n + 31) / 32) * 32 * k1_split(n)); }
-template <class T> size_t k1c_smem_bytes(int n) { return sizeof(T) * k1c_smem_elems<T>(n, k1c_threads(n), true); }
+// leading block of phase 1 (CTA form) held in shared memory: the largest
+// that fits next to the scratch arrays, at most n
+template <class T> int k1c_block(int n, size_t optin)
+{
+  const size_t base = sizeof(T) * k1c_smem_elems(n, k1c_threads(n), 0);
+  if (base >= optin) return 0;
+  int B = n;
+  while (B > 0 && base + sizeof(T) * (size_t)B * (size_t)(B | 1) > optin) B--;
+  return B;
+}
 template <class T> size_t k2_smem_per_thread(int n) { return sizeof(T) * 2 * (size_t)n; }
 
 // Layout of the workspace for one chunk of Lc matrices.
@@ -85,7 +94,9 @@ template <class T> struct Plan {
   int n = 0, nm = 0;
   long L = 0, Lc = 0;
   int rcap = 0;
-  bool sm = false;  // Z / S staged in shared memory (n > 32)
+  int k1b = 0;        // phase 1 (CTA form): leading block held in shared memory
+  int zrows = 0;      // phase 3: rows of Z per CTA in shared memory (0: Z in the workspace)
+  int zsplit = 1;     // phase 3: CTAs per matrix
   size_t off_d = 0, off_e = 0, off_meta = 0, off_rec = 0, off_z = 0, bytes = 0;
 };
 
@@ -106,10 +117,29 @@ cudaError_t make_plan(long L, int nm, int n, const DevProps &dp, Plan<T> &pl, co
   pl.L = L;
   pl.rcap = rcap_opt > 0 ? std::max(rcap_opt, 4) : rec_capacity<T>(n);
   const size_t optin = (size_t)dp.smem_optin;
-  pl.sm = n > 32 && k1c_smem_bytes<T>(n) <= optin && k3c_smem_bytes<T>(n, true) <= optin;
-  if (n > 32 && !pl.sm && k3c_smem_bytes<T>(n, false) > optin) return cudaErrorInvalidValue;
+  pl.k1b = n > 32 ? k1c_block<T>(n, optin) : 0;
+  pl.zrows = 0;
+  pl.zsplit = 1;
+  if (n > 32) {
+    // rows of Z that fit in shared memory next to the record buffers, at
+    // most 512 (one thread per row); the fewest CTAs per matrix that hold
+    // all rows, unless the caller asks for more
+    const size_t fixed = k3c_smem_bytes<T>(n, 0);
+    const size_t row = sizeof(T) * (size_t)(n | 1);
+    const int rmax = fixed < optin ? (int)std::min<size_t>(512, (optin - fixed) / row) : 0;
+    if (rmax >= 32 || rmax >= n) {
+      int split = (n + rmax - 1) / rmax;
+      const int want = opts ? opts->split : 0;
+      if (want > split) split = std::min(want, (n + 31) / 32);
+      pl.zsplit = split;
+      pl.zrows = (n + split - 1) / split;
+    } else if (fixed > optin) {
+      return cudaErrorInvalidValue;
+    }
+  }
+  const bool zglob = n > 32 && pl.zrows == 0;
   const size_t per = sizeof(T) * 2 * (size_t)n + sizeof(Meta) + sizeof(Rec<T>) * (size_t)pl.rcap +
-                     ((n > 32 && !pl.sm) ? sizeof(T) * (size_t)n * n : 0);
+                     (zglob ? sizeof(T) * (size_t)n * n : 0);
   long lc = (long)(kWsBudget / per);
   lc = std::max(lc, kMinChunk);
   if (opts && opts->chunk > 0) lc = opts->chunk;
@@ -124,7 +154,7 @@ cudaError_t make_plan(long L, int nm, int n, const DevProps &dp, Plan<T> &pl, co
   pl.off_rec = off;
   off = align256(off + sizeof(Rec<T>) * (size_t)pl.rcap * pl.Lc);
   pl.off_z = off;
-  if (n > 32 && !pl.sm) off = align256(off + sizeof(T) * (size_t)n * n * pl.Lc);
+  if (zglob) off = align256(off + sizeof(T) * (size_t)n * n * pl.Lc);
   pl.bytes = off;
   return cudaSuccess;
 }
@@ -181,31 +211,20 @@ template <class T> void launch_k1r(const KP<T> &p, unsigned blocks, size_t smem,
   else k1_reg<T, 4><<<blocks, 32 * 16, smem, st>>>(p);
 }
 
-template <class T> cudaError_t set_k1_smem(int n, bool sm, size_t bytes)
+template <class T> cudaError_t set_k1_smem(int n, size_t bytes)
 {
   const int sp = k1_split(n);
-  if (sm) {
-    if (sp == 4) return set_smem(k1_cta<T, true, 4>, bytes);
-    if (sp == 2) return set_smem(k1_cta<T, true, 2>, bytes);
-    return set_smem(k1_cta<T, true, 1>, bytes);
-  }
-  if (sp == 4) return set_smem(k1_cta<T, false, 4>, bytes);
-  if (sp == 2) return set_smem(k1_cta<T, false, 2>, bytes);
-  return set_smem(k1_cta<T, false, 1>, bytes);
+  if (sp == 4) return set_smem(k1_cta<T, 4>, bytes);
+  if (sp == 2) return set_smem(k1_cta<T, 2>, bytes);
+  return set_smem(k1_cta<T, 1>, bytes);
 }
 
-template <class T> void launch_k1(const KP<T> &p, bool sm, unsigned blocks, int nt, size_t smem, cudaStream_t st)
+template <class T> void launch_k1(const KP<T> &p, unsigned blocks, int nt, size_t smem, cudaStream_t st)
 {
   const int sp = k1_split(p.n);
-  if (sm) {
-    if (sp == 4) k1_cta<T, true, 4><<<blocks, nt, smem, st>>>(p);
-    else if (sp == 2) k1_cta<T, true, 2><<<blocks, nt, smem, st>>>(p);
-    else k1_cta<T, true, 1><<<blocks, nt, smem, st>>>(p);
-  } else {
-    if (sp == 4) k1_cta<T, false, 4><<<blocks, nt, smem, st>>>(p);
-    else if (sp == 2) k1_cta<T, false, 2><<<blocks, nt, smem, st>>>(p);
-    else k1_cta<T, false, 1><<<blocks, nt, smem, st>>>(p);
-  }
+  if (sp == 4) k1_cta<T, 4><<<blocks, nt, smem, st>>>(p);
+  else if (sp == 2) k1_cta<T, 2><<<blocks, nt, smem, st>>>(p);
+  else k1_cta<T, 1><<<blocks, nt, smem, st>>>(p);
 }
 
 template <class T>
@@ -265,11 +284,16 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const size_t k1w_smem = sizeof(T) * k1w_slot<T>() * K1W_NW;
   const size_t k3w_smem = sizeof(K3WSlot<T>) * K3W_NW;
   // phase 3: one row per thread up to 512 rows, two above
-  const int k3_nt = n > 512 ? (((n + 1) / 2 + 31) / 32) * 32 : ((n + 31) / 32) * 32;
+  const bool zsm = pl.zrows > 0;
+  const int k3_nt = zsm ? ((pl.zrows + 31) / 32) * 32
+                        : (n > 512 ? (((n + 1) / 2 + 31) / 32) * 32 : ((n + 31) / 32) * 32);
+  p.zrows = pl.zrows;
+  p.zsplit = pl.zsplit;
+  p.k1b = pl.k1b;
   const int k1c_nt = k1c_threads(n);
   const bool k1_in_regs = reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin;
-  const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems<T>(n, k1c_nt, pl.sm);
-  const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.sm);
+  const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems(n, k1c_nt, pl.k1b);
+  const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.zrows);
   int k2_tpb = 32;
   {
     const size_t per = k2_smem_per_thread<T>(n);
@@ -284,10 +308,10 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   } else {
     if (k1_in_regs) {
       if ((err = set_k1r_smem<T>(n, k1c_smem)) != cudaSuccess) return err;
-    } else if ((err = set_k1_smem<T>(n, pl.sm, k1c_smem)) != cudaSuccess) {
+    } else if ((err = set_k1_smem<T>(n, k1c_smem)) != cudaSuccess) {
       return err;
     }
-    if (pl.sm) {
+    if (zsm) {
       if ((err = set_smem(k3_cta<T, true, 1>, k3c_smem)) != cudaSuccess) return err;
     } else if ((err = set_smem(n > 512 ? k3_cta<T, false, 2> : k3_cta<T, false, 1>, k3c_smem)) != cudaSuccess) {
       return err;
@@ -309,7 +333,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     } else if (k1_in_regs) {
       launch_k1r<T>(p, (unsigned)lc, k1c_smem, stream);
     } else {
-      launch_k1<T>(p, pl.sm, (unsigned)lc, k1c_nt, k1c_smem, stream);
+      launch_k1<T>(p, (unsigned)lc, k1c_nt, k1c_smem, stream);
     }
     trace(chunk, 1, stream);
     k2_ql<T><<<(unsigned)((lc + k2_tpb - 1) / k2_tpb), k2_tpb, k2_smem, stream>>>(p);
@@ -317,8 +341,8 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     if (n <= 32) {
       const unsigned nb = (unsigned)((lc + K3W_NW - 1) / K3W_NW);
       k3_warp<T><<<nb, 32 * K3W_NW, k3w_smem, stream>>>(p);
-    } else if (pl.sm) {
-      k3_cta<T, true, 1><<<(unsigned)lc, k3_nt, k3c_smem, stream>>>(p);
+    } else if (zsm) {
+      k3_cta<T, true, 1><<<(unsigned)(lc * pl.zsplit), k3_nt, k3c_smem, stream>>>(p);
     } else if (n > 512) {
       k3_cta<T, false, 2><<<(unsigned)lc, k3_nt, k3c_smem, stream>>>(p);
     } else {

@@ -32,7 +32,8 @@ class EigenGError(RuntimeError):
 class Opts(ctypes.Structure):
     """eigen_GPU_batch_opts of include/eigen_GPU_batch.h."""
     _fields_ = [("method", ctypes.c_int), ("sort", ctypes.c_int), ("max_sweep", ctypes.c_int),
-                ("rec_cap", ctypes.c_int), ("chunk", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("rec_cap", ctypes.c_int), ("chunk", ctypes.c_int), ("split", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 def lib():
@@ -178,11 +179,11 @@ def eigen_GPU_batch(a, w, wk, n, nm=None, m=None, stream=None):
 
 
 def eigen_GPU_batch_ex(a, w, wk, n, nm=None, m=None, info=None, method=TQL2, sort=True, max_sweep=100,
-                       stream=None, rec_cap=0, chunk=0):
+                       stream=None, rec_cap=0, chunk=0, split=0):
     """Extended call; returns the cudaError_t status (0 on success)."""
     L, nm = _dims(a, n, nm)
     m = n if m is None else m
-    o = Opts(method, 1 if sort else 0, max_sweep, rec_cap, chunk)
+    o = Opts(method, 1 if sort else 0, max_sweep, rec_cap, chunk, split)
     lw = 0 if wk is None else wk.numel() * wk.element_size()
     return getattr(lib(), "eigen_GPU_batch_ex_" + _sfx(a.dtype))(
         L, nm, n, m, _ptr(a), _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), _stream(stream))
@@ -198,14 +199,15 @@ def eigen_GPU_batch_noalloc(a, w, n, nm=None, m=None, info=None, stream=None):
     return lib().eigen_GPU_batch_noalloc_DP(L, nm, n, m, _ptr(a), _ptr(w), _ptr(info), _stream(stream))
 
 
-def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=None, rec_cap=0, chunk=0):
+def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=None, rec_cap=0, chunk=0,
+          split=0):
     """Convenience wrapper: solves in place, returns (w, info)."""
     L, nm = _dims(a, n, nm)
     w = torch.empty((L, n), dtype=a.dtype, device=a.device)
     info = torch.zeros(L, dtype=torch.int32, device=a.device)
     if wk is None and method != JACOBI:
         wk = workspace(L, nm, n, a.dtype, a.device, rec_cap, chunk)
-    st = eigen_GPU_batch_ex(a, w, wk, n, nm, n, info, method, sort, max_sweep, stream, rec_cap, chunk)
+    st = eigen_GPU_batch_ex(a, w, wk, n, nm, n, info, method, sort, max_sweep, stream, rec_cap, chunk, split)
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
     return w, info

@@ -66,7 +66,11 @@ typedef struct eigen_GPU_batch_opts {
                     inside the apply phase, with identical results. */
   int chunk;     /* matrices per internal chunk; <= 0: automatic (workspace
                     about 4 GiB or 512 matrices).  Bounds the workspace. */
-  int reserved[3];
+  int split;     /* n > 32: thread blocks sharing one matrix's rows in the
+                    apply phase; <= 0: automatic (the fewest whose rows fit
+                    in shared memory).  Larger values trade re-reads of the
+                    rotation records for more warps per SM. */
+  int reserved[2];
 } eigen_GPU_batch_opts;
 
 /* Workspace bytes for eigen_GPU_batch_ex_* with these options (NULL:

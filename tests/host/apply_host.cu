@@ -1,5 +1,5 @@
-// Host build of the phase-3 wavefront (csrc/eigb_kernels.cuh: parse_group,
-// wave_apply) for CPU unit tests: applies a rotation record stream to a
+// Host build of the phase-3 apply (csrc/eigb_kernels.cuh: seg_walk,
+// seg_apply) for CPU unit tests: applies a rotation record stream to a
 // row-major n x n matrix, staging it in chunks of `ch` records exactly as
 // k3_cta does.
 #include "../../eigeng-batched_b200/csrc/eigb_kernels.cuh"
@@ -8,21 +8,21 @@ template <class T> static int run(int n, T *Z, const T *recs, int nrec, int ch)
 {
   using namespace eigb;
   const Rec<T> *src = reinterpret_cast<const Rec<T> *>(recs);
-  int base = 0, groups = 0;
+  int base = 0, segs = 0;
   while (base < nrec) {
     const int cnt = nrec - base < ch ? nrec - base : ch;
     const Rec<T> *rb = src + base;
+    const int used = seg_walk(rb, cnt);
     int q = 0;
-    while (true) {
-      int i0[K3_WAVE], len[K3_WAVE], off[K3_WAVE];
-      const int ns = parse_group(rb, cnt, q, i0, len, off);
-      if (ns == 0) break;
-      groups++;
-      for (int r = 0; r < n; r++) wave_apply<T, 1>(Z + r * n, 1, n, rb, i0, len, off, ns);
+    while (q < used) {
+      const int L = hdr_cnt(rb[q]), i0 = hdr_i0(rb[q]);
+      for (int r = 0; r < n; r++) seg_apply<T, 1>(Z + r * n, 1, rb + q + 1, i0, L);
+      q += 1 + L;
+      segs++;
     }
-    base += q > 0 ? q : cnt;
+    base += used > 0 ? used : cnt;
   }
-  return groups;
+  return segs;
 }
 
 extern "C" int host_apply_d(int n, double *Z, const double *recs, int nrec, int ch) { return run<double>(n, Z, recs, nrec, ch); }

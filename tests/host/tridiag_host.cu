@@ -33,33 +33,42 @@ template <class T> struct HostTeam {
   }
 };
 
-template <class T, int SPLIT> static void run(int n, int nthr, T *S, int ld, T *d, T *e)
+// The matrix (full symmetric, column-major, leading dimension ldg) is in G;
+// its leading B x B block is moved to a separate "shared" array for the run
+// and back afterwards, as k1_cta stages it.
+template <class T, int SPLIT> static void run(int n, int nthr, T *G, int ldg, int B, T *d, T *e)
 {
   HostShared<T> sh(nthr);
-  std::vector<T> beta(n + 1), pv(n + 1), part(nthr), red(72);
+  const int ld = B | 1;
+  std::vector<T> beta(n + 1), pv(n + 1), part(nthr), red(72), S((size_t)B * ld + 1);
+  for (int c = 0; c < B; c++)
+    for (int r = 0; r < B; r++) S[r + (size_t)c * ld] = G[r + (size_t)c * ldg];
   std::vector<std::thread> th;
   for (int t = 0; t < nthr; t++)
     th.emplace_back([&, t]() {
       HostTeam<T> tm{t, nthr, 0, &sh};
-      eigb::tridiag_qt<T, SPLIT>(tm, S, ld, n, d, e, beta.data(), pv.data(), part.data(), red.data());
+      eigb::tridiag_qt<T, SPLIT>(tm, S.data(), ld, G, ldg, B, n, d, e, beta.data(), pv.data(), part.data(),
+                                 red.data());
     });
   for (auto &x : th) x.join();
+  for (int c = 0; c < B; c++)
+    for (int r = 0; r < B; r++) G[r + (size_t)c * ldg] = S[r + (size_t)c * ld];
 }
 
-template <class T> static void run_split(int n, int nthr, int split, T *S, int ld, T *d, T *e)
+template <class T> static void run_split(int n, int nthr, int split, T *S, int ld, int B, T *d, T *e)
 {
-  if (split == 4) run<T, 4>(n, nthr, S, ld, d, e);
-  else if (split == 2) run<T, 2>(n, nthr, S, ld, d, e);
-  else run<T, 1>(n, nthr, S, ld, d, e);
+  if (split == 4) run<T, 4>(n, nthr, S, ld, B, d, e);
+  else if (split == 2) run<T, 2>(n, nthr, S, ld, B, d, e);
+  else run<T, 1>(n, nthr, S, ld, B, d, e);
 }
 
-extern "C" void host_tridiag_d(int n, int nthr, int split, double *S, int ld, double *d, double *e)
+extern "C" void host_tridiag_d(int n, int nthr, int split, double *S, int ld, int B, double *d, double *e)
 {
-  run_split<double>(n, nthr, split, S, ld, d, e);
+  run_split<double>(n, nthr, split, S, ld, B, d, e);
 }
-extern "C" void host_tridiag_f(int n, int nthr, int split, float *S, int ld, float *d, float *e)
+extern "C" void host_tridiag_f(int n, int nthr, int split, float *S, int ld, int B, float *d, float *e)
 {
-  run_split<float>(n, nthr, split, S, ld, d, e);
+  run_split<float>(n, nthr, split, S, ld, B, d, e);
 }
 
 // register-resident variant: one "thread" per GPU thread of the CTA

@@ -23,9 +23,10 @@ def E():
     return eigeng_b200
 
 
-def gpu_solve(a0, n, nm=None, method=0, sort=True, max_sweep=100, rec_cap=0, chunk=0):
+def gpu_solve(a0, n, nm=None, method=0, sort=True, max_sweep=100, rec_cap=0, chunk=0, split=0):
     a = torch.from_numpy(np.ascontiguousarray(a0)).cuda()
-    w, info = E().solve(a, n, nm, method=method, sort=sort, max_sweep=max_sweep, rec_cap=rec_cap, chunk=chunk)
+    w, info = E().solve(a, n, nm, method=method, sort=sort, max_sweep=max_sweep, rec_cap=rec_cap, chunk=chunk,
+                        split=split)
     torch.cuda.synchronize()
     return w.cpu().numpy(), a.cpu().numpy(), info.cpu().numpy()
 
@@ -76,6 +77,25 @@ def test_parity_with_oracle(oracle_mod, n, dtype, method):
         assert (np.abs(w - wl) <= 64 * n * eps * scale).all()
         res, orth = O.residuals(a0, w, z, n)
         assert res.max() < 2e-11 and orth.max() < 2e-11
+
+
+@pytest.mark.parametrize("n,dtype", [(1024, np.float64), (1024, np.float32), (700, np.float64), (513, np.float64)])
+def test_largest_sizes(oracle_mod, n, dtype):
+    """Up to the size limit n = 1024: Z kept in the workspace (large FP64),
+    several row blocks per matrix in shared memory, two rows per thread,
+    phase 1 with most of the matrix outside shared memory."""
+    O = oracle_mod
+    a0 = O.sym_uniform(2, n, seed=n).astype(dtype)
+    w, z, info = gpu_solve(a0, n)
+    assert (info == 0).all()
+    eps = np.finfo(dtype).eps
+    wl, _ = O.lapack_eigh(a0.astype(np.float64), n)
+    scale = np.abs(wl).max(axis=1, keepdims=True)
+    assert (np.abs(w - wl) <= 64 * n * eps * scale).all()
+    res, orth = O.residuals(a0.astype(np.float64), w.astype(np.float64), z.astype(np.float64), n)
+    assert res.max() < 256 * n * eps and orth.max() < 256 * n * eps, (res.max(), orth.max())
+    e1, e2, fl = device_gate(a0, w, z, n)
+    assert (fl == 0).all(), (e1, e2)
 
 
 @pytest.mark.parametrize("n", [4, 16, 32, 33, 64, 128])
@@ -264,6 +284,22 @@ def test_record_overflow_path_is_identical(oracle_mod, n, method):
     assert np.array_equal(i1, i2)
     assert np.array_equal(w1, w2)
     assert np.array_equal(z1, z2)
+
+
+@pytest.mark.parametrize("n,nm", [(40, 40), (100, 103), (200, 200), (256, 256)])
+def test_apply_row_split_is_bit_identical(oracle_mod, n, nm):
+    """The apply phase may split a matrix's rows over several thread blocks
+    (each applies every rotation to its own rows): results do not depend
+    on the split, with or without the in-kernel regeneration path."""
+    O = oracle_mod
+    a0 = np.zeros((6, n, nm))
+    a0[:, :, :n] = O.sym_uniform(6, n, seed=n + 3)
+    w1, z1, i1 = gpu_solve(a0, n, nm)
+    for split in (2, 3, 5):
+        w2, z2, i2 = gpu_solve(a0, n, nm, split=split)
+        assert np.array_equal(w1, w2) and np.array_equal(z1, z2) and np.array_equal(i1, i2), split
+    w3, z3, i3 = gpu_solve(a0, n, nm, split=3, rec_cap=4 * n)   # records overflow: regenerated per block
+    assert np.array_equal(w1, w3) and np.array_equal(z1, z3) and np.array_equal(i1, i3)
 
 
 def test_chunked_batch_and_determinism(oracle_mod):

@@ -36,7 +36,7 @@ def hostlibs():
         f = getattr(libs["ql_host"], "host_ql_fast" + s)
         f.argtypes = [I, P, P, I, I, I, P, P, P]
         f.restype = I
-        getattr(libs["tridiag_host"], "host_tridiag" + s).argtypes = [I, I, I, P, I, P, P]
+        getattr(libs["tridiag_host"], "host_tridiag" + s).argtypes = [I, I, I, P, I, I, P, P]
         getattr(libs["tridiag_host"], "host_tridiag_reg" + s).argtypes = [I, P, I, P, P]
         getattr(libs["apply_host"], "host_apply" + s).argtypes = [I, P, P, I, I]
         getattr(libs["apply_host"], "host_apply" + s).restype = I
@@ -134,11 +134,17 @@ def test_ql_sweep_limit_reports_index(oracle_mod, hostlibs):
     assert st == 0 and ierr == 1
 
 
-@pytest.mark.parametrize("n,nthr,split", [(2, 32, 1), (3, 32, 1), (8, 32, 1), (32, 32, 1), (33, 64, 1), (64, 64, 1),
-                                          (100, 128, 1), (64, 96, 1), (33, 256, 4), (64, 256, 4), (100, 512, 4),
-                                          (77, 192, 2), (128, 512, 4)])
+@pytest.mark.parametrize("n,nthr,split,blk", [(2, 32, 1, 2), (3, 32, 1, 3), (8, 32, 1, 8), (32, 32, 1, 32),
+                                              (33, 64, 1, 33), (64, 64, 1, 64), (100, 128, 1, 100), (64, 96, 1, 64),
+                                              (33, 256, 4, 33), (64, 256, 4, 64), (100, 512, 4, 100),
+                                              (77, 192, 2, 77), (128, 512, 4, 128),
+                                              # leading block in "shared memory", outer band in G
+                                              (100, 512, 4, 60), (77, 192, 2, 1), (64, 256, 4, 0),
+                                              (96, 128, 1, 95), (130, 640, 4, 100)])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, split, dtype):
+def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, split, blk, dtype):
+    """Phase 1 (eigb_tridiag.cuh) with the whole matrix, part of it or none
+    of it in the shared-memory array."""
     O = oracle_mod
     a0 = O.sym_uniform(1, n, seed=n)[0].astype(dtype)
     ld = n | 1
@@ -147,7 +153,7 @@ def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, split, dtype):
     d = np.zeros(n, dtype)
     e = np.zeros(n, dtype)
     f = hostlibs["tridiag_host"].host_tridiag_d if dtype == np.float64 else hostlibs["tridiag_host"].host_tridiag_f
-    f(n, nthr, split, _p(S), ld, _p(d), _p(e))
+    f(n, nthr, split, _p(S), ld, blk, _p(d), _p(e))
     eps = np.finfo(dtype).eps
     scale = np.abs(a0).max() * n
     M = S[:, :n].T.astype(np.float64)     # M[r, c] with r = row
@@ -167,7 +173,7 @@ def test_tridiag_team_code(oracle_mod, hostlibs, n, nthr, split, dtype):
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_tridiag_register_variant(oracle_mod, hostlibs, n, nm, dtype):
     """The register-resident phase 1 (eigb_tridiag_reg.cuh): reads the upper
-    triangle of a (nm x n, column-major), leaves M = Q^T in its place."""
+    triangle of a (nm x n, column-major), leaves Q (A = Q T Q^T) in its place."""
     O = oracle_mod
     a0 = O.sym_uniform(1, n, seed=n + 1)[0].astype(dtype)
     A = np.full((n, nm), np.nan, dtype)  # A[c, r] = element (r, c)
@@ -180,8 +186,7 @@ def test_tridiag_register_variant(oracle_mod, hostlibs, n, nm, dtype):
     f(n, _p(A), nm, _p(d), _p(e))
     eps = np.finfo(dtype).eps
     scale = np.abs(a0).max() * n
-    M = A[:, :n].T.astype(np.float64)
-    Q = M.T
+    Q = A[:, :n].T.astype(np.float64)
     T = np.diag(d.astype(np.float64)) + np.diag(e[:-1].astype(np.float64), 1) + np.diag(e[:-1].astype(np.float64), -1)
     assert np.abs(Q @ T @ Q.T - a0).max() <= 64 * eps * scale
     assert np.abs(Q.T @ Q - np.eye(n)).max() <= 64 * eps * n
@@ -218,10 +223,10 @@ def test_fast_generator_is_bit_identical(oracle_mod, hostlibs, n, method, dtype)
 @pytest.mark.parametrize("n", [3, 8, 17, 33, 64, 100])
 @pytest.mark.parametrize("method", [0, 1])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_wavefront_apply_matches_sequential(oracle_mod, hostlibs, n, method, dtype):
-    """Phase 3 applies groups of sweeps as a skewed pipeline (identity
-    outside each sweep's range); the result equals applying every rotation
-    in order, also when the stream is staged in small chunks."""
+def test_pipelined_apply_matches_sequential(oracle_mod, hostlibs, n, method, dtype):
+    """Phase 3 applies each sweep as one rotation chain whose operands are
+    loaded a block ahead; the result equals applying every rotation in
+    order, also when the stream is staged in small chunks."""
     O = oracle_mod
     a0 = O.sym_uniform(1, n, seed=7 * n + method)[0].astype(dtype)
     d, e = tred(O, a0, n)
@@ -236,6 +241,6 @@ def test_wavefront_apply_matches_sequential(oracle_mod, hostlibs, n, method, dty
     eps = np.finfo(dtype).eps
     for ch in (4 * (n + 1), n + 1, 10 ** 6):
         z = np.ascontiguousarray(q0.copy())
-        groups = f(n, _p(z), _p(flat), flat.shape[0], ch)
-        assert groups > 0
+        segs = f(n, _p(z), _p(flat), flat.shape[0], ch)
+        assert segs > 0
         assert np.abs(z - ref).max() <= 64 * n * eps * np.abs(ref).max()
