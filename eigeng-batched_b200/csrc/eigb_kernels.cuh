@@ -38,6 +38,7 @@ template <class T> struct KP {
   int k1b;       // phase 1 (CTA form): leading block kept in shared memory
   int zrows;     // phase 3 with Z in shared memory: rows per CTA ...
   int zsplit;    // ... and CTAs per matrix
+  int k2mpw;     // phase 2: matrices per warp (1..32)
   int *info;     // optional per-matrix status for the caller (may be null)
   long Lc;       // matrices in this chunk
   int n, nm;
@@ -48,6 +49,7 @@ template <class T> struct KP {
 };
 
 constexpr int K1W_NW = 4;       // warps (matrices) per CTA in k1_warp
+constexpr int K2_MAX_WARPS = 8; // warps per CTA in k2_ql at most
 constexpr int K1W_LD = 33;      // padded leading dimension, odd
 constexpr int K3W_NW = 4;       // warps per CTA in k3_warp
 constexpr int K3W_CH = 128;     // records staged per warp
@@ -167,14 +169,21 @@ __global__ void __launch_bounds__(32 * NB * NB, 1) k1_reg(const KP<T> p)
 
 // ---------------------------------------------------------------- phase 2
 template <class T>
-__global__ void k2_ql(const KP<T> p)
+__global__ void __launch_bounds__(K2_MAX_WARPS * 32) k2_ql(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int st = blockDim.x;
-  const long k = (long)blockIdx.x * st + threadIdx.x;
-  if (k >= p.Lc) return;  // no barriers in this kernel
+  // lanes 0 .. k2mpw-1 of each warp run one matrix each: fewer matrices
+  // per warp spread a small batch over more warps (the chains are serial,
+  // so time follows the slowest lane of a warp, and lanes diverge)
+  const int mpw = p.k2mpw;
+  const int lane = threadIdx.x & 31;
+  if (lane >= mpw) return;  // no barriers in this kernel
+  const int st = (blockDim.x >> 5) * mpw;  // matrices per block
+  const int slot = (threadIdx.x >> 5) * mpw + lane;
+  const long k = (long)blockIdx.x * st + slot;
+  if (k >= p.Lc) return;
   const int n = p.n;
-  T *dd = reinterpret_cast<T *>(smem_raw) + threadIdx.x;
+  T *dd = reinterpret_cast<T *>(smem_raw) + slot;
   T *ee = dd + (size_t)n * st;
   const T *din = p.d + k * n;
   const T *ein = p.e + k * n;
@@ -410,48 +419,68 @@ constexpr int K3_U = 8;
     OUT = y_;                                     \
   }
 
+// block of K3_U columns starting COFF below p, and its records from rp[RI]
+#define EIGB_LOAD(ZB, RB, COFF, RI)                  \
+  {                                                  \
+    _Pragma("unroll") for (int u = 0; u < K3_U; u++) \
+    {                                                \
+      ZB[u] = p[-((COFF) + u) * cs];                 \
+      RB[u] = rp[(RI) + u];                          \
+    }                                                \
+  }
+// a block: the products that do not depend on the carried value first,
+// then the chain, in which each rotation waits for a single fma
+#define EIGB_BLOCK(ZB, RB)                                       \
+  {                                                              \
+    T cz_[K3_U], sz_[K3_U];                                      \
+    _Pragma("unroll") for (int u = 0; u < K3_U; u++)             \
+    {                                                            \
+      cz_[u] = RB[u].c * ZB[u];                                  \
+      sz_[u] = RB[u].s * ZB[u];                                  \
+    }                                                            \
+    _Pragma("unroll") for (int u = 0; u < K3_U; u++)             \
+    {                                                            \
+      const T y_ = fma(RB[u].c, h, sz_[u]);                      \
+      h = fma(-RB[u].s, h, cz_[u]);                              \
+      p[(1 - u) * cs] = y_;                                      \
+    }                                                            \
+    p -= K3_U * cs;                                              \
+  }
+
 // One segment: rotations i0, i0-1, ..., i0-len+1 (records rp[0..len)) on a
 // row whose column c is zr[c*cs].  Rotation i replaces (z_i, z_{i+1}) by
 // (c z_i - s z_{i+1}, s z_i + c z_{i+1}); z_{i+1} is carried in h, which
-// enters as column i0+1 and leaves as column i0-len+1.
+// enters as column i0+1 and leaves as column i0-len+1.  Blocks of K3_U
+// rotations alternate between two register sets: while one block is
+// applied, the next one's columns and records are already being loaded
+// (they lie below every column the current block stores).
 template <class T, int CS>
 __host__ __device__ __forceinline__ void seg_apply(T *__restrict__ zr, const int cs_rt,
                                                    const Rec<T> *__restrict__ rp, const int i0, const int len)
 {
   const int cs = CS > 0 ? CS : cs_rt;
-  T *p = zr + i0 * cs;  // column of the next rotation's z_i
+  T *p = zr + i0 * cs;  // column of the next rotation's z_i (rotation j of the segment)
   T h = p[cs];
   int j = 0;
-  if (len >= 2 * K3_U) {
-    T z[K3_U];
-    Rec<T> r[K3_U];
-#pragma unroll
-    for (int u = 0; u < K3_U; u++) {
-      z[u] = p[-u * cs];
-      r[u] = rp[u];
+  if (len >= K3_U) {
+    T za[K3_U], zb[K3_U];
+    Rec<T> ra[K3_U], rb[K3_U];
+    EIGB_LOAD(za, ra, 0, 0)  // invariant: za/ra hold block j, j + K3_U <= len, p at rotation j
+    for (; j + 3 * K3_U <= len; j += 2 * K3_U) {
+      EIGB_LOAD(zb, rb, K3_U, j + K3_U)
+      EIGB_BLOCK(za, ra)
+      EIGB_LOAD(za, ra, K3_U, j + 2 * K3_U)  // p is at rotation j + K3_U now
+      EIGB_BLOCK(zb, rb)
     }
-    for (; j + 2 * K3_U <= len; j += K3_U) {
-      T zn[K3_U];
-      Rec<T> rn[K3_U];
-#pragma unroll
-      for (int u = 0; u < K3_U; u++) {
-        zn[u] = p[-(K3_U + u) * cs];  // columns below every store of this block
-        rn[u] = rp[j + K3_U + u];
-      }
-#pragma unroll
-      for (int u = 0; u < K3_U; u++) EIGB_CHAIN(r[u], z[u], p[(1 - u) * cs])
-      p -= K3_U * cs;
-#pragma unroll
-      for (int u = 0; u < K3_U; u++) {
-        z[u] = zn[u];
-        r[u] = rn[u];
-      }
+    if (j + 2 * K3_U <= len) {
+      EIGB_LOAD(zb, rb, K3_U, j + K3_U)
+      EIGB_BLOCK(za, ra)
+      EIGB_BLOCK(zb, rb)
+      j += 2 * K3_U;
+    } else {
+      EIGB_BLOCK(za, ra)
+      j += K3_U;
     }
-    // j + K3_U <= len: the block in registers is still inside the segment
-#pragma unroll
-    for (int u = 0; u < K3_U; u++) EIGB_CHAIN(r[u], z[u], p[(1 - u) * cs])
-    p -= K3_U * cs;
-    j += K3_U;
   }
   for (; j < len; j++, p -= cs) {
     const T z0 = p[0];
@@ -459,6 +488,8 @@ __host__ __device__ __forceinline__ void seg_apply(T *__restrict__ zr, const int
   }
   p[cs] = h;
 }
+#undef EIGB_LOAD
+#undef EIGB_BLOCK
 #undef EIGB_CHAIN
 
 // End of the last complete segment (header + rotations) in rbuf[0..cnt).
@@ -503,7 +534,7 @@ __device__ __forceinline__ void apply_chunk(const Rec<T> *rbuf, const int used, 
 // column-major, Z(r, c) at Z[r + c*n], so that a warp's accesses at a fixed
 // column are coalesced.
 template <class T, bool SM, int RPT>
-__global__ void __launch_bounds__(512) k3_cta(const KP<T> p)
+__global__ void __launch_bounds__(SM ? 256 : 512, 1) k3_cta(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int zsplit = SM ? p.zsplit : 1;

@@ -56,6 +56,51 @@ __host__ __device__ __forceinline__ T dot_col(const T *__restrict__ Sr, const in
   return (a0 + a1) + (a2 + a3);
 }
 
+// The update loops below load a batch of row elements before storing any:
+// a store to Sr[k] followed by the load of Sr[k+1] cannot be reordered by
+// the compiler, which would otherwise expose one full memory latency per
+// element (L2 latency for the part of the matrix in global memory).
+constexpr int TQ_BATCH = 8;
+
+// Sr[k] += u_k * wr + (alpha u_k + p_k) * ur for k in [lo, hi)
+template <class T>
+__host__ __device__ __forceinline__ void rank2_row(T *__restrict__ Sr, const size_t ld, const T *__restrict__ u,
+                                                   const T *__restrict__ pv, const T alpha, const T ur, const T wr,
+                                                   int lo, const int hi)
+{
+  for (; lo + TQ_BATCH <= hi; lo += TQ_BATCH) {
+    T a[TQ_BATCH];
+#pragma unroll
+    for (int q = 0; q < TQ_BATCH; q++) a[q] = Sr[(size_t)(lo + q) * ld];
+#pragma unroll
+    for (int q = 0; q < TQ_BATCH; q++) {
+      const T uk = u[lo + q];
+      const T wk = fma(alpha, uk, pv[lo + q]);
+      Sr[(size_t)(lo + q) * ld] = fma(wk, ur, fma(uk, wr, a[q]));
+    }
+  }
+  for (; lo < hi; lo++) {
+    const T uk = u[lo];
+    const T wk = fma(alpha, uk, pv[lo]);
+    Sr[(size_t)lo * ld] = fma(wk, ur, fma(uk, wr, Sr[(size_t)lo * ld]));
+  }
+}
+
+// Sr[k] += q u_k for k in [lo, hi)
+template <class T>
+__host__ __device__ __forceinline__ void axpy_row(T *__restrict__ Sr, const size_t ld, const T *__restrict__ u,
+                                                  const T q, int lo, const int hi)
+{
+  for (; lo + TQ_BATCH <= hi; lo += TQ_BATCH) {
+    T a[TQ_BATCH];
+#pragma unroll
+    for (int j = 0; j < TQ_BATCH; j++) a[j] = Sr[(size_t)(lo + j) * ld];
+#pragma unroll
+    for (int j = 0; j < TQ_BATCH; j++) Sr[(size_t)(lo + j) * ld] = fma(q, u[lo + j], a[j]);
+  }
+  for (; lo < hi; lo++) Sr[(size_t)lo * ld] = fma(q, u[lo], Sr[(size_t)lo * ld]);
+}
+
 // Storage of tridiag_qt: element (r, c) is S[r + c*ld] (shared memory) when
 // r < B and c < B, else G[r + c*ldg] (global memory).  B = n keeps the whole
 // matrix in shared memory, B = 0 none of it; in between, the leading B x B
@@ -150,18 +195,8 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, T *G, const in
     if (r < i) {
       const T wr = fma(alpha, ur, pr);
       const int mid = max(lo, min(hi, Br));
-      size_t off = (size_t)lo * ld;
-      for (int k = lo; k < mid; k++, off += ld) {
-        const T uk = ucol[k];
-        const T wk = fma(alpha, uk, pv[k]);
-        Sr[off] = fma(wk, ur, fma(uk, wr, Sr[off]));
-      }
-      off = (size_t)mid * ldg;
-      for (int k = mid; k < hi; k++, off += ldg) {
-        const T uk = ucol[k];
-        const T wk = fma(alpha, uk, pv[k]);
-        Gr[off] = fma(wk, ur, fma(uk, wr, Gr[off]));
-      }
+      rank2_row(Sr, (size_t)ld, ucol, pv, alpha, ur, wr, lo, mid);
+      rank2_row(Gr, (size_t)ldg, ucol, pv, alpha, ur, wr, mid, hi);
     }
     // the barrier in the next step's first sum() orders these updates
   }
@@ -194,8 +229,8 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, T *G, const in
         part[h * nr + r] = q;
       } else {
         q *= bk;
-        for (int c = lo; c < mid; c++) Sr[(size_t)c * ld] = fma(q, ucol[c], Sr[(size_t)c * ld]);
-        for (int c = mid; c < hi; c++) Gr[(size_t)c * ldg] = fma(q, ucol[c], Gr[(size_t)c * ldg]);
+        axpy_row(Sr, (size_t)ld, ucol, q, lo, mid);
+        axpy_row(Gr, (size_t)ldg, ucol, q, mid, hi);
       }
     }
     if (SPLIT > 1) {
@@ -205,8 +240,8 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, T *G, const in
 #pragma unroll
         for (int s = 0; s < SPLIT; s++) q += part[s * nr + r];
         q *= bk;
-        for (int c = lo; c < mid; c++) Sr[(size_t)c * ld] = fma(q, ucol[c], Sr[(size_t)c * ld]);
-        for (int c = mid; c < hi; c++) Gr[(size_t)c * ldg] = fma(q, ucol[c], Gr[(size_t)c * ldg]);
+        axpy_row(Sr, (size_t)ld, ucol, q, lo, mid);
+        axpy_row(Gr, (size_t)ldg, ucol, q, mid, hi);
       }
     }
     tm.sync();  // column k is overwritten by the next extension; part is reused

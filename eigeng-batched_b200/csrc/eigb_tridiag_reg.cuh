@@ -48,13 +48,17 @@ __host__ __device__ __forceinline__ void ld2(const T *p, T &a, T &b)
   b = v.y;
 }
 
+// Reflectors applied per barrier in the formation of M.
+constexpr int QB = 4;
+
 template <int NB> struct RegLayout {
   static constexpr int NR = 32 * NB;
   static constexpr int NT = NR * NB;
 };
 
 // Shared-memory elements of tridiag_qt_reg: V (max(n*NR, n*(n|1)), also the
-// staging area of the input and of the output), part[2*NB*NR], pv[NR], beta[NR], red[72].
+// staging area of the input and of the output), part[2*QB*NB*NR], pv[NR],
+// beta[NR], red[72], gram[3*NR].
 // Offset of the arrays after V, rounded to 4 elements so that the paired
 // loads of V and pv stay aligned for every n.
 template <int NB> __host__ __device__ inline size_t reg_voff(int n)
@@ -66,7 +70,7 @@ template <int NB> __host__ __device__ inline size_t reg_voff(int n)
 template <int NB> __host__ __device__ inline size_t reg_smem_elems(int n)
 {
   constexpr int NR = RegLayout<NB>::NR;
-  return reg_voff<NB>(n) + 2 * (size_t)NB * NR + 2 * (size_t)NR + 72;
+  return reg_voff<NB>(n) + 2 * (size_t)QB * NB * NR + 2 * (size_t)NR + 72 + 3 * (size_t)NR;
 }
 
 // A: the input matrix (upper triangle used), overwritten with Q (A = Q T Q^T).
@@ -82,9 +86,10 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   const int lds = n | 1;
   T *V = sm;
   T *part = sm + reg_voff<NB>(n);
-  T *pv = part + 2 * NB * NR;
+  T *pv = part + 2 * QB * NB * NR;
   T *beta_s = pv + NR;
   T *red = beta_s + NR;
+  T *gram = red + 72;  // gram[3k + d - 1] = u_k . u_{k+d}
 
   // ---- stage the upper triangle, then build the register slices ----
   for (int idx = t; idx < n * n; idx += tm.size()) {
@@ -173,42 +178,83 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   if (t == 0) e_out[n - 1] = T(0);
 
   // ---- M = H_1 ... H_{n-1}: M <- M + beta_k (M u_k) u_k^T from M = I ----
+  // QB reflectors per barrier.  With a_j = M u_j for the M before the
+  // block (all QB products in one exchange of partial sums), applying
+  // u_0 .. u_3 in order is M += sum_j q_j u_j^T with
+  //   q_j = beta_j (a_j + sum_{i<j} q_i (u_i . u_j)),
+  // a recurrence per row on the Gram entries of the block, computed here
+  // once for all k (each thread one pair; its walk over c starts at its
+  // lane so that the threads of a warp read different banks).
+  for (int idx = t; idx < 3 * n; idx += tm.size()) {
+    const int k = idx / 3, d = idx % 3 + 1;
+    T g = T(0);
+    if (k >= 1 && k + d < n) {
+      const T *u = V + (size_t)k * NR, *v = V + (size_t)(k + d) * NR;
+      int c = lane % k;
+      for (int j = 0; j < k; j++) {
+        g = fma(u[c], v[c], g);
+        c = (c + 1 == k) ? 0 : c + 1;
+      }
+    }
+    gram[idx] = g;
+  }
   T *Mr = S;
 #pragma unroll
   for (int c = 0; c < 32; c++) Mr[c] = (c0 + c == r) ? T(1) : T(0);
-  for (int k = 1; k < n; k++) {
-    const T bk = beta_s[k];
-    const T *Vk = V + (size_t)k * NR;
-    T *pb = part + (k & 1) * NB * NR;  // double buffer: one barrier per step
-    const bool act = (c0 < k) && (32 * rb < k);
+  tm.sync();
+  for (int k0 = 1, blk = 0; k0 < n; k0 += QB, blk++) {
+    const int kl = min(k0 + QB - 1, n - 1);  // last reflector of the block
+    T *pb = part + (blk & 1) * QB * NB * NR;  // double buffer: one barrier per block
+    const bool act = (c0 < kl) && (32 * rb < kl);
     if (act) {
-      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
 #pragma unroll
-      for (int c = 0; c < 32; c += 4) {
-        T v0, v1, v2, v3;
-        ld2(Vk + c0 + c, v0, v1);
-        ld2(Vk + c0 + c + 2, v2, v3);
-        a0 = fma(Mr[c + 0], v0, a0);
-        a1 = fma(Mr[c + 1], v1, a1);
-        a2 = fma(Mr[c + 2], v2, a2);
-        a3 = fma(Mr[c + 3], v3, a3);
+      for (int j = 0; j < QB; j++) {
+        T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+        if (k0 + j <= kl) {
+          const T *Vk = V + (size_t)(k0 + j) * NR;
+#pragma unroll
+          for (int c = 0; c < 32; c += 4) {
+            T v0, v1, v2, v3;
+            ld2(Vk + c0 + c, v0, v1);
+            ld2(Vk + c0 + c + 2, v2, v3);
+            a0 = fma(Mr[c + 0], v0, a0);
+            a1 = fma(Mr[c + 1], v1, a1);
+            a2 = fma(Mr[c + 2], v2, a2);
+            a3 = fma(Mr[c + 3], v3, a3);
+          }
+        }
+        pb[(j * NB + cb) * NR + r] = (a0 + a1) + (a2 + a3);
       }
-      pb[cb * NR + r] = (a0 + a1) + (a2 + a3);
     }
     tm.sync();
     if (act) {
-      const int nact = (k + 31) >> 5;
-      T q = T(0);
+      const int nact = (kl + 31) >> 5;
+      T q[QB];
 #pragma unroll
-      for (int s = 0; s < NB; s++)
-        if (s < nact) q += pb[s * NR + r];
-      q *= bk;
+      for (int j = 0; j < QB; j++) {
+        T a = T(0);
 #pragma unroll
-      for (int c = 0; c < 32; c += 2) {
-        T v0, v1;
-        ld2(Vk + c0 + c, v0, v1);
-        Mr[c] = fma(q, v0, Mr[c]);
-        Mr[c + 1] = fma(q, v1, Mr[c + 1]);
+        for (int s = 0; s < NB; s++)
+          if (s < nact) a += pb[(j * NB + s) * NR + r];
+        if (k0 + j <= kl) {
+#pragma unroll
+          for (int i2 = 0; i2 < j; i2++) a = fma(q[i2], gram[3 * (k0 + i2) + (j - i2) - 1], a);
+          q[j] = beta_s[k0 + j] * a;
+        } else {
+          q[j] = T(0);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < QB; j++) {
+        if (k0 + j > kl) break;
+        const T *Vk = V + (size_t)(k0 + j) * NR;
+#pragma unroll
+        for (int c = 0; c < 32; c += 2) {
+          T v0, v1;
+          ld2(Vk + c0 + c, v0, v1);
+          Mr[c] = fma(q[j], v0, Mr[c]);
+          Mr[c + 1] = fma(q[j], v1, Mr[c + 1]);
+        }
       }
     }
   }

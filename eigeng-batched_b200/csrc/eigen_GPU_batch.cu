@@ -24,7 +24,7 @@ namespace eigb {
 namespace {
 
 constexpr int kMaxDev = 64;
-constexpr size_t kWsBudget = (size_t)4 << 30;  // workspace target per call
+constexpr size_t kWsBudget = (size_t)8 << 30;  // workspace target per call
 constexpr long kMinChunk = 512;
 
 struct DevProps {
@@ -77,17 +77,32 @@ inline void trace(long chunk, int slot, cudaStream_t stream)
 }
 
 inline int k1c_threads(int n) { return std::min(1024, ((n + 31) / 32) * 32 * k1_split(n)); }
-// leading block of phase 1 (CTA form) held in shared memory: the largest
-// that fits next to the scratch arrays, at most n
+// leading block of phase 1 (CTA form) held in shared memory: the whole
+// matrix when it fits; otherwise the largest that fits next to the scratch
+// arrays, for FP64 at most 128 x 128, which leaves L1 room for the outer
+// band (measured on B200 at n = 200 and 256: 15-20 % faster than the
+// largest block; FP32 is fastest with the largest)
 template <class T> int k1c_block(int n, size_t optin)
 {
   const size_t base = sizeof(T) * k1c_smem_elems(n, k1c_threads(n), 0);
   if (base >= optin) return 0;
   int B = n;
+  if (sizeof(T) == 8 && base + sizeof(T) * (size_t)n * (size_t)(n | 1) > optin) B = std::min(n, 128);
   while (B > 0 && base + sizeof(T) * (size_t)B * (size_t)(B | 1) > optin) B--;
   return B;
 }
 template <class T> size_t k2_smem_per_thread(int n) { return sizeof(T) * 2 * (size_t)n; }
+
+// Phase 2 matrices per warp: the largest power of two that still gives
+// each SM about three warps (measured on B200: 8 per warp for 4096
+// matrices, 32 for 16384).
+inline int k2_mpw(long L, int sms)
+{
+  const long target = 3L * sms;
+  int m = 32;
+  while (m > 1 && (L + m - 1) / m < target) m >>= 1;
+  return m;
+}
 
 // Layout of the workspace for one chunk of Lc matrices.
 template <class T> struct Plan {
@@ -122,11 +137,11 @@ cudaError_t make_plan(long L, int nm, int n, const DevProps &dp, Plan<T> &pl, co
   pl.zsplit = 1;
   if (n > 32) {
     // rows of Z that fit in shared memory next to the record buffers, at
-    // most 512 (one thread per row); the fewest CTAs per matrix that hold
+    // most 256 (one thread per row); the fewest CTAs per matrix that hold
     // all rows, unless the caller asks for more
     const size_t fixed = k3c_smem_bytes<T>(n, 0);
     const size_t row = sizeof(T) * (size_t)(n | 1);
-    const int rmax = fixed < optin ? (int)std::min<size_t>(512, (optin - fixed) / row) : 0;
+    const int rmax = fixed < optin ? (int)std::min<size_t>(256, (optin - fixed) / row) : 0;
     if (rmax >= 32 || rmax >= n) {
       int split = (n + rmax - 1) / rmax;
       const int want = opts ? opts->split : 0;
@@ -142,6 +157,8 @@ cudaError_t make_plan(long L, int nm, int n, const DevProps &dp, Plan<T> &pl, co
                      (zglob ? sizeof(T) * (size_t)n * n : 0);
   long lc = (long)(kWsBudget / per);
   lc = std::max(lc, kMinChunk);
+  if (lc < L) lc = (L + (L + lc - 1) / lc - 1) / ((L + lc - 1) / lc);  // equal chunks: phase 2
+                                                                         // costs its latency per chunk
   if (opts && opts->chunk > 0) lc = opts->chunk;
   pl.Lc = std::min(L, lc);
   size_t off = 0;
@@ -294,14 +311,23 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const bool k1_in_regs = reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin;
   const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems(n, k1c_nt, pl.k1b);
   const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.zrows);
-  int k2_tpb = 32;
+  // phase 2: matrices per warp, then warps per block within the shared
+  // memory budget (2n values per matrix)
+  p.k2mpw = k2_mpw(std::min(L, pl.Lc), dp.sms);
+  int k2_mpb = 32;  // matrices per block, a multiple of k2mpw
   {
     const size_t per = k2_smem_per_thread<T>(n);
     const size_t budget = std::min<size_t>((size_t)dp.smem_optin, 96 * 1024);
-    k2_tpb = (int)std::max<size_t>(1, std::min<size_t>(32, budget / per));
-    if ((size_t)k2_tpb * per > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
+    const int warps = (int)std::max<size_t>(
+        1, std::min<size_t>(std::max(1, std::min(K2_MAX_WARPS, 32 / p.k2mpw)), budget / (per * p.k2mpw)));
+    k2_mpb = warps * p.k2mpw;
+    if ((size_t)k2_mpb * per > (size_t)dp.smem_optin) {
+      p.k2mpw = 1;
+      k2_mpb = 1;
+      if (per > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
+    }
   }
-  const size_t k2_smem = k2_smem_per_thread<T>(n) * k2_tpb;
+  const size_t k2_smem = k2_smem_per_thread<T>(n) * k2_mpb;
   if (n <= 32) {
     if ((err = set_smem(k1_warp<T>, k1w_smem)) != cudaSuccess) return err;
     if ((err = set_smem(k3_warp<T>, k3w_smem)) != cudaSuccess) return err;
@@ -336,7 +362,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
       launch_k1<T>(p, (unsigned)lc, k1c_nt, k1c_smem, stream);
     }
     trace(chunk, 1, stream);
-    k2_ql<T><<<(unsigned)((lc + k2_tpb - 1) / k2_tpb), k2_tpb, k2_smem, stream>>>(p);
+    k2_ql<T><<<(unsigned)((lc + k2_mpb - 1) / k2_mpb), 32 * (k2_mpb / p.k2mpw), k2_smem, stream>>>(p);
     trace(chunk, 2, stream);
     if (n <= 32) {
       const unsigned nb = (unsigned)((lc + K3W_NW - 1) / K3W_NW);

@@ -65,7 +65,7 @@ typedef struct eigen_GPU_batch_opts {
                     rotations do not fit is finished by regenerating them
                     inside the apply phase, with identical results. */
   int chunk;     /* matrices per internal chunk; <= 0: automatic (workspace
-                    about 4 GiB or 512 matrices).  Bounds the workspace. */
+                    about 8 GiB or 512 matrices).  Bounds the workspace. */
   int split;     /* n > 32: thread blocks sharing one matrix's rows in the
                     apply phase; <= 0: automatic (the fewest whose rows fit
                     in shared memory).  Larger values trade re-reads of the
