@@ -134,6 +134,27 @@ def make_batch(torch, family, L, n, dtype, seed, device):
     return out
 
 
+FAMILY_TEXT = {
+    "letkf": "LETKF-like (n-1) I + Y^T Y, Y iid N(0,1)/sqrt(n)",
+    "symu": "(B + B^T)/2, B iid U[-1,1]",
+}
+
+
+def measured_traffic(kernel, dtype, n):
+    """DRAM bytes per matrix (read + write) of a phase kernel from the
+    committed ncu summary profiles/dram_traffic.txt, or None."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "dram_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for ln in f:
+            parts = ln.split()
+            if len(parts) >= 4 and not ln.startswith("#") and parts[0] == kernel and parts[1] == dtype \
+                    and parts[2] == str(n):
+                return float(parts[3])
+    return None
+
+
 def alg_bytes(n, esize):
     """Compulsory bytes per matrix: read A, write V and w (SURVEY 8(d) model)."""
     return esize * (2 * n * n + n)
@@ -264,12 +285,14 @@ def main():
 
     # per-phase kernel times on the launching stream (one extra traced solve
     # per step count, same inputs as the timed region)
-    phases = []
+    phases, nchunks = [], 1
     for i in range(args.steps):
         a = base.clone()
-        with E.PhaseTrace(chunks=1) as tr:
+        with E.PhaseTrace(chunks=64) as tr:
             solve(a)
-        phases.extend(tr.ms())
+        per_chunk = tr.ms()
+        nchunks = max(1, len(per_chunk))
+        phases.append(np.array(per_chunk).sum(axis=0))  # workspace chunks run one after another
     ph = np.array(phases).mean(axis=0) if phases else np.zeros(3)
     hbm, peak_kind = peaks()
 
@@ -279,47 +302,46 @@ def main():
     names = ["tridiag_qt", "ql_rotations", "apply_rotations"]
     dom = int(np.argmax(ph))
     achieved = pb[dom] * L / (ph[dom] / 1000.0) / 1e9 if ph[dom] > 0 else 0.0
+    traffic = measured_traffic(names[dom], args.dtype, n)
 
     line = {
         "metric": f"eigendecomps/s (n={n}, {args.dtype}, {args.family}, L={L})",
         "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": args.dtype, "data": "synthetic (seeded on device; LETKF-like family of the config)",
+        "dtype": args.dtype, "data": "synthetic, seeded on device: " + FAMILY_TEXT[args.family],
         "config": {"workload": f"{args.family} L={L} n={n} {args.dtype} {args.method} sorted",
                    "L_per_gpu": L, "n": n, "l2_flush": "inputs larger than L2 (fresh copy per step)",
                    "parallelism": f"replicas x{world} (independent matrices)"},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": 3 * nchunks * args.steps,
         "correctness": {"reference_gate_flags": gate_fail, "info_nonzero": info_fail,
                         "max_err1": float(e1.max().item()), "max_err2": float(e2.max().item())},
         "phases_ms": {k: float(v) for k, v in zip(names, ph)},
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "traffic": traffic * L if traffic else None,
+                     "traffic_source": "profiles/dram_traffic.txt (ncu capture at L=1024, per matrix x L)"
+                     if traffic else None,
                      "alg_bytes_per_matrix": pb[dom]},
         "hbm_fraction_whole_solve": alg_bytes(n, esize) * value / world / 1e9 / hbm,
         "clocks": clk.summary(),
     }
 
     if not args.no_e2e:
-        # end to end through the C ABI with host buffers: pinned H2D of the
-        # inputs, solve, D2H of eigenvectors and eigenvalues, every step
+        # end to end through the public host-buffer call (eigeng_b200.solve_host):
+        # every step copies A in from pinned host memory, solves, and copies
+        # the eigenvectors and eigenvalues back, the copies of one chunk
+        # overlapping the solve of another
         host_in = base.cpu().pin_memory()
         host_out = torch.empty_like(host_in).pin_memory()
         host_w = torch.empty((L, n), dtype=dt).pin_memory()
-        dev_a = torch.empty_like(base)
         for _ in range(2):
-            dev_a.copy_(host_in, non_blocking=True)
-            solve(dev_a)
-            host_out.copy_(dev_a, non_blocking=True)
-            host_w.copy_(w, non_blocking=True)
+            E.solve_host(host_in, n, w_host=host_w, z_host=host_out, method=method, stream=stream)
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1_ = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            dev_a.copy_(host_in, non_blocking=True)
-            solve(dev_a)
-            host_out.copy_(dev_a, non_blocking=True)
-            host_w.copy_(w, non_blocking=True)
+            E.solve_host(host_in, n, w_host=host_w, z_host=host_out, method=method, stream=stream)
         e1_.record(stream)
         barrier()
         ems = e0.elapsed_time(e1_)

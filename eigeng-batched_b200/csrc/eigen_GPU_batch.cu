@@ -18,6 +18,7 @@
 #include <mutex>
 
 #include "eigb_kernels.cuh"
+#include "eigb_symfunc.cuh"
 #include "../../include/eigen_GPU_batch.h"
 
 namespace eigb {
@@ -453,6 +454,24 @@ cudaError_t run_noalloc(long L, int nm, int n, int m, T *a, T *w, int *info, cud
   return run<T>(L, nm, n, m, a, w, scratch, kNoallocScratchBytes, info, &o, stream);
 }
 
+static_assert(EIGEN_GPU_FUNC_DIAG == SYMF_DIAG && EIGEN_GPU_FUNC_POW == SYMF_POW && EIGEN_GPU_FUNC_EXP == SYMF_EXP,
+              "matrix-function codes of the header and the kernel agree");
+
+template <class T>
+cudaError_t symfunc_run(long L, int nm, int n, const T *v, const T *w, T *z, int func, double p, cudaStream_t stream)
+{
+  if (L < 1 || n < 1 || nm < n || n > 1024 || v == nullptr || w == nullptr || z == nullptr)
+    return cudaErrorInvalidValue;
+  if (func < SYMF_DIAG || func > SYMF_EXP) return cudaErrorInvalidValue;
+  if (v == z) return cudaErrorInvalidValue;  // Z is written while V is still read
+  const int nt = (n + SF_TILE - 1) / SF_TILE;
+  const int ntiles = nt * (nt + 1) / 2;
+  const long blocks = L * ntiles;
+  if (blocks > 0x7fffffffL) return cudaErrorInvalidValue;
+  k_symfunc<T><<<(unsigned)blocks, 256, 0, stream>>>(L, nm, n, v, w, z, func, (T)p, ntiles);
+  return cudaGetLastError();
+}
+
 template <class T>
 cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, const T *z, double *err1, double *err2,
                       int *flags, float *ref_flags, cudaStream_t stream)
@@ -536,6 +555,18 @@ cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, c
                                        int *info, const cudaStream_t stream)
 {
   return eigb::run_noalloc<double>(L, nm, n, m, a, w, info, stream);
+}
+
+cudaError_t eigen_GPU_batch_symfunc_DP(const int L, const int nm, const int n, const double *v, const double *w,
+                                       double *z, const int func, const double p, const cudaStream_t stream)
+{
+  return eigb::symfunc_run<double>(L, nm, n, v, w, z, func, p, stream);
+}
+
+cudaError_t eigen_GPU_batch_symfunc_FP(const int L, const int nm, const int n, const float *v, const float *w,
+                                       float *z, const int func, const double p, const cudaStream_t stream)
+{
+  return eigb::symfunc_run<float>(L, nm, n, v, w, z, func, p, stream);
 }
 
 cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents)

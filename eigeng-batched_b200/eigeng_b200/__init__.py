@@ -63,6 +63,10 @@ def lib():
             f = getattr(L, "eigen_GPU_check_ex_" + s)
             f.argtypes = [I, I, I, I, P, P, P, P, P, P, P]
             f.restype = I
+        for s_ in ("DP", "FP"):
+            f = getattr(L, "eigen_GPU_batch_symfunc_" + s_)
+            f.argtypes = [I, I, I, P, P, P, I, ctypes.c_double, P]
+            f.restype = I
         L.eigen_GPU_batch_noalloc_DP.argtypes = [I, I, I, I, P, P, P, P]
         L.eigen_GPU_batch_noalloc_DP.restype = I
         L.eigen_GPU_batch_trace.argtypes = [P, I]
@@ -86,6 +90,10 @@ class PhaseTrace:
         st = lib().eigen_GPU_batch_trace(self._arr, len(self.events))
         if st != 0:
             raise EigenGError(f"eigen_GPU_batch_trace failed with cudaError {st}")
+        # events re-recorded by the solve come after this mark; the others
+        # keep their earlier placeholder record
+        self._mark = torch.cuda.Event(enable_timing=True)
+        self._mark.record()
         return self
 
     def __exit__(self, *exc):
@@ -93,14 +101,14 @@ class PhaseTrace:
         return False
 
     def ms(self):
+        """Phase times of every chunk the traced solve ran."""
         torch.cuda.synchronize()
         out = []
         for c in range(len(self.events) // 4):
             e = self.events[4 * c:4 * c + 4]
-            try:
-                out.append(tuple(e[i].elapsed_time(e[i + 1]) for i in range(3)))
-            except RuntimeError:
+            if self._mark.elapsed_time(e[0]) < 0:  # not recorded by the solve
                 break
+            out.append(tuple(e[i].elapsed_time(e[i + 1]) for i in range(3)))
         return out
 
 
@@ -113,6 +121,7 @@ def exported_symbols():
         "eigen_GPU_check_DP", "eigen_GPU_check_FP",
         "eigen_GPU_check_ex_DP", "eigen_GPU_check_ex_FP",
         "eigen_GPU_batch_trace", "eigen_GPU_batch_noalloc_DP",
+        "eigen_GPU_batch_symfunc_DP", "eigen_GPU_batch_symfunc_FP",
     ]
 
 
@@ -211,6 +220,103 @@ def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
     return w, info
+
+
+FUNC_DIAG, FUNC_POW, FUNC_EXP = 0, 1, 2
+
+
+def symfunc(v, w, n, func=FUNC_POW, p=0.5, nm=None, z=None, stream=None):
+    """eigen_GPU_batch_symfunc: z_k = V_k diag(f(w_k)) V_k^T for a solved
+    batch (v: eigenvectors, w: eigenvalues); returns z (allocated when None)."""
+    L, nm = _dims(v, n, nm)
+    if z is None:
+        z = torch.empty_like(v)
+    st = getattr(lib(), "eigen_GPU_batch_symfunc_" + _sfx(v.dtype))(L, nm, n, _ptr(v), _ptr(w), _ptr(z), func,
+                                                                     float(p), _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_symfunc failed with cudaError {st}")
+    return z
+
+
+def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True, max_sweep=100,
+               stream=None, device=None, z_host=None):
+    """Solves a batch held in host memory (pinned for the copies to be
+    asynchronous): eigenvectors overwrite ``a_host`` (or go to ``z_host``,
+    same shape, leaving ``a_host`` intact), eigenvalues go to ``w_host``
+    (allocated pinned when None), which is returned.
+
+    The batch goes through the device in chunks on three streams -- copy in,
+    solve, copy out -- so that the copies of one chunk overlap the solve of
+    another; three device buffers rotate.  ``chunk`` > 0 sets equal chunks.  The work starts after what is
+    already queued on ``stream`` (default: the current stream) and
+    ``stream`` waits for all of it, so events recorded there bracket the
+    whole transfer and solve.  Results equal eigen_GPU_batch_ex's on the
+    same matrices."""
+    nm = n if nm is None else nm
+    if a_host.is_cuda or not a_host.is_contiguous() or a_host.numel() % (nm * n):
+        raise EigenGError("a_host must be a contiguous host tensor of L*nm*n elements")
+    L = a_host.numel() // (nm * n)
+    a_host = a_host.view(L, n, nm)
+    z_host = a_host if z_host is None else z_host.view(L, n, nm)
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    caller = stream if stream is not None else torch.cuda.current_stream(dev)
+    dt = a_host.dtype
+    if w_host is None:
+        w_host = torch.empty((L, n), dtype=dt, pin_memory=True)
+    # chunk boundaries: equal chunks of `chunk` matrices when given; else
+    # 1/8, 3/8, 3/8, 1/8 of the batch -- small first and last chunks shorten
+    # the copy that nothing overlaps at either end, while few chunks keep
+    # the per-chunk latency of the QL phase from adding up
+    if chunk > 0:
+        bounds = list(range(0, L, chunk)) + [L]
+    elif L >= 2048:
+        bounds = [0, L // 8, L // 2, L - L // 8, L]
+    else:
+        bounds = [0, L]
+    nch = len(bounds) - 1
+    C = max(bounds[i + 1] - bounds[i] for i in range(nch))
+    nbuf = min(3, nch)
+    da = [torch.empty((C, n, nm), dtype=dt, device=dev) for _ in range(nbuf)]
+    dw = [torch.empty((C, n), dtype=dt, device=dev) for _ in range(nbuf)]
+    info = torch.zeros(C, dtype=torch.int32, device=dev)
+    wk = workspace(C, nm, n, dt, dev) if method != JACOBI else None
+    s_in, s_run, s_out = (torch.cuda.Stream(dev) for _ in range(3))
+    start = torch.cuda.Event()
+    start.record(caller)
+    for s_ in (s_in, s_run, s_out):
+        s_.wait_event(start)
+    freed = [None] * nbuf       # copy-out of the buffer's previous chunk
+    for i in range(nch):
+        c0, c1 = bounds[i], bounds[i + 1]
+        b = i % nbuf
+        cnt = c1 - c0
+        if freed[b] is not None:
+            s_in.wait_event(freed[b])
+        with torch.cuda.stream(s_in):
+            da[b][:cnt].copy_(a_host[c0:c1], non_blocking=True)
+        loaded = torch.cuda.Event()
+        loaded.record(s_in)
+        s_run.wait_event(loaded)
+        st = eigen_GPU_batch_ex(da[b][:cnt], dw[b][:cnt], wk, n, nm, n, info[:cnt], method, sort, max_sweep,
+                                s_run)
+        if st != 0:
+            raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
+        solved = torch.cuda.Event()
+        solved.record(s_run)
+        s_out.wait_event(solved)
+        with torch.cuda.stream(s_out):
+            z_host[c0:c1].copy_(da[b][:cnt], non_blocking=True)
+            w_host[c0:c1].copy_(dw[b][:cnt], non_blocking=True)
+        freed[b] = torch.cuda.Event()
+        freed[b].record(s_out)
+    done = torch.cuda.Event()
+    done.record(s_out)
+    caller.wait_event(done)
+    # the device buffers are released only after the caller's stream has
+    # waited for the last copy
+    for t in da + dw + [info] + ([wk] if wk is not None else []):
+        t.record_stream(caller)
+    return w_host
 
 
 def check(a0, w, z, n, nm=None, stream=None):

@@ -125,6 +125,27 @@ cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, c
                                        int *info, const cudaStream_t stream);
 
 /*
+ * Symmetric matrix function of a solved batch (counterpart of the
+ * reference's prototype symdmt.cu:5-80, z = a diag(d) a^T, and of the use
+ * its README:171 names: powers such as the square root or the inverse):
+ *   z_k = V_k diag(f(w_k)) V_k^T   for every matrix k,
+ * with V_k at v + k*nm*n (eigenvectors as left by eigen_GPU_batch_*),
+ * w_k at w + k*n and the full symmetric result at z + k*nm*n (padding rows
+ * untouched).  func: EIGEN_GPU_FUNC_DIAG f(x) = x (w already holds f of
+ * the eigenvalues, as symdmt), EIGEN_GPU_FUNC_POW f(x) = pow(x, p) (p = 0.5
+ * square root, -1 inverse; NaN for negative x with non-integer p),
+ * EIGEN_GPU_FUNC_EXP f(x) = exp(p x).  z must not alias v.  Asynchronous
+ * on stream; returns cudaErrorInvalidValue for invalid arguments.
+ */
+#define EIGEN_GPU_FUNC_DIAG 0
+#define EIGEN_GPU_FUNC_POW 1
+#define EIGEN_GPU_FUNC_EXP 2
+cudaError_t eigen_GPU_batch_symfunc_DP(const int L, const int nm, const int n, const double *v, const double *w,
+                                       double *z, const int func, const double p, const cudaStream_t stream);
+cudaError_t eigen_GPU_batch_symfunc_FP(const int L, const int nm, const int n, const float *v, const float *w,
+                                       float *z, const int func, const double p, const cudaStream_t stream);
+
+/*
  * Phase timing (counterpart of the reference's compile-time TIMER,
  * eigen_GPU_batch.cu:157-244, which prints per-phase times from warp 0).
  * When set, every later solve on the calling process records, for chunk c

@@ -212,3 +212,15 @@ def residuals(a0, w, z, n):
     res = np.linalg.norm(R, axis=(1, 2)) / anorm
     orth = np.linalg.norm(np.transpose(V, (0, 2, 1)) @ V - np.eye(n)[None], axis=(1, 2))
     return res, orth
+
+
+def symdmt(v, d, n):
+    """z = V diag(d) V^T per matrix, the reference prototype symdmt.cu:5-80
+    (z(i,j) = sum_k a(i,k) d(k) a(j,k)), in FP64.  v: (L, n, nm) column-major
+    eigenvectors (v[k, j, i] = V_k(i, j)), d: (L, n).  Returns (L, n, n)
+    column-major (z[k, j, i] = Z_k(i, j))."""
+    v = np.asarray(v, dtype=np.float64)[:, :n, :n]       # [k, col j, row i]
+    d = np.asarray(d, dtype=np.float64).reshape(-1, n)
+    V = np.transpose(v, (0, 2, 1))                        # V[k, i, j]
+    Z = (V * d[:, None, :]) @ np.transpose(V, (0, 2, 1))
+    return np.transpose(Z, (0, 2, 1))

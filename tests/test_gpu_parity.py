@@ -314,3 +314,23 @@ def test_chunked_batch_and_determinism(oracle_mod):
         w2, z2, i2 = gpu_solve(a0, n, chunk=chunk)
         assert np.array_equal(w1, w2) and np.array_equal(z1, z2) and np.array_equal(i1, i2)
         assert np.array_equal(w1[3], w1[0]) and np.array_equal(z1[3], z1[0])
+
+
+def test_solve_host_matches_device_solve(oracle_mod):
+    """solve_host (host buffers, chunks on three streams) gives exactly the
+    device solve's results, with a ragged last chunk and padding rows."""
+    O = oracle_mod
+    n, nm, L = 48, 50, 37
+    a0 = np.zeros((L, n, nm))
+    a0[:, :, :n] = O.sym_uniform(L, n, seed=11)
+    w1, z1, _ = gpu_solve(a0, n, nm)
+    ah = torch.from_numpy(a0.copy()).pin_memory()
+    wh = E().solve_host(ah, n, nm, chunk=10)
+    torch.cuda.synchronize()
+    assert np.array_equal(wh.numpy(), w1)
+    assert np.array_equal(ah.numpy()[:, :, :n], z1[:, :, :n])
+    af = torch.from_numpy(a0.astype(np.float32))             # not pinned: copies still complete
+    wf = E().solve_host(af, n, nm)
+    torch.cuda.synchronize()
+    w2, _, _ = gpu_solve(a0.astype(np.float32), n, nm)
+    assert np.array_equal(wf.numpy(), w2)

@@ -136,3 +136,26 @@ def test_nan_input_terminates_with_status(oracle_mod):
     a = a0.copy()
     w, info, _ = O.eigen_batch(a, 6)
     assert info[0] != 0 and info[1] == 0
+
+
+def test_symdmt_restatement(oracle_mod):
+    """oracle.symdmt is z(i,j) = sum_k a(i,k) d(k) a(j,k) (symdmt.cu:5-80);
+    with d = eigenvalues it rebuilds the matrix."""
+    O = oracle_mod
+    rng = np.random.default_rng(0)
+    n = 6
+    v = rng.standard_normal((2, n, n))
+    d = rng.standard_normal((2, n))
+    z = O.symdmt(v, d, n)
+    for k in range(2):
+        for i in range(n):
+            for j in range(n):
+                ref = sum(v[k, kk, i] * d[k, kk] * v[k, kk, j] for kk in range(n))
+                assert abs(z[k, j, i] - ref) <= 1e-12
+    a0 = O.sym_uniform(2, n, seed=1)
+    a = a0.copy()
+    w, info, _ = O.eigen_batch(a, n)
+    back = O.symdmt(a, w, n)
+    A = np.triu(np.transpose(a0, (0, 2, 1)))
+    A = A + np.transpose(np.triu(A, 1), (0, 2, 1))
+    assert np.abs(np.transpose(back, (0, 2, 1)) - A).max() <= 1024 * np.finfo(float).eps * np.abs(A).max()  # QL deflates at 512 eps
