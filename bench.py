@@ -35,7 +35,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "cusolver"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--L", type=int, default=4096)
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
@@ -220,10 +220,107 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_cusolver(args):
+    """Reported baseline on the same GPU: cuSOLVER's batched dense
+    eigensolver (cusolverDnXsyevBatched; for n <= 32 also syevjBatched with
+    the reference's settings, tolerance 512 eps / 16 eps and 10 sweeps,
+    cusolver.hpp:23-25,108-110), on the same device-resident inputs and
+    timing rules as this library's arm (fresh copy per step, CUDA events)."""
+    import ctypes
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    lib = ctypes.CDLL(os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64", "libcusolver.so.11"))
+    P, I, I64, SZ = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_size_t
+    dt = torch.float64 if args.dtype == "f64" else torch.float32
+    cdt = 1 if dt == torch.float64 else 0  # CUDA_R_64F / CUDA_R_32F
+    n, L = args.n, args.L
+    h, prm = P(), P()
+    assert lib.cusolverDnCreate(ctypes.byref(h)) == 0
+    assert lib.cusolverDnCreateParams(ctypes.byref(prm)) == 0
+    stream = torch.cuda.current_stream(dev)
+    assert lib.cusolverDnSetStream(h, P(stream.cuda_stream)) == 0
+    base = make_batch(torch, args.family, L, n, dt, seed=1234, device=dev)
+    nbuf = args.steps + args.warmup
+    copies = [base.clone() for _ in range(nbuf)]
+    w = torch.empty((L, n), dtype=dt, device=dev)
+    info = torch.zeros(L, dtype=torch.int32, device=dev)
+    lib.cusolverDnXsyevBatched_bufferSize.argtypes = [P, P, I, I, I64, I, P, I64, I, P, I, ctypes.POINTER(SZ),
+                                                      ctypes.POINTER(SZ), I64]
+    lib.cusolverDnXsyevBatched.argtypes = [P, P, I, I, I64, I, P, I64, I, P, I, P, SZ, P, SZ, P, I64]
+    dws, hws = SZ(0), SZ(0)
+    st = lib.cusolverDnXsyevBatched_bufferSize(h, prm, 1, 1, n, cdt, P(base.data_ptr()), n, cdt, P(w.data_ptr()),
+                                               cdt, ctypes.byref(dws), ctypes.byref(hws), L)
+    if st != 0:
+        print(json.dumps({"impl": "cusolver", "unavailable": f"cusolverDnXsyevBatched_bufferSize status {st}"}))
+        return
+    dbuf = torch.empty(max(dws.value, 16), dtype=torch.uint8, device=dev)
+    hbuf = ctypes.create_string_buffer(max(hws.value, 16))
+
+    def solve(a):
+        return lib.cusolverDnXsyevBatched(h, prm, 1, 1, n, cdt, P(a.data_ptr()), n, cdt, P(w.data_ptr()), cdt,
+                                          P(dbuf.data_ptr()), dws.value, hbuf, hws.value, P(info.data_ptr()), L)
+
+    def timed(fn):
+        for i in range(args.warmup):
+            assert fn(copies[i]) == 0
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            assert fn(copies[args.warmup + i]) == 0
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    ms = timed(solve)
+    line = {
+        "impl": "cusolver", "routine": "cusolverDnXsyevBatched",
+        "metric": f"eigendecomps/s (n={n}, {args.dtype}, {args.family}, L={L})",
+        "value": L / (ms / 1000.0), "unit": "matrices/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
+        "data": "synthetic, seeded on device: " + FAMILY_TEXT[args.family],
+        "config": {"workload": f"{args.family} L={L} n={n} {args.dtype}", "L_per_gpu": L, "n": n},
+        "info_nonzero": int((info != 0).sum().item()),
+    }
+    if n <= 32:
+        sinfo = P()
+        assert lib.cusolverDnCreateSyevjInfo(ctypes.byref(sinfo)) == 0
+        lib.cusolverDnXsyevjSetTolerance.argtypes = [P, ctypes.c_double]
+        lib.cusolverDnXsyevjSetMaxSweeps.argtypes = [P, I]
+        lib.cusolverDnXsyevjSetTolerance(sinfo, 512 * 2.0 ** -52 if dt == torch.float64 else 16 * 2.0 ** -23)
+        lib.cusolverDnXsyevjSetMaxSweeps(sinfo, 10)
+        pre = "D" if dt == torch.float64 else "S"
+        fb = getattr(lib, f"cusolverDn{pre}syevjBatched_bufferSize")
+        fs = getattr(lib, f"cusolverDn{pre}syevjBatched")
+        fb.argtypes = [P, I, I, I, P, I, P, ctypes.POINTER(I), P, I]
+        fs.argtypes = [P, I, I, I, P, I, P, P, I, P, P, I]
+        lw = I(0)
+        assert fb(h, 1, 1, n, P(base.data_ptr()), n, P(w.data_ptr()), ctypes.byref(lw), sinfo, L) == 0
+        work = torch.empty(max(lw.value, 1), dtype=dt, device=dev)
+        msj = timed(lambda a: fs(h, 1, 1, n, P(a.data_ptr()), n, P(w.data_ptr()), P(work.data_ptr()), lw.value,
+                                 P(info.data_ptr()), sinfo, L))
+        line["syevjBatched"] = {"value": L / (msj / 1000.0), "unit": "matrices/s", "ms_per_step": msj,
+                                "tolerance": "512 eps (FP64) / 16 eps (FP32)", "max_sweeps": 10}
+        lib.cusolverDnDestroySyevjInfo(sinfo)
+    print(json.dumps(line), flush=True)
+    if args.out:
+        with open(args.out, "a") as f:
+            f.write(json.dumps(line) + "\n")
+    lib.cusolverDnDestroyParams(prm)
+    lib.cusolverDnDestroy(h)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.impl == "cusolver":
+        return run_cusolver(args)
     import torch
     import torch.distributed as dist
     import eigeng_b200 as E
@@ -319,7 +416,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
                      "traffic": traffic * L if traffic else None,
-                     "traffic_source": "profiles/dram_traffic.txt (ncu capture at L=1024, per matrix x L)"
+                     "traffic_source": "profiles/dram_traffic.txt (ncu DRAM bytes per matrix at 2-4x L2 inputs, x L)"
                      if traffic else None,
                      "alg_bytes_per_matrix": pb[dom]},
         "hbm_fraction_whole_solve": alg_bytes(n, esize) * value / world / 1e9 / hbm,

@@ -504,24 +504,118 @@ template <class T> __host__ __device__ __forceinline__ int seg_walk(const Rec<T>
   return q;
 }
 
+#define EIGB_PAIR_STEP(X, RA, RB, OUT)               \
+  {                                                  \
+    const T ya_ = fma((RA).c, ha, (RA).s * (X));     \
+    ha = fma(-(RA).s, ha, (RA).c * (X));             \
+    const T yb_ = fma((RB).c, hb, (RB).s * ya_);     \
+    hb = fma(-(RB).s, hb, (RB).c * ya_);             \
+    OUT = yb_;                                       \
+  }
+
+// Two consecutive sweeps over the same rotations i0 .. i0-len+1 (records
+// ra[0..len), rb[0..len)) as a two-stage pipeline on one row: the second
+// sweep trails the first by one column and takes the first's output from
+// registers, so each column is loaded and stored once for both sweeps
+// (half the shared-memory traffic of two seg_apply calls) and the two
+// fma chains are independent within a step.  Same result, rotation by
+// rotation, as seg_apply(ra) followed by seg_apply(rb).
+template <class T, int CS>
+__host__ __device__ __forceinline__ void seg_apply_pair(T *__restrict__ zr, const int cs_rt,
+                                                        const Rec<T> *__restrict__ ra,
+                                                        const Rec<T> *__restrict__ rb, const int i0, const int len)
+{
+  const int cs = CS > 0 ? CS : cs_rt;
+  T *p = zr + i0 * cs;
+  T ha = p[cs];
+  T hb;
+  {  // first sweep, rotation i0: its output z_{i0+1} is the second sweep's carry
+    const T x = p[0];
+    const Rec<T> r = ra[0];
+    hb = fma(r.c, ha, r.s * x);
+    ha = fma(-r.s, ha, r.c * x);
+  }
+  p -= cs;  // at column i0 - j for step j: first sweep rotation i0-j, second i0-j+1
+  int j = 1;
+  constexpr int U = 4;
+  if (len - 1 >= 2 * U) {
+    T x[U], xn[U];
+    Rec<T> a[U], b[U], an[U], bn[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      x[u] = p[-u * cs];
+      a[u] = ra[j + u];
+      b[u] = rb[j - 1 + u];
+    }
+    for (; j + 2 * U <= len; j += U) {
+#pragma unroll
+      for (int u = 0; u < U; u++) {  // next block, below every store of this one
+        xn[u] = p[-(U + u) * cs];
+        an[u] = ra[j + U + u];
+        bn[u] = rb[j - 1 + U + u];
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) EIGB_PAIR_STEP(x[u], a[u], b[u], p[(2 - u) * cs])
+      p -= U * cs;
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        x[u] = xn[u];
+        a[u] = an[u];
+        b[u] = bn[u];
+      }
+    }
+    // j + U <= len: the block in registers is inside the segment
+#pragma unroll
+    for (int u = 0; u < U; u++) EIGB_PAIR_STEP(x[u], a[u], b[u], p[(2 - u) * cs])
+    p -= U * cs;
+    j += U;
+  }
+  for (; j < len; j++, p -= cs) {
+    const T x0 = p[0];
+    EIGB_PAIR_STEP(x0, ra[j], rb[j - 1], p[2 * cs])
+  }
+  {  // second sweep, last rotation i0-len+1
+    const Rec<T> r = rb[len - 1];
+    p[2 * cs] = fma(r.c, hb, r.s * ha);
+    p[cs] = fma(-r.s, hb, r.c * ha);
+  }
+}
+#undef EIGB_PAIR_STEP
+
 // Applies the segments of rbuf[0..used) (complete, as found by seg_walk) to
-// the rows this thread owns.
-template <class T, bool SM, int RPT>
-__device__ __forceinline__ void apply_chunk(const Rec<T> *rbuf, const int used, const int cs, const bool (&own)[RPT],
-                                            T *const (&zr)[RPT])
+// one row; two consecutive segments over the same rotations (the sweeps of
+// one QL index) go through seg_apply_pair.
+template <class T, int CS>
+__host__ __device__ __forceinline__ void apply_segments(const Rec<T> *rbuf, const int used, T *zr, const int cs)
 {
   int q = 0;
   while (q < used) {
     const Rec<T> hd = rbuf[q];
     const int L = hdr_cnt(hd), i0 = hdr_i0(hd);
-#pragma unroll
-    for (int j = 0; j < RPT; j++)
-      if (own[j]) {
-        if (SM) seg_apply<T, 1>(zr[j], 1, rbuf + q + 1, i0, L);
-        else seg_apply<T, 0>(zr[j], cs, rbuf + q + 1, i0, L);
+    const int q2 = q + 1 + L;
+    if (L >= 1 && q2 < used) {
+      const Rec<T> h2 = rbuf[q2];
+      if (hdr_cnt(h2) == L && hdr_i0(h2) == i0) {
+        seg_apply_pair<T, CS>(zr, cs, rbuf + q + 1, rbuf + q2 + 1, i0, L);
+        q = q2 + 1 + L;
+        continue;
       }
-    q += 1 + L;
+    }
+    seg_apply<T, CS>(zr, cs, rbuf + q + 1, i0, L);
+    q = q2;
   }
+}
+
+template <class T, bool SM, int RPT>
+__device__ __forceinline__ void apply_chunk(const Rec<T> *rbuf, const int used, const int cs, const bool (&own)[RPT],
+                                            T *const (&zr)[RPT])
+{
+#pragma unroll
+  for (int j = 0; j < RPT; j++)
+    if (own[j]) {
+      if (SM) apply_segments<T, 1>(rbuf, used, zr[j], 1);
+      else apply_segments<T, 0>(rbuf, used, zr[j], cs);
+    }
 }
 
 // Phase 1 leaves Q in a; rotations act on the rows of Q independently, so

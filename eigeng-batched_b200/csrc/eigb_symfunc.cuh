@@ -102,16 +102,17 @@ __global__ void __launch_bounds__(256) k_symfunc(const long L, const int nm, con
         for (int y = 0; y < 4; y++) acc[x][y] = fma(a[x], b[y], acc[x][y]);
     }
   }
-  // Z(i, j) = acc, and Z(j, i) for tiles off the diagonal
+  // Z(i, j) = Z(j, i) = acc for i <= j (every element of an off-diagonal
+  // tile; the upper half of a diagonal tile), so Z is exactly symmetric
 #pragma unroll
   for (int y = 0; y < 4; y++) {
     const int j = j0 + tc + 16 * y;
 #pragma unroll
     for (int x = 0; x < 4; x++) {
       const int i = i0 + tr + 16 * x;
-      if (i < n && j < n) {
+      if (i < n && j < n && i <= j) {
         Z[i + (size_t)j * nm] = acc[x][y];
-        if (ti != tj) Z[j + (size_t)i * nm] = acc[x][y];
+        if (i != j) Z[j + (size_t)i * nm] = acc[x][y];
       }
     }
   }

@@ -1,5 +1,5 @@
 // Host build of the phase-3 apply (csrc/eigb_kernels.cuh: seg_walk,
-// seg_apply) for CPU unit tests: applies a rotation record stream to a
+// apply_segments with seg_apply and seg_apply_pair) for CPU unit tests: applies a rotation record stream to a
 // row-major n x n matrix, staging it in chunks of `ch` records exactly as
 // k3_cta does.
 #include "../../eigeng-batched_b200/csrc/eigb_kernels.cuh"
@@ -13,13 +13,8 @@ template <class T> static int run(int n, T *Z, const T *recs, int nrec, int ch)
     const int cnt = nrec - base < ch ? nrec - base : ch;
     const Rec<T> *rb = src + base;
     const int used = seg_walk(rb, cnt);
-    int q = 0;
-    while (q < used) {
-      const int L = hdr_cnt(rb[q]), i0 = hdr_i0(rb[q]);
-      for (int r = 0; r < n; r++) seg_apply<T, 1>(Z + r * n, 1, rb + q + 1, i0, L);
-      q += 1 + L;
-      segs++;
-    }
+    for (int r = 0; r < n; r++) apply_segments<T, 1>(rb, used, Z + r * n, 1);
+    for (int q = 0; q < used; q += 1 + hdr_cnt(rb[q])) segs++;
     base += used > 0 ? used : cnt;
   }
   return segs;
