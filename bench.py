@@ -234,7 +234,10 @@ def run_cusolver(args):
         return
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    lib = ctypes.CDLL(os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "lib64", "libcusolver.so.11"))
+    # the cuSOLVER that ships with torch, consistent with the cuBLAS torch has
+    # already loaded (the system one may need a newer cuBLAS)
+    import nvidia.cusolver
+    lib = ctypes.CDLL(os.path.join(list(nvidia.cusolver.__path__)[0], "lib", "libcusolver.so.11"))
     P, I, I64, SZ = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_size_t
     dt = torch.float64 if args.dtype == "f64" else torch.float32
     cdt = 1 if dt == torch.float64 else 0  # CUDA_R_64F / CUDA_R_32F

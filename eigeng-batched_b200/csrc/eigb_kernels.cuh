@@ -15,12 +15,14 @@
 //                  matrix's rows split over CTAs when needed) or, for the
 //                  largest FP64 sizes, Z in the workspace
 //   k_jacobi_warp  cyclic Jacobi for n <= 32 (jac_tiled.hpp:3-152)
-//   k_check        FP64 residual / orthogonality gate (eigen_GPU_check.cu)
+//   k_check        FP64 residual / orthogonality gate (eigen_GPU_check.cu),
+//                  one warp per matrix; k_check_cta the tiled form for n > 32
 #pragma once
 #include <stdio.h>
 
 #include "eigb_common.cuh"
 #include "eigb_ql.cuh"
+#include "eigb_symfunc.cuh"
 #include "eigb_tridiag.cuh"
 #include "eigb_tridiag_reg.cuh"
 
@@ -39,6 +41,7 @@ template <class T> struct KP {
   int zrows;     // phase 3 with Z in shared memory: rows per CTA ...
   int zsplit;    // ... and CTAs per matrix
   int k2mpw;     // phase 2: matrices per warp (1..32)
+  const T *ap;   // packed upper-triangle input (nullptr: the upper triangle of a)
   int *info;     // optional per-matrix status for the caller (may be null)
   long Lc;       // matrices in this chunk
   int n, nm;
@@ -47,6 +50,11 @@ template <class T> struct KP {
   int max_sweep;
   int sort;
 };
+
+// Packed upper triangle (LAPACK 'U' order): element (r, c), r <= c, at
+// ap[r + c(c+1)/2]; matrix k starts at ap + k n(n+1)/2.
+__host__ __device__ __forceinline__ size_t packed_size(int n) { return (size_t)n * (n + 1) / 2; }
+__host__ __device__ __forceinline__ int packed_at(int r, int c) { return r + c * (c + 1) / 2; }
 
 constexpr int K1W_NW = 4;       // warps (matrices) per CTA in k1_warp
 constexpr int K2_MAX_WARPS = 8; // warps per CTA in k2_ql at most
@@ -61,10 +69,10 @@ __host__ __device__ constexpr int k1_split(int n) { return n <= 256 ? 4 : (n <= 
 
 // ---------------------------------------------------------------- n == 1
 template <class T>
-__global__ void k_n1(const long L, const int nm, T *a, T *w)
+__global__ void k_n1(const long L, const int nm, T *a, T *w, const T *ap)
 {
   for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < L; k += (long)gridDim.x * blockDim.x) {
-    w[k] = a[k * nm];
+    w[k] = ap ? ap[k] : a[k * nm];
     a[k * nm] = T(1);
   }
 }
@@ -84,8 +92,9 @@ __global__ void __launch_bounds__(32 * K1W_NW) k1_warp(const KP<T> p)
   WarpTeam tm;
   const int n = p.n, nm = p.nm, r = tm.rank;
   T *A = p.a + (size_t)k * nm * n;
+  const T *Ap = p.ap ? p.ap + (size_t)k * packed_size(n) : nullptr;
   for (int c = 0; c < n; c++)
-    if (r <= c) S[r + c * K1W_LD] = A[r + (size_t)c * nm];
+    if (r <= c) S[r + c * K1W_LD] = Ap ? Ap[packed_at(r, c)] : A[r + (size_t)c * nm];
   __syncwarp();
   for (int c = 0; c < n; c++)
     if (r > c && r < n) S[r + c * K1W_LD] = S[c + r * K1W_LD];
@@ -95,8 +104,6 @@ __global__ void __launch_bounds__(32 * K1W_NW) k1_warp(const KP<T> p)
     for (int c = 0; c < n; c++) A[r + (size_t)c * nm] = S[r + c * K1W_LD];
 }
 
-// Shared memory of k1_cta: red[72], beta[n], pv[n], part[nthreads], then S
-// (shared-memory variant) n x (n|1).
 // Shared-memory elements of k1_cta: red[72], beta[n], pv[n], part[nthreads]
 // and the leading B x B block of the matrix (leading dimension B|1).
 __host__ __device__ inline size_t k1c_smem_elems(int n, int nthreads, int B)
@@ -123,14 +130,20 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
   T *part = pv + n;     // nt
   T *S = part + nt;     // B x B
   // full symmetric matrix from the upper triangle: the leading block in S
-  // (coalesced reads), the outer band mirrored in place
+  // (coalesced reads), the outer band mirrored in place (or, from a packed
+  // input, written to a in both triangles)
+  const T *Ap = p.ap ? p.ap + (size_t)k * packed_size(n) : nullptr;
   for (int idx = t; idx < B * B; idx += nt) {
     const int r = idx % B, c = idx / B;
-    if (r <= c) S[r + c * ld] = A[r + (size_t)c * nm];
+    if (r <= c) S[r + c * ld] = Ap ? Ap[packed_at(r, c)] : A[r + (size_t)c * nm];
   }
   for (long idx = t; idx < (long)n * n; idx += nt) {
     const int r = (int)(idx % n), c = (int)(idx / n);
-    if (r > c && r >= B) A[r + (size_t)c * nm] = A[c + (size_t)r * nm];
+    if (Ap) {
+      if (r >= B || c >= B) A[r + (size_t)c * nm] = Ap[r <= c ? packed_at(r, c) : packed_at(c, r)];
+    } else if (r > c && r >= B) {
+      A[r + (size_t)c * nm] = A[c + (size_t)r * nm];
+    }
   }
   __syncthreads();
   for (int idx = t; idx < B * B; idx += nt) {
@@ -164,7 +177,7 @@ __global__ void __launch_bounds__(32 * NB * NB, 1) k1_reg(const KP<T> p)
   const long k = blockIdx.x;
   CtaTeam tm;
   tridiag_qt_reg<T, NB>(tm, p.a + (size_t)k * p.nm * p.n, p.nm, p.n, p.d + k * p.n, p.e + k * p.n,
-                        reinterpret_cast<T *>(smem_raw));
+                        reinterpret_cast<T *>(smem_raw), p.ap ? p.ap + (size_t)k * packed_size(p.n) : nullptr);
 }
 
 // ---------------------------------------------------------------- phase 2
@@ -787,7 +800,10 @@ __global__ void __launch_bounds__(32 * K1W_NW) k_jacobi_warp(const KP<T> p)
   // full symmetric matrix from the upper triangle; Z = I
   for (int c = 0; c < 32; c++) {
     T v = T(0);
-    if (own && c < n) v = (r <= c) ? A[r + (size_t)c * nm] : A[c + (size_t)r * nm];
+    if (own && c < n) {
+      if (p.ap) v = p.ap[(size_t)k * packed_size(n) + (r <= c ? packed_at(r, c) : packed_at(c, r))];
+      else v = (r <= c) ? A[r + (size_t)c * nm] : A[c + (size_t)r * nm];
+    }
     As[r + c * 33] = v;
     Zs[r + c * 33] = (r == c) ? T(1) : T(0);
   }
@@ -952,6 +968,130 @@ __global__ void k_check(const long L, const int nm, const int n, const int m, co
         ans[2] = (float)TOL;
         ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
       }
+    }
+  }
+}
+
+// The same two norms for n > 32, one CTA of 256 threads per matrix: the
+// products A Z (n x m) and Z^T Z (upper triangle, m x m) are formed tile by
+// tile (64 x 64, 16-row panels staged in shared memory, a 4 x 4 FP64
+// register tile per thread, rows and columns 16 apart) and squared into
+// per-thread sums; one CTA reduction at the end (deterministic).
+constexpr int CK_TILE = 64, CK_KC = 16, CK_LDP = CK_TILE + 2;
+
+template <class T>
+__global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, const int n, const int m,
+                                                   const T *a0, const T *w, const T *z, double *err1,
+                                                   double *err2, int *flags, float *ref_flags)
+{
+  __shared__ double P[CK_KC][CK_LDP];  // P(tile row, k)
+  __shared__ double Q[CK_KC][CK_LDP];  // Q(k, tile column)
+  __shared__ double red[64];
+  const long id = blockIdx.x;
+  if (id >= L) return;
+  const T *a = a0 + (size_t)id * nm * n;
+  const T *zz = z + (size_t)id * nm * n;
+  const T *d = w + (size_t)id * n;
+  const int t = threadIdx.x, tr = t % 16, tc = t / 16;
+  const int ntn = (n + CK_TILE - 1) / CK_TILE, ntm = (m + CK_TILE - 1) / CK_TILE;
+  double s1 = 0.0, s2 = 0.0;
+  // tiles: ntn x ntm of A Z, then the upper ntm x ntm of Z^T Z
+  const int nres = ntn * ntm, nort = ntm * (ntm + 1) / 2;
+  for (int tile = 0; tile < nres + nort; tile++) {
+    const bool res = tile < nres;
+    int ti, tj;
+    if (res) {
+      ti = tile % ntn;
+      tj = tile / ntn;
+    } else {
+      symf_tile(tile - nres, ntm, ti, tj);
+    }
+    const int i0 = ti * CK_TILE, j0 = tj * CK_TILE;
+    const int ilim = res ? n : m;
+    double acc[4][4];
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+      for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
+    for (int kc = 0; kc < n; kc += CK_KC) {
+      __syncthreads();  // the previous panels are consumed
+#pragma unroll
+      for (int q = 0; q < (CK_KC * CK_TILE) / 256; q++) {
+        const int e = t + 256 * q;
+        const int rr = e % CK_TILE, cc = e / CK_TILE;  // rr: tile row / column, cc: k offset
+        const int kk = kc + cc;
+        const int i = i0 + rr, j = j0 + rr;
+        double pv = 0.0, qv = 0.0;
+        if (kk < n) {
+          if (i < ilim) {
+            if (res) pv = (double)((i <= kk) ? a[i + (size_t)kk * nm] : a[kk + (size_t)i * nm]);  // A(i, k)
+            else pv = (double)zz[kk + (size_t)i * nm];                                         // Z(k, i)
+          }
+          if (j < m) qv = (double)zz[kk + (size_t)j * nm];  // Z(k, j)
+        }
+        P[cc][rr] = pv;
+        Q[cc][rr] = qv;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < CK_KC; c++) {
+        double pa[4], qb[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          pa[u] = P[c][tr + 16 * u];
+          qb[u] = Q[c][tc + 16 * u];
+        }
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+          for (int y = 0; y < 4; y++) acc[x][y] = fma(pa[x], qb[y], acc[x][y]);
+      }
+    }
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+      for (int y = 0; y < 4; y++) {
+        const int i = i0 + tr + 16 * x, j = j0 + tc + 16 * y;
+        if (res) {
+          if (i < n && j < m) {
+            const double rr = acc[x][y] - (double)d[j] * (double)zz[i + (size_t)j * nm];
+            s1 = fma(rr, rr, s1);
+          }
+        } else if (i < m && j < m && i <= j) {
+          const double rr = acc[x][y] - (i == j ? 1.0 : 0.0);
+          s2 += (i == j ? 1.0 : 2.0) * rr * rr;
+        }
+      }
+  }
+  // CTA sums of s1, s2
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
+  if ((t & 31) == 0) {
+    red[t >> 5] = s1;
+    red[32 + (t >> 5)] = s2;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double e1 = 0.0, e2 = 0.0;
+    for (int q = 0; q < 8; q++) {
+      e1 += red[q];
+      e2 += red[32 + q];
+    }
+    e1 = sqrt(e1);
+    e2 = sqrt(e2);
+    const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
+    const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
+    const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
+    const bool f1 = e1 > dmax * TOL, f2 = e2 > n * TOL;
+    if (err1) err1[id] = e1;
+    if (err2) err2[id] = e2;
+    if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
+    if (ref_flags) {
+      float *ans = ref_flags + (size_t)id * nm * n * (sizeof(T) / sizeof(float));
+      ans[0] = (float)(f1 ? e1 / dmax : 0.0);
+      ans[1] = (float)(f2 ? e2 : 0.0);
+      ans[2] = (float)TOL;
+      ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
     }
   }
 }

@@ -51,6 +51,53 @@ __host__ __device__ __forceinline__ void ld2(const T *p, T &a, T &b)
 // Reflectors applied per barrier in the formation of M.
 constexpr int QB = 4;
 
+// Row slice times reflector, sum_c S[c] v_c over the 32 columns of a
+// block (Vc = the reflector at the block's first column).  With PIV the
+// block holds the reflector pivot at column cp, whose value ul is not in
+// shared memory yet: the selects substitute it (only the warps of that one
+// column block take this path).
+template <class T, bool PIV>
+__host__ __device__ __forceinline__ T reg_symv(const T (&S)[32], const T *Vc, const int cp, const T ul)
+{
+  T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
+#pragma unroll
+  for (int c = 0; c < 32; c += 4) {
+    T v0, v1, v2, v3;
+    ld2(Vc + c, v0, v1);
+    ld2(Vc + c + 2, v2, v3);
+    if (PIV) {
+      v0 = (c + 0 == cp) ? ul : v0;
+      v1 = (c + 1 == cp) ? ul : v1;
+      v2 = (c + 2 == cp) ? ul : v2;
+      v3 = (c + 3 == cp) ? ul : v3;
+    }
+    a0 = fma(S[c + 0], v0, a0);
+    a1 = fma(S[c + 1], v1, a1);
+    a2 = fma(S[c + 2], v2, a2);
+    a3 = fma(S[c + 3], v3, a3);
+  }
+  return (a0 + a1) + (a2 + a3);
+}
+
+// S[c] += u_c w2r + p_c ur over the block's 32 columns (pivot as in reg_symv)
+template <class T, bool PIV>
+__host__ __device__ __forceinline__ void reg_rank2(T (&S)[32], const T *Vc, const T *pc, const T ur, const T w2r,
+                                                   const int cp, const T ul)
+{
+#pragma unroll
+  for (int c = 0; c < 32; c += 2) {
+    T u0, u1, p0, p1;
+    ld2(Vc + c, u0, u1);
+    ld2(pc + c, p0, p1);
+    if (PIV) {
+      u0 = (c + 0 == cp) ? ul : u0;
+      u1 = (c + 1 == cp) ? ul : u1;
+    }
+    S[c] = fma(p0, ur, fma(u0, w2r, S[c]));
+    S[c + 1] = fma(p1, ur, fma(u1, w2r, S[c + 1]));
+  }
+}
+
 template <int NB> struct RegLayout {
   static constexpr int NR = 32 * NB;
   static constexpr int NT = NR * NB;
@@ -74,8 +121,11 @@ template <int NB> __host__ __device__ inline size_t reg_smem_elems(int n)
 }
 
 // A: the input matrix (upper triangle used), overwritten with Q (A = Q T Q^T).
+// Ap: when given, the input is read from this packed upper triangle instead
+// (element (r, c), r <= c, at Ap[r + c(c+1)/2]); Q still goes to A.
 template <class T, int NB, class Team>
-__host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int n, T *d_out, T *e_out, T *sm)
+__host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int n, T *d_out, T *e_out, T *sm,
+                                        const T *Ap = nullptr)
 {
   constexpr int NR = RegLayout<NB>::NR;
   const int t = tm.rank;
@@ -94,7 +144,7 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   // ---- stage the upper triangle, then build the register slices ----
   for (int idx = t; idx < n * n; idx += tm.size()) {
     const int rr = idx % n, cc = idx / n;
-    if (rr <= cc) V[rr + cc * lds] = A[rr + (size_t)cc * nm];
+    if (rr <= cc) V[rr + cc * lds] = Ap ? Ap[rr + cc * (cc + 1) / 2] : A[rr + (size_t)cc * nm];
   }
   tm.sync();
   T S[32];
@@ -106,6 +156,10 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   tm.sync();  // the staging area becomes the reflector store
 
   // ---- reduction, i = n-1 .. 1 ----
+  // The pivot u_{i-1} = ul of step i is kept aside (gram[i], free until
+  // the formation of M) and copied into the reflector after the loop, so
+  // the reflector slot never changes while other warps read it; during
+  // step i the warps of its column block substitute it in registers.
   for (int i = n - 1; i >= 1; --i) {
     T *Vi = V + (size_t)i * NR;
     const int cbi = i >> 5;
@@ -121,30 +175,17 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
     const T anorm = -copysign_t(sqr_t(sig), ulast);
     const T ul = ulast - anorm;
     const T beta = T(1) / flip0to1(ul * anorm);
-    if (cb == cbi && r == i - 1) Vi[r] = ul;  // pivot (read by others after the next barrier)
+    if (cb == cbi && r == i - 1) gram[i] = ul;
     if (t == 0) {
       e_out[i - 1] = anorm;
       beta_s[i] = beta;
     }
     const bool act = (c0 < i) && (32 * rb < i);
+    const int cp = (i - 1) - c0;  // pivot column within this block, if 0 <= cp < 32
+    const bool piv = (cb == ((i - 1) >> 5));
     if (act) {  // partial p_r over this block's columns; u_{i-1} is ul
-      const int cp = (i - 1) - c0;
-      T a0 = T(0), a1 = T(0), a2 = T(0), a3 = T(0);
-#pragma unroll
-      for (int c = 0; c < 32; c += 4) {
-        T v0, v1, v2, v3;
-        ld2(Vi + c0 + c, v0, v1);
-        ld2(Vi + c0 + c + 2, v2, v3);
-        v0 = (c + 0 == cp) ? ul : v0;
-        v1 = (c + 1 == cp) ? ul : v1;
-        v2 = (c + 2 == cp) ? ul : v2;
-        v3 = (c + 3 == cp) ? ul : v3;
-        a0 = fma(S[c + 0], v0, a0);
-        a1 = fma(S[c + 1], v1, a1);
-        a2 = fma(S[c + 2], v2, a2);
-        a3 = fma(S[c + 3], v3, a3);
-      }
-      part[cb * NR + r] = (r < i) ? (a0 + a1) + (a2 + a3) : T(0);
+      const T a = piv ? reg_symv<T, true>(S, Vi + c0, cp, ul) : reg_symv<T, false>(S, Vi + c0, cp, ul);
+      part[cb * NR + r] = (r < i) ? a : T(0);
     }
     tm.sync();
     const int nact = (i + 31) >> 5;
@@ -155,27 +196,23 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
         if (q < nact) pr += part[q * NR + r];
       pr *= beta;
     }
-    if (cb == 0) pv[r] = pr;  // 0 for r >= i
-    const T ur = Vi[r];       // u_r with the pivot in place, 0 for r >= i
+    if (cb == 0) pv[r] = pr;                    // 0 for r >= i
+    const T ur = (r == i - 1) ? ul : Vi[r];     // u_r with the pivot, 0 for r >= i
     const T alpha = tm.sum(cb == 0 ? pr * ur : T(0), red) * (beta * T(0.5));
     if (act) {
       // A += u w^T + w u^T with w = p + alpha u, i.e.
       // a_rk += u_k (p_r + 2 alpha u_r) + p_k u_r
       const T w2r = fma(alpha + alpha, ur, pr);
-#pragma unroll
-      for (int c = 0; c < 32; c += 2) {
-        T u0, u1, p0, p1;
-        ld2(Vi + c0 + c, u0, u1);
-        ld2(pv + c0 + c, p0, p1);
-        S[c] = fma(p0, ur, fma(u0, w2r, S[c]));
-        S[c + 1] = fma(p1, ur, fma(u1, w2r, S[c + 1]));
-      }
+      if (piv) reg_rank2<T, true>(S, Vi + c0, pv + c0, ur, w2r, cp, ul);
+      else reg_rank2<T, false>(S, Vi + c0, pv + c0, ur, w2r, cp, ul);
     }
     // the barrier in the next step's first sum() orders pv/part reuse
   }
   tm.sync();
+  for (int k = 1 + t; k < n; k += tm.size()) V[(size_t)k * NR + k - 1] = gram[k];
   if (r < n && cb == rb) d_out[r] = get32(S, r - c0);
   if (t == 0) e_out[n - 1] = T(0);
+  tm.sync();
 
   // ---- M = H_1 ... H_{n-1}: M <- M + beta_k (M u_k) u_k^T from M = I ----
   // QB reflectors per barrier.  With a_j = M u_j for the M before the

@@ -245,9 +245,11 @@ template <class T> void launch_k1(const KP<T> &p, unsigned blocks, int nt, size_
   else k1_cta<T, 1><<<blocks, nt, smem, st>>>(p);
 }
 
+// ap: packed upper-triangle input (nullptr: the upper triangle of a); the
+// eigenvectors go to a either way
 template <class T>
 cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork, int *info,
-                const eigen_GPU_batch_opts *opts, cudaStream_t stream)
+                const eigen_GPU_batch_opts *opts, cudaStream_t stream, const T *ap = nullptr)
 {
   if (bad_args(L, nm, n, m) || a == nullptr || w == nullptr) return cudaErrorInvalidValue;
   int method = EIGEN_GPU_BATCH_TQL2, sort = 1, max_sweep = 100;
@@ -261,7 +263,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   cudaError_t err;
   if (n == 1) {
     const int blocks = (int)std::min<long>((L + 255) / 256, 4096);
-    k_n1<T><<<blocks, 256, 0, stream>>>(L, nm, a, w);
+    k_n1<T><<<blocks, 256, 0, stream>>>(L, nm, a, w, ap);
     if (info) cudaMemsetAsync(info, 0, sizeof(int) * (size_t)L, stream);
     return cudaGetLastError();
   }
@@ -280,6 +282,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     if ((err = set_smem(k_jacobi_warp<T>, smem)) != cudaSuccess) return err;
     p.a = a;
     p.w = w;
+    p.ap = ap;
     p.info = info;
     p.Lc = L;
     const long blocks = (L + K1W_NW - 1) / K1W_NW;
@@ -352,6 +355,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     trace(chunk, 0, stream);
     p.a = a + (size_t)c0 * nm * n;
     p.w = w + (size_t)c0 * n;
+    p.ap = ap ? ap + (size_t)c0 * packed_size(n) : nullptr;
     p.info = info ? info + c0 : nullptr;
     p.Lc = lc;
     if (n <= 32) {
@@ -477,6 +481,11 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
                       int *flags, float *ref_flags, cudaStream_t stream)
 {
   if (bad_args(L, nm, n, m) || !a0 || !w || !z) return cudaErrorInvalidValue;
+  if (n > 32) {
+    if (L > 0x7fffffffL) return cudaErrorInvalidValue;
+    k_check_cta<T><<<(unsigned)L, 256, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+    return cudaGetLastError();
+  }
   const long blocks = std::min<long>((L + 3) / 4, 65535);
   k_check<T><<<(unsigned)blocks, 128, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
   return cudaGetLastError();
@@ -549,6 +558,22 @@ void eigen_GPU_check_FP(const int L, const int nm, const int n, const int m, flo
   if (eigb::check_run<float>(L, nm, n, m, a, w, z, nullptr, nullptr, nullptr, reinterpret_cast<float *>(a),
                              stream) == cudaSuccess)
     eigb::k_check_print<float><<<1, 1, 0, stream>>>(L, nm, n, a);
+}
+
+cudaError_t eigen_GPU_batch_packed_DP(const int L, const int n, const double *ap, double *z, const int ldz,
+                                      double *w, void *wk, const size_t lwork, int *info,
+                                      const eigen_GPU_batch_opts *opts, const cudaStream_t stream)
+{
+  if (ap == nullptr) return cudaErrorInvalidValue;
+  return eigb::run<double>(L, ldz, n, n, z, w, wk, lwork, info, opts, stream, ap);
+}
+
+cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap, float *z, const int ldz, float *w,
+                                      void *wk, const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                      const cudaStream_t stream)
+{
+  if (ap == nullptr) return cudaErrorInvalidValue;
+  return eigb::run<float>(L, ldz, n, n, z, w, wk, lwork, info, opts, stream, ap);
 }
 
 cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, const int m, double *a, double *w,

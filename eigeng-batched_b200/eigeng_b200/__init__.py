@@ -64,6 +64,10 @@ def lib():
             f.argtypes = [I, I, I, I, P, P, P, P, P, P, P]
             f.restype = I
         for s_ in ("DP", "FP"):
+            f = getattr(L, "eigen_GPU_batch_packed_" + s_)
+            f.argtypes = [I, I, P, P, I, P, P, SZ, P, ctypes.POINTER(Opts), P]
+            f.restype = I
+        for s_ in ("DP", "FP"):
             f = getattr(L, "eigen_GPU_batch_symfunc_" + s_)
             f.argtypes = [I, I, I, P, P, P, I, ctypes.c_double, P]
             f.restype = I
@@ -122,6 +126,7 @@ def exported_symbols():
         "eigen_GPU_check_ex_DP", "eigen_GPU_check_ex_FP",
         "eigen_GPU_batch_trace", "eigen_GPU_batch_noalloc_DP",
         "eigen_GPU_batch_symfunc_DP", "eigen_GPU_batch_symfunc_FP",
+        "eigen_GPU_batch_packed_DP", "eigen_GPU_batch_packed_FP",
     ]
 
 
@@ -220,6 +225,39 @@ def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
     return w, info
+
+
+def packed_size(n):
+    return n * (n + 1) // 2
+
+
+def pack_upper(a, n, nm=None):
+    """Packed upper triangles (LAPACK 'U' order) of a batch in the full
+    column-major layout: (L, n(n+1)/2), element (r, c), r <= c, at
+    r + c(c+1)/2."""
+    nm = n if nm is None else nm
+    A = a.reshape(-1, n, nm)
+    return torch.cat([A[:, c, :c + 1] for c in range(n)], dim=1).contiguous()
+
+
+def solve_packed(ap, n, ldz=None, method=TQL2, sort=True, max_sweep=100, stream=None, rec_cap=0, chunk=0, split=0):
+    """eigen_GPU_batch_packed: solves a batch given as packed upper
+    triangles; returns (z, w, info) with z in the full layout."""
+    if not ap.is_cuda or not ap.is_contiguous() or ap.numel() % packed_size(n):
+        raise EigenGError("ap must be a contiguous CUDA tensor of L*n(n+1)/2 elements")
+    L = ap.numel() // packed_size(n)
+    ldz = n if ldz is None else ldz
+    z = torch.empty((L, n, ldz), dtype=ap.dtype, device=ap.device)
+    w = torch.empty((L, n), dtype=ap.dtype, device=ap.device)
+    info = torch.zeros(L, dtype=torch.int32, device=ap.device)
+    wk = workspace(L, ldz, n, ap.dtype, ap.device, rec_cap, chunk) if method != JACOBI else None
+    o = Opts(method, 1 if sort else 0, max_sweep, rec_cap, chunk, split)
+    lw = 0 if wk is None else wk.numel()
+    st = getattr(lib(), "eigen_GPU_batch_packed_" + _sfx(ap.dtype))(
+        L, n, _ptr(ap), _ptr(z), ldz, _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_packed failed with cudaError {st}")
+    return z, w, info
 
 
 FUNC_DIAG, FUNC_POW, FUNC_EXP = 0, 1, 2

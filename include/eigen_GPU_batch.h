@@ -125,6 +125,24 @@ cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, c
                                        int *info, const cudaStream_t stream);
 
 /*
+ * Packed input (the "flexible data format" the reference's README:166 lists
+ * as future work; no counterpart in its code): matrix k is the upper
+ * triangle in LAPACK 'U' packed order, element (r, c), r <= c (0-based), at
+ * ap[k*n(n+1)/2 + r + c(c+1)/2] -- half the input bytes of the full
+ * layout.  ap is not modified; the eigenvectors go to z (column-major,
+ * leading dimension ldz >= n, matrix k at z + k*ldz*n) and the eigenvalues
+ * to w, exactly as eigen_GPU_batch_ex_* would leave them for the same
+ * matrices.  Workspace, options and status as eigen_GPU_batch_ex_*
+ * (eigen_GPU_batch_ex_BufferSize_* with nm = ldz gives lwork).
+ */
+cudaError_t eigen_GPU_batch_packed_DP(const int L, const int n, const double *ap, double *z, const int ldz,
+                                      double *w, void *wk, const size_t lwork, int *info,
+                                      const eigen_GPU_batch_opts *opts, const cudaStream_t stream);
+cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap, float *z, const int ldz, float *w,
+                                      void *wk, const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                      const cudaStream_t stream);
+
+/*
  * Symmetric matrix function of a solved batch (counterpart of the
  * reference's prototype symdmt.cu:5-80, z = a diag(d) a^T, and of the use
  * its README:171 names: powers such as the square root or the inverse):

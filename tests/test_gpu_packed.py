@@ -1,0 +1,48 @@
+"""Packed upper-triangle input (eigen_GPU_batch_packed_*): the same
+eigenpairs, bit for bit, as the full-storage solve of the same matrices,
+for every phase-1 form (warp, registers, shared-memory block with the band
+in global memory) and for Jacobi and n = 1; the packed input is not
+modified."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def E():
+    import eigeng_b200
+    return eigeng_b200
+
+
+@pytest.mark.parametrize("n,ldz", [(1, 1), (2, 3), (5, 5), (32, 32), (33, 35), (100, 100), (128, 129), (129, 129),
+                                   (200, 200), (256, 256)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_packed_matches_full(oracle_mod, n, ldz, dtype):
+    O = oracle_mod
+    L = 7
+    a0 = np.zeros((L, n, ldz))
+    a0[:, :, :n] = O.sym_uniform(L, n, seed=n + 17)
+    a = torch.from_numpy(a0.astype(dtype)).cuda()
+    ap = E().pack_upper(a, n, ldz)
+    ap0 = ap.clone()
+    z, w, info = E().solve_packed(ap, n, ldz)
+    wf, infof = E().solve(a, n, ldz)
+    torch.cuda.synchronize()
+    assert torch.equal(ap, ap0)
+    assert torch.equal(info, infof) and (info == 0).all()
+    assert torch.equal(w, wf)
+    assert torch.equal(z[:, :, :n], a[:, :, :n])
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_packed_other_methods(oracle_mod, method):
+    O = oracle_mod
+    n = 24
+    a = torch.from_numpy(O.sym_uniform(5, n, seed=3)).cuda()
+    ap = E().pack_upper(a, n)
+    z, w, info = E().solve_packed(ap, n, method=method)
+    wf, infof = E().solve(a, n, method=method)
+    torch.cuda.synchronize()
+    assert torch.equal(w, wf) and torch.equal(z, a) and torch.equal(info, infof)

@@ -245,6 +245,44 @@ def test_reference_check_api_writes_flags():
     assert flags[2, 0] > 0 and flags[2, 1] > 0
 
 
+@pytest.mark.parametrize("n,nm,m", [(20, 20, 20), (40, 43, 40), (100, 100, 77), (200, 201, 200)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_gate_norms_match_numpy(oracle_mod, n, nm, m, dtype):
+    """eigen_GPU_check_ex (one warp per matrix for n <= 32, tiled CTA form
+    above): ||A Z - Z D||_F over the first m pairs and ||Z^T Z - I||_F
+    (m x m) in FP64, on eigenvectors perturbed by ~1e-6 so that the norms
+    are far above rounding."""
+    import ctypes
+    import eigeng_b200 as e
+    O = oracle_mod
+    L = 5
+    a0 = np.zeros((L, n, nm))
+    a0[:, :, :n] = O.sym_uniform(L, n, seed=n + 1)
+    w, z, _ = gpu_solve(a0.astype(dtype), n, nm)
+    rng = np.random.default_rng(n)
+    zp = (z.astype(np.float64) + 1e-6 * rng.standard_normal(z.shape)).astype(dtype)
+    ad = torch.from_numpy(a0.astype(dtype)).cuda()
+    wd = torch.from_numpy(w).cuda()
+    zd = torch.from_numpy(np.ascontiguousarray(zp)).cuda()
+    e1 = torch.empty(L, dtype=torch.float64, device="cuda")
+    e2 = torch.empty(L, dtype=torch.float64, device="cuda")
+    fl = torch.empty(L, dtype=torch.int32, device="cuda")
+    sfx = "DP" if dtype == np.float64 else "FP"
+    P = ctypes.c_void_p
+    st = getattr(e.lib(), "eigen_GPU_check_ex_" + sfx)(L, nm, n, m, P(ad.data_ptr()), P(wd.data_ptr()),
+                                                       P(zd.data_ptr()), P(e1.data_ptr()), P(e2.data_ptr()),
+                                                       P(fl.data_ptr()), P(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert st == 0
+    A = np.transpose(a0.astype(dtype).astype(np.float64), (0, 2, 1))[:, :n, :n]
+    A = np.triu(A) + np.transpose(np.triu(A, 1), (0, 2, 1))
+    Z = np.transpose(zp.astype(np.float64), (0, 2, 1))[:, :n, :m]
+    D = w.astype(np.float64)[:, :m]
+    r1 = np.linalg.norm(A @ Z - Z * D[:, None, :], axis=(1, 2))
+    r2 = np.linalg.norm(np.transpose(Z, (0, 2, 1)) @ Z - np.eye(m)[None], axis=(1, 2))
+    assert np.allclose(e1.cpu().numpy(), r1, rtol=1e-6) and np.allclose(e2.cpu().numpy(), r2, rtol=1e-6)
+
+
 def test_invalid_arguments_rejected():
     import eigeng_b200 as e
     a = torch.zeros((2, 8, 8), dtype=torch.float64, device="cuda")
