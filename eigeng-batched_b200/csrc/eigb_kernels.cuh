@@ -62,7 +62,8 @@ constexpr int K1W_LD = 33;      // padded leading dimension, odd
 constexpr int K3W_NW = 4;       // warps per CTA in k3_warp
 constexpr int K3W_CH = 128;     // records staged per warp
 
-template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD * 32 + 32 + 32 + 72; }
+// per warp: S (K1W_LD x 32), beta[32], pv[32], red[72], ubuf[4*32], gram[3*32]
+template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD * 32 + 32 + 32 + 72 + 128 + 96; }
 
 // threads per row in k1_cta (column ranges split across warps)
 __host__ __device__ constexpr int k1_split(int n) { return n <= 256 ? 4 : (n <= 512 ? 2 : 1); }
@@ -89,6 +90,8 @@ __global__ void __launch_bounds__(32 * K1W_NW) k1_warp(const KP<T> p)
   T *beta_s = S + K1W_LD * 32;
   T *pv = beta_s + 32;
   T *red = pv + 32;
+  T *ubuf = red + 72;
+  T *gram = ubuf + 128;
   WarpTeam tm;
   const int n = p.n, nm = p.nm, r = tm.rank;
   T *A = p.a + (size_t)k * nm * n;
@@ -99,16 +102,17 @@ __global__ void __launch_bounds__(32 * K1W_NW) k1_warp(const KP<T> p)
   for (int c = 0; c < n; c++)
     if (r > c && r < n) S[r + c * K1W_LD] = S[c + r * K1W_LD];
   __syncwarp();
-  tridiag_qt<T, 1>(tm, S, K1W_LD, S, K1W_LD, n, n, p.d + k * n, p.e + k * n, beta_s, pv, pv, red);
+  tridiag_qt<T, 1>(tm, S, K1W_LD, S, K1W_LD, n, n, p.d + k * n, p.e + k * n, beta_s, pv, pv, red, ubuf, gram);
   if (r < n)
     for (int c = 0; c < n; c++) A[r + (size_t)c * nm] = S[r + c * K1W_LD];
 }
 
-// Shared-memory elements of k1_cta: red[72], beta[n], pv[n], part[nthreads]
-// and the leading B x B block of the matrix (leading dimension B|1).
+// Shared-memory elements of k1_cta: red[72], beta[n], pv[n],
+// part[TQ_QB*nthreads], ubuf[TQ_QB*n], gram[3n] and the leading B x B block
+// of the matrix (leading dimension B|1).
 __host__ __device__ inline size_t k1c_smem_elems(int n, int nthreads, int B)
 {
-  return 72 + 2 * (size_t)n + (size_t)nthreads + (size_t)B * (size_t)(B | 1);
+  return 72 + 2 * (size_t)n + (size_t)TQ_QB * nthreads + (size_t)(TQ_QB + 3) * n + (size_t)B * (size_t)(B | 1);
 }
 
 // One CTA per matrix; the leading p.k1b x p.k1b block of the matrix is
@@ -127,8 +131,10 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
   T *red = sm;          // 72
   T *beta_s = sm + 72;  // n
   T *pv = beta_s + n;   // n
-  T *part = pv + n;     // nt
-  T *S = part + nt;     // B x B
+  T *part = pv + n;     // TQ_QB * nt
+  T *ubuf = part + TQ_QB * nt;  // TQ_QB * n
+  T *gram = ubuf + TQ_QB * n;   // 3n
+  T *S = gram + 3 * n;  // B x B
   // full symmetric matrix from the upper triangle: the leading block in S
   // (coalesced reads), the outer band mirrored in place (or, from a packed
   // input, written to a in both triangles)
@@ -152,7 +158,7 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
   }
   __syncthreads();
   CtaTeam tm;
-  tridiag_qt<T, SPLIT>(tm, S, ld, A, nm, B, n, p.d + k * n, p.e + k * n, beta_s, pv, part, red);
+  tridiag_qt<T, SPLIT>(tm, S, ld, A, nm, B, n, p.d + k * n, p.e + k * n, beta_s, pv, part, red, ubuf, gram);
   // the storage holds M = Q^T; a receives Q: the leading block transposed
   // out of S, the outer band transposed in place (pairs (r, c), (c, r)
   // both lie outside the block)

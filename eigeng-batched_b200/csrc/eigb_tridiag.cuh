@@ -101,6 +101,56 @@ __host__ __device__ __forceinline__ void axpy_row(T *__restrict__ Sr, const size
   for (; lo < hi; lo++) Sr[(size_t)lo * ld] = fma(q, u[lo], Sr[(size_t)lo * ld]);
 }
 
+// Reflectors applied per barrier in the formation of M.
+constexpr int TQ_QB = 4;
+
+// a[j] += sum_{c in [lo,hi)} Sr[c] U[j][c] for the TQ_QB reflectors in U
+// (row stride nu): every element of the row is loaded once for all four
+template <class T>
+__host__ __device__ __forceinline__ void dot4_row(const T *__restrict__ Sr, const size_t ld, const T *__restrict__ U,
+                                                  const int nu, int lo, const int hi, T (&a)[TQ_QB])
+{
+  for (; lo + TQ_BATCH <= hi; lo += TQ_BATCH) {
+    T m[TQ_BATCH];
+#pragma unroll
+    for (int q = 0; q < TQ_BATCH; q++) m[q] = Sr[(size_t)(lo + q) * ld];
+#pragma unroll
+    for (int q = 0; q < TQ_BATCH; q++)
+#pragma unroll
+      for (int j = 0; j < TQ_QB; j++) a[j] = fma(m[q], U[j * nu + lo + q], a[j]);
+  }
+  for (; lo < hi; lo++) {
+    const T m = Sr[(size_t)lo * ld];
+#pragma unroll
+    for (int j = 0; j < TQ_QB; j++) a[j] = fma(m, U[j * nu + lo], a[j]);
+  }
+}
+
+// Sr[c] += sum_j q[j] U[j][c] for c in [lo, hi)
+template <class T>
+__host__ __device__ __forceinline__ void axpy4_row(T *__restrict__ Sr, const size_t ld, const T *__restrict__ U,
+                                                   const int nu, const T (&q)[TQ_QB], int lo, const int hi)
+{
+  for (; lo + TQ_BATCH <= hi; lo += TQ_BATCH) {
+    T m[TQ_BATCH];
+#pragma unroll
+    for (int x = 0; x < TQ_BATCH; x++) m[x] = Sr[(size_t)(lo + x) * ld];
+#pragma unroll
+    for (int x = 0; x < TQ_BATCH; x++) {
+      T v = m[x];
+#pragma unroll
+      for (int j = 0; j < TQ_QB; j++) v = fma(q[j], U[j * nu + lo + x], v);
+      Sr[(size_t)(lo + x) * ld] = v;
+    }
+  }
+  for (; lo < hi; lo++) {
+    T v = Sr[(size_t)lo * ld];
+#pragma unroll
+    for (int j = 0; j < TQ_QB; j++) v = fma(q[j], U[j * nu + lo], v);
+    Sr[(size_t)lo * ld] = v;
+  }
+}
+
 // Storage of tridiag_qt: element (r, c) is S[r + c*ld] (shared memory) when
 // r < B and c < B, else G[r + c*ldg] (global memory).  B = n keeps the whole
 // matrix in shared memory, B = 0 none of it; in between, the leading B x B
@@ -122,11 +172,12 @@ template <class T> struct HybridRow {
 // On exit d_out[0:n] = diagonal, e_out[0:n] = off-diagonal (e_out[k]
 // couples k and k+1, e_out[n-1] = 0, the reference's convention
 // tred1_tiled.hpp:207-212) and the storage holds M = Q^T with A = Q T Q^T.
-// Shared scratch: beta_s[n], pv[n], part[SPLIT*nr], red[72] (64 for team
-// reductions, red[64] carries the reflector pivot to the team).
+// Shared scratch: beta_s[n], pv[n], part[TQ_QB*SPLIT*nr], red[72] (64 for
+// team reductions, red[64] carries the reflector pivot to the team),
+// ubuf[TQ_QB*n] and gram[3n] for the formation of M.
 template <class T, int SPLIT, class Team>
 __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, T *G, const int ldg, const int B, const int n,
-                                    T *d_out, T *e_out, T *beta_s, T *pv, T *part, T *red)
+                                    T *d_out, T *e_out, T *beta_s, T *pv, T *part, T *red, T *ubuf, T *gram)
 {
   const int nt = tm.size();
   const int nr = nt / SPLIT;
@@ -207,44 +258,79 @@ __host__ __device__ void tridiag_qt(Team &tm, T *S, const int ld, T *G, const in
 
   // ---- M = H_1 H_2 ... H_{n-1}, built in the leading k x k block ----
   // Step k extends M_{k-1} by e_{k-1} (row and column k-1) and applies
-  // H_k from the right: M <- M + beta_k (M u) u^T, u = column k.  Every
-  // thread writes only the entries of its own row and column range, which
-  // are also the only entries it reads, so the extension needs no barrier.
-  for (int k = 1; k < n; k++) {
-    const T bk = beta_s[k];
-    const T *ucol = (k < B) ? S + (size_t)k * ld : G + (size_t)k * ldg;
+  // H_k from the right: M <- M + beta_k (M u) u^T, u = column k.  TQ_QB
+  // steps per block: the block's reflectors are copied aside (the
+  // extensions overwrite their columns), all its extensions are applied
+  // first (H_k leaves row and column k-1 alone, so they commute), then with
+  // a_j = M u_j for the M before the block,
+  //   q_j = beta_j (a_j + sum_{i<j} q_i (u_i . u_j)),  M += sum_j q_j u_j^T,
+  // from the Gram entries gram[3k + d - 1] = u_k . u_{k+d} computed here.
+  // Every thread writes only entries of its own row and column range.
+  for (int idx = t; idx < 3 * n; idx += nt) {
+    const int k = idx / 3, dd = idx % 3 + 1;
+    T g = T(0);
+    if (k >= 1 && k + dd < n) {
+      const T *uk = (k < B) ? S + (size_t)k * ld : G + (size_t)k * ldg;
+      const T *uj = (k + dd < B) ? S + (size_t)(k + dd) * ld : G + (size_t)(k + dd) * ldg;
+      for (int q = 0; q < k; q++) g = fma(uk[q], uj[q], g);
+    }
+    gram[idx] = g;
+  }
+  for (int k0 = 1; k0 < n; k0 += TQ_QB) {
+    const int kl = min(k0 + TQ_QB - 1, n - 1);  // last step of the block
+    for (int idx = t; idx < TQ_QB * n; idx += nt) {
+      const int j = idx / n, q = idx % n, k = k0 + j;
+      T v = T(0);
+      if (k <= kl && q < k) v = ((k < B) ? S + (size_t)k * ld : G + (size_t)k * ldg)[q];
+      ubuf[idx] = v;
+    }
+    tm.sync();  // the block's reflectors are aside; their columns may change
+    // this thread's columns for the whole block: the extensions, the
+    // products and the update below touch the same entries
     int lo, hi;
-    split_range<SPLIT>(k, h, lo, hi);
-    const int mid = max(lo, min(hi, Br));
-    if (r < k) {
-      if (k == 1) {
-        if (h == 0) row.at(0) = T(1);  // M_0 = [1]
-      } else if (r < k - 1) {
+    split_range<SPLIT>(kl, h, lo, hi);
+    for (int k = k0; k <= kl; k++) {
+      if (r < k - 1) {
         if (lo <= k - 1 && k - 1 < hi) row.at(k - 1) = T(0);
-      } else {  // r == k-1: row k-1 of the extension
-        for (int c = lo; c < hi; c++) row.at(c) = (c == k - 1) ? T(1) : T(0);
-      }
-      T q = dot_col(Sr, ld, ucol, lo, mid) + dot_col(Gr, ldg, ucol, mid, hi);
-      if (SPLIT > 1) {
-        part[h * nr + r] = q;
-      } else {
-        q *= bk;
-        axpy_row(Sr, (size_t)ld, ucol, q, lo, mid);
-        axpy_row(Gr, (size_t)ldg, ucol, q, mid, hi);
+      } else if (r == k - 1) {  // row k-1 of the extension (M_0 = [1] for k = 1)
+        for (int c = lo; c < min(hi, k); c++) row.at(c) = (c == k - 1) ? T(1) : T(0);
       }
     }
-    if (SPLIT > 1) {
-      tm.sync();
-      if (r < k) {
-        T q = T(0);
+    const int mid = max(lo, min(hi, Br));
+    T a[TQ_QB];
 #pragma unroll
-        for (int s = 0; s < SPLIT; s++) q += part[s * nr + r];
-        q *= bk;
-        axpy_row(Sr, (size_t)ld, ucol, q, lo, mid);
-        axpy_row(Gr, (size_t)ldg, ucol, q, mid, hi);
+    for (int j = 0; j < TQ_QB; j++) a[j] = T(0);
+    if (r < kl) {
+      dot4_row(Sr, (size_t)ld, ubuf, n, lo, mid, a);
+      dot4_row(Gr, (size_t)ldg, ubuf, n, mid, hi, a);
+      if (SPLIT > 1) {
+#pragma unroll
+        for (int j = 0; j < TQ_QB; j++) part[(j * SPLIT + h) * nr + r] = a[j];
       }
     }
-    tm.sync();  // column k is overwritten by the next extension; part is reused
+    if (SPLIT > 1) tm.sync();
+    if (r < kl) {
+      if (SPLIT > 1) {
+#pragma unroll
+        for (int j = 0; j < TQ_QB; j++) {
+          T x = T(0);
+#pragma unroll
+          for (int s2 = 0; s2 < SPLIT; s2++) x += part[(j * SPLIT + s2) * nr + r];
+          a[j] = x;
+        }
+      }
+      T q[TQ_QB];
+#pragma unroll
+      for (int j = 0; j < TQ_QB; j++) {
+        T x = a[j];
+#pragma unroll
+        for (int i2 = 0; i2 < j; i2++) x = fma(q[i2], gram[3 * (k0 + i2) + (j - i2) - 1], x);
+        q[j] = (k0 + j <= kl) ? beta_s[k0 + j] * x : T(0);
+      }
+      axpy4_row(Sr, (size_t)ld, ubuf, n, q, lo, mid);
+      axpy4_row(Gr, (size_t)ldg, ubuf, n, q, mid, hi);
+    }
+    tm.sync();  // ubuf and part are reused by the next block
   }
   if (r < n) {
     int lo, hi;

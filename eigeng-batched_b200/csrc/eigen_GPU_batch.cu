@@ -64,6 +64,27 @@ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 cudaEvent_t *g_trace = nullptr;
 int g_ntrace = 0;
 
+inline bool trace_on()
+{
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_trace != nullptr;
+}
+
+// second stream for the two-lane schedule, one per device, created once
+cudaStream_t g_lane[kMaxDev];
+cudaError_t lane_stream(cudaStream_t *out)
+{
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_lane[dev] == nullptr && (err = cudaStreamCreateWithFlags(&g_lane[dev], cudaStreamNonBlocking)) != cudaSuccess)
+    return err;
+  *out = g_lane[dev];
+  return cudaSuccess;
+}
+
 inline void trace(long chunk, int slot, cudaStream_t stream)
 {
   cudaEvent_t *ev;
@@ -349,37 +370,89 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   }
   if ((err = set_smem(k2_ql<T>, k2_smem)) != cudaSuccess) return err;
 
+  // the three phase launches of cnt matrices described by q, on st
+  auto phase1 = [&](const KP<T> &q, long cnt, cudaStream_t st) {
+    if (n <= 32) {
+      k1_warp<T><<<(unsigned)((cnt + K1W_NW - 1) / K1W_NW), 32 * K1W_NW, k1w_smem, st>>>(q);
+    } else if (k1_in_regs) {
+      launch_k1r<T>(q, (unsigned)cnt, k1c_smem, st);
+    } else {
+      launch_k1<T>(q, (unsigned)cnt, k1c_nt, k1c_smem, st);
+    }
+  };
+  auto phase2 = [&](const KP<T> &q, long cnt, cudaStream_t st) {
+    k2_ql<T><<<(unsigned)((cnt + k2_mpb - 1) / k2_mpb), 32 * (k2_mpb / q.k2mpw), k2_smem, st>>>(q);
+  };
+  auto phase3 = [&](const KP<T> &q, long cnt, cudaStream_t st) {
+    if (n <= 32) {
+      k3_warp<T><<<(unsigned)((cnt + K3W_NW - 1) / K3W_NW), 32 * K3W_NW, k3w_smem, st>>>(q);
+    } else if (zsm) {
+      k3_cta<T, true, 1><<<(unsigned)(cnt * pl.zsplit), k3_nt, k3c_smem, st>>>(q);
+    } else if (n > 512) {
+      k3_cta<T, false, 2><<<(unsigned)cnt, k3_nt, k3c_smem, st>>>(q);
+    } else {
+      k3_cta<T, false, 1><<<(unsigned)cnt, k3_nt, k3c_smem, st>>>(q);
+    }
+  };
+  // Two lanes per chunk (halves of its matrices) on the caller's stream and
+  // a second stream: the second lane starts after the first lane's phase
+  // 1, so each lane's latency-bound phase 2, which occupies few SMs, runs
+  // under the other lane's phase 1 or 3.  Not while the phase trace is on
+  // (the trace times the phases one after another).
+  const bool tracing = trace_on();
+  const long lane_min = 8L * dp.sms;
+  cudaStream_t s2 = nullptr;
+  if (!tracing && pl.Lc >= 2 * lane_min && (err = lane_stream(&s2)) != cudaSuccess) return err;
+
   for (long c0 = 0; c0 < L; c0 += pl.Lc) {
     const long lc = std::min(pl.Lc, L - c0);
     const long chunk = c0 / pl.Lc;
-    trace(chunk, 0, stream);
     p.a = a + (size_t)c0 * nm * n;
     p.w = w + (size_t)c0 * n;
     p.ap = ap ? ap + (size_t)c0 * packed_size(n) : nullptr;
     p.info = info ? info + c0 : nullptr;
     p.Lc = lc;
-    if (n <= 32) {
-      const unsigned nb = (unsigned)((lc + K1W_NW - 1) / K1W_NW);
-      k1_warp<T><<<nb, 32 * K1W_NW, k1w_smem, stream>>>(p);
-    } else if (k1_in_regs) {
-      launch_k1r<T>(p, (unsigned)lc, k1c_smem, stream);
+    if (s2 != nullptr && lc >= 2 * lane_min) {
+      const long m0 = lc / 2;
+      KP<T> pa = p, pb = p;
+      pa.Lc = m0;
+      pb.Lc = lc - m0;
+      pb.a += (size_t)m0 * nm * n;
+      pb.w += (size_t)m0 * n;
+      if (pb.ap) pb.ap += (size_t)m0 * packed_size(n);
+      if (pb.info) pb.info += m0;
+      pb.d += (size_t)m0 * n;
+      pb.e += (size_t)m0 * n;
+      pb.meta += m0;
+      pb.rec += (size_t)m0 * pl.rcap;
+      if (!zsm && n > 32) pb.zs += (size_t)m0 * n * n;
+      cudaEvent_t ev_k1 = nullptr, ev_done = nullptr;
+      if ((err = cudaEventCreateWithFlags(&ev_k1, cudaEventDisableTiming)) != cudaSuccess) return err;
+      if ((err = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming)) != cudaSuccess) {
+        cudaEventDestroy(ev_k1);
+        return err;
+      }
+      phase1(pa, m0, stream);
+      cudaEventRecord(ev_k1, stream);
+      cudaStreamWaitEvent(s2, ev_k1, 0);
+      phase2(pa, m0, stream);
+      phase3(pa, m0, stream);
+      phase1(pb, lc - m0, s2);
+      phase2(pb, lc - m0, s2);
+      phase3(pb, lc - m0, s2);
+      cudaEventRecord(ev_done, s2);
+      cudaStreamWaitEvent(stream, ev_done, 0);
+      cudaEventDestroy(ev_k1);  // released once the recorded work completes
+      cudaEventDestroy(ev_done);
     } else {
-      launch_k1<T>(p, (unsigned)lc, k1c_nt, k1c_smem, stream);
+      trace(chunk, 0, stream);
+      phase1(p, lc, stream);
+      trace(chunk, 1, stream);
+      phase2(p, lc, stream);
+      trace(chunk, 2, stream);
+      phase3(p, lc, stream);
+      trace(chunk, 3, stream);
     }
-    trace(chunk, 1, stream);
-    k2_ql<T><<<(unsigned)((lc + k2_mpb - 1) / k2_mpb), 32 * (k2_mpb / p.k2mpw), k2_smem, stream>>>(p);
-    trace(chunk, 2, stream);
-    if (n <= 32) {
-      const unsigned nb = (unsigned)((lc + K3W_NW - 1) / K3W_NW);
-      k3_warp<T><<<nb, 32 * K3W_NW, k3w_smem, stream>>>(p);
-    } else if (zsm) {
-      k3_cta<T, true, 1><<<(unsigned)(lc * pl.zsplit), k3_nt, k3c_smem, stream>>>(p);
-    } else if (n > 512) {
-      k3_cta<T, false, 2><<<(unsigned)lc, k3_nt, k3c_smem, stream>>>(p);
-    } else {
-      k3_cta<T, false, 1><<<(unsigned)lc, k3_nt, k3c_smem, stream>>>(p);
-    }
-    trace(chunk, 3, stream);
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
   }
   return cudaSuccess;

@@ -316,12 +316,17 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
     nbuf = min(3, nch)
     da = [torch.empty((C, n, nm), dtype=dt, device=dev) for _ in range(nbuf)]
     dw = [torch.empty((C, n), dtype=dt, device=dev) for _ in range(nbuf)]
-    info = torch.zeros(C, dtype=torch.int32, device=dev)
-    wk = workspace(C, nm, n, dt, dev) if method != JACOBI else None
-    s_in, s_run, s_out = (torch.cuda.Stream(dev) for _ in range(3))
+    # two compute streams with their own workspace: consecutive chunks solve
+    # concurrently, so one chunk's latency-bound QL phase (which occupies
+    # few SMs) overlaps the other chunk's reduction or apply phase
+    nrun = min(2, nch)
+    info = [torch.zeros(C, dtype=torch.int32, device=dev) for _ in range(nrun)]
+    wk = [workspace(C, nm, n, dt, dev) if method != JACOBI else None for _ in range(nrun)]
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    s_runs = [torch.cuda.Stream(dev) for _ in range(nrun)]
     start = torch.cuda.Event()
     start.record(caller)
-    for s_ in (s_in, s_run, s_out):
+    for s_ in [s_in, s_out] + s_runs:
         s_.wait_event(start)
     freed = [None] * nbuf       # copy-out of the buffer's previous chunk
     for i in range(nch):
@@ -334,9 +339,10 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
             da[b][:cnt].copy_(a_host[c0:c1], non_blocking=True)
         loaded = torch.cuda.Event()
         loaded.record(s_in)
+        s_run = s_runs[i % nrun]
         s_run.wait_event(loaded)
-        st = eigen_GPU_batch_ex(da[b][:cnt], dw[b][:cnt], wk, n, nm, n, info[:cnt], method, sort, max_sweep,
-                                s_run)
+        st = eigen_GPU_batch_ex(da[b][:cnt], dw[b][:cnt], wk[i % nrun], n, nm, n, info[i % nrun][:cnt], method,
+                                sort, max_sweep, s_run)
         if st != 0:
             raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
         solved = torch.cuda.Event()
@@ -352,7 +358,7 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
     caller.wait_event(done)
     # the device buffers are released only after the caller's stream has
     # waited for the last copy
-    for t in da + dw + [info] + ([wk] if wk is not None else []):
+    for t in da + dw + info + [x for x in wk if x is not None]:
         t.record_stream(caller)
     return w_host
 

@@ -40,7 +40,8 @@ template <class T, int SPLIT> static void run(int n, int nthr, T *G, int ldg, in
 {
   HostShared<T> sh(nthr);
   const int ld = B | 1;
-  std::vector<T> beta(n + 1), pv(n + 1), part(nthr), red(72), S((size_t)B * ld + 1);
+  std::vector<T> beta(n + 1), pv(n + 1), part(eigb::TQ_QB * nthr), red(72), S((size_t)B * ld + 1),
+      ubuf(eigb::TQ_QB * (size_t)n), gram(3 * (size_t)n);
   for (int c = 0; c < B; c++)
     for (int r = 0; r < B; r++) S[r + (size_t)c * ld] = G[r + (size_t)c * ldg];
   std::vector<std::thread> th;
@@ -48,7 +49,7 @@ template <class T, int SPLIT> static void run(int n, int nthr, T *G, int ldg, in
     th.emplace_back([&, t]() {
       HostTeam<T> tm{t, nthr, 0, &sh};
       eigb::tridiag_qt<T, SPLIT>(tm, S.data(), ld, G, ldg, B, n, d, e, beta.data(), pv.data(), part.data(),
-                                 red.data());
+                                 red.data(), ubuf.data(), gram.data());
     });
   for (auto &x : th) x.join();
   for (int c = 0; c < B; c++)
