@@ -64,27 +64,6 @@ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 cudaEvent_t *g_trace = nullptr;
 int g_ntrace = 0;
 
-inline bool trace_on()
-{
-  std::lock_guard<std::mutex> lk(g_mu);
-  return g_trace != nullptr;
-}
-
-// second stream for the two-lane schedule, one per device, created once
-cudaStream_t g_lane[kMaxDev];
-cudaError_t lane_stream(cudaStream_t *out)
-{
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
-  if (err != cudaSuccess) return err;
-  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (g_lane[dev] == nullptr && (err = cudaStreamCreateWithFlags(&g_lane[dev], cudaStreamNonBlocking)) != cudaSuccess)
-    return err;
-  *out = g_lane[dev];
-  return cudaSuccess;
-}
-
 inline void trace(long chunk, int slot, cudaStream_t stream)
 {
   cudaEvent_t *ev;
@@ -394,16 +373,6 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
       k3_cta<T, false, 1><<<(unsigned)cnt, k3_nt, k3c_smem, st>>>(q);
     }
   };
-  // Two lanes per chunk (halves of its matrices) on the caller's stream and
-  // a second stream: the second lane starts after the first lane's phase
-  // 1, so each lane's latency-bound phase 2, which occupies few SMs, runs
-  // under the other lane's phase 1 or 3.  Not while the phase trace is on
-  // (the trace times the phases one after another).
-  const bool tracing = trace_on();
-  const long lane_min = 8L * dp.sms;
-  cudaStream_t s2 = nullptr;
-  if (!tracing && pl.Lc >= 2 * lane_min && (err = lane_stream(&s2)) != cudaSuccess) return err;
-
   for (long c0 = 0; c0 < L; c0 += pl.Lc) {
     const long lc = std::min(pl.Lc, L - c0);
     const long chunk = c0 / pl.Lc;
@@ -412,47 +381,13 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     p.ap = ap ? ap + (size_t)c0 * packed_size(n) : nullptr;
     p.info = info ? info + c0 : nullptr;
     p.Lc = lc;
-    if (s2 != nullptr && lc >= 2 * lane_min) {
-      const long m0 = lc / 2;
-      KP<T> pa = p, pb = p;
-      pa.Lc = m0;
-      pb.Lc = lc - m0;
-      pb.a += (size_t)m0 * nm * n;
-      pb.w += (size_t)m0 * n;
-      if (pb.ap) pb.ap += (size_t)m0 * packed_size(n);
-      if (pb.info) pb.info += m0;
-      pb.d += (size_t)m0 * n;
-      pb.e += (size_t)m0 * n;
-      pb.meta += m0;
-      pb.rec += (size_t)m0 * pl.rcap;
-      if (!zsm && n > 32) pb.zs += (size_t)m0 * n * n;
-      cudaEvent_t ev_k1 = nullptr, ev_done = nullptr;
-      if ((err = cudaEventCreateWithFlags(&ev_k1, cudaEventDisableTiming)) != cudaSuccess) return err;
-      if ((err = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming)) != cudaSuccess) {
-        cudaEventDestroy(ev_k1);
-        return err;
-      }
-      phase1(pa, m0, stream);
-      cudaEventRecord(ev_k1, stream);
-      cudaStreamWaitEvent(s2, ev_k1, 0);
-      phase2(pa, m0, stream);
-      phase3(pa, m0, stream);
-      phase1(pb, lc - m0, s2);
-      phase2(pb, lc - m0, s2);
-      phase3(pb, lc - m0, s2);
-      cudaEventRecord(ev_done, s2);
-      cudaStreamWaitEvent(stream, ev_done, 0);
-      cudaEventDestroy(ev_k1);  // released once the recorded work completes
-      cudaEventDestroy(ev_done);
-    } else {
-      trace(chunk, 0, stream);
-      phase1(p, lc, stream);
-      trace(chunk, 1, stream);
-      phase2(p, lc, stream);
-      trace(chunk, 2, stream);
-      phase3(p, lc, stream);
-      trace(chunk, 3, stream);
-    }
+    trace(chunk, 0, stream);
+    phase1(p, lc, stream);
+    trace(chunk, 1, stream);
+    phase2(p, lc, stream);
+    trace(chunk, 2, stream);
+    phase3(p, lc, stream);
+    trace(chunk, 3, stream);
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
   }
   return cudaSuccess;

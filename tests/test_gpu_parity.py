@@ -372,22 +372,3 @@ def test_solve_host_matches_device_solve(oracle_mod):
     torch.cuda.synchronize()
     w2, _, _ = gpu_solve(a0.astype(np.float32), n, nm)
     assert np.array_equal(wf.numpy(), w2)
-
-
-@pytest.mark.parametrize("n", [24, 48, 136])
-def test_two_lane_schedule_is_bit_identical(oracle_mod, n):
-    """Large chunks run as two lanes on two streams (the second starting
-    after the first one's phase 1); with the phase trace on they run one
-    after another.  Both give identical results."""
-    O = oracle_mod
-    e = E()
-    sms = torch.cuda.get_device_properties(0).multi_processor_count
-    L = 16 * sms + 3                                   # above the two-lane threshold, odd split
-    a0 = O.sym_uniform(L, n, seed=n)
-    a1 = torch.from_numpy(a0.copy()).cuda()
-    w1, i1 = e.solve(a1, n)
-    a2 = torch.from_numpy(a0.copy()).cuda()
-    with e.PhaseTrace(4):
-        w2, i2 = e.solve(a2, n)
-    torch.cuda.synchronize()
-    assert torch.equal(w1, w2) and torch.equal(a1, a2) and torch.equal(i1, i2)
