@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--extra", action="store_true", help="also time n=32 (L=16384) and n=256 (L=2048)")
+    ap.add_argument("--uneven", type=int, default=0,
+                    help="mixed-size workload: this many matrices, n uniform in [8, 512], A = Q diag(l) Q^T")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
     return ap.parse_args()
 
@@ -318,10 +320,67 @@ def run_cusolver(args):
     lib.cusolverDnDestroy(h)
 
 
+def make_uneven(torch, L, dtype, seed, device):
+    """Mixed-size batch: n_k iid uniform in [8, 512]; A_k = Q diag(l) Q^T with
+    Q from the QR factorization of an iid N(0,1) matrix and l log-spaced
+    from 1 to 1e6 with random signs.  Returns (flat A, orders)."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(8, 513, size=L)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    parts = [None] * L
+    for n in np.unique(ns):
+        idx = np.nonzero(ns == n)[0]
+        x = torch.randn((len(idx), n, n), generator=g, dtype=torch.float64, device=device)
+        q, _ = torch.linalg.qr(x)
+        lam = torch.logspace(0, 6, int(n), dtype=torch.float64, device=device)
+        sgn = torch.where(torch.rand((len(idx), n), generator=g, device=device, dtype=torch.float64) < 0.5, -1.0, 1.0)
+        a = (q * (lam * sgn)[:, None, :]) @ q.transpose(1, 2)
+        a = 0.5 * (a + a.transpose(1, 2))
+        for j, k in enumerate(idx):
+            parts[k] = a[j].transpose(0, 1).reshape(-1)  # column-major
+    return torch.cat(parts).to(dtype).contiguous(), [int(x) for x in ns]
+
+
+def run_uneven_bench(args):
+    """Mixed-size batch through eigen_GPU_batch_uneven_* (inputs resident,
+    a fresh copy per step, CUDA events); one GPU."""
+    import torch
+    import eigeng_b200 as E
+    dt = torch.float64 if args.dtype == "f64" else torch.float32
+    dev = torch.device("cuda", 0)
+    base, ns = make_uneven(torch, args.uneven, dt, 1234, dev)
+    copies = [base.clone() for _ in range(args.steps + args.warmup)]
+    for i in range(args.warmup):
+        E.solve_uneven(copies[i], ns)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        w, info = E.solve_uneven(copies[args.warmup + i], ns)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    line = {"metric": f"eigendecomps/s (uneven n~U[8,512], {args.dtype}, L={args.uneven})",
+            "value": args.uneven / (ms / 1000.0), "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.dtype,
+            "data": "synthetic, seeded: Q diag(l) Q^T, l log-spaced 1..1e6 with random signs",
+            "config": {"workload": f"uneven L={args.uneven} n~U[8,512] {args.dtype} tql2 sorted",
+                       "elements": int(base.numel()), "distinct_n": len(set(ns))},
+            "info_nonzero": int((info != 0).sum().item())}
+    print(json.dumps(line), flush=True)
+    if args.out:
+        with open(args.out, "a") as f:
+            f.write(json.dumps(line) + "\n")
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.uneven:
+        return run_uneven_bench(args)
     if args.impl == "cusolver":
         return run_cusolver(args)
     import torch

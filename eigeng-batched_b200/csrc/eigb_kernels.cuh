@@ -42,6 +42,12 @@ template <class T> struct KP {
   int zsplit;    // ... and CTAs per matrix
   int k2mpw;     // phase 2: matrices per warp (1..32)
   const T *ap;   // packed upper-triangle input (nullptr: the upper triangle of a)
+  // uneven batches: matrix k of a launch is matrix kid[k] of the caller's
+  // batch, at a + aoff[kid[k]] (leading dimension nm = n), eigenvalues at
+  // w + woff[kid[k]], status at info[kid[k]]; nullptr: matrix k at
+  // a + k nm n, w + k n, info + k
+  const int *kid;
+  const long long *aoff, *woff;
   int *info;     // optional per-matrix status for the caller (may be null)
   long Lc;       // matrices in this chunk
   int n, nm;
@@ -50,6 +56,19 @@ template <class T> struct KP {
   int max_sweep;
   int sort;
 };
+
+template <class T> __device__ __forceinline__ T *mat_ptr(const KP<T> &p, long k)
+{
+  return p.kid ? p.a + p.aoff[p.kid[k]] : p.a + (size_t)k * p.nm * p.n;
+}
+template <class T> __device__ __forceinline__ T *val_ptr(const KP<T> &p, long k)
+{
+  return p.kid ? p.w + p.woff[p.kid[k]] : p.w + (size_t)k * p.n;
+}
+template <class T> __device__ __forceinline__ void put_info(const KP<T> &p, long k, int v)
+{
+  if (p.info) p.info[p.kid ? p.kid[k] : k] = v;
+}
 
 // Packed upper triangle (LAPACK 'U' order): element (r, c), r <= c, at
 // ap[r + c(c+1)/2]; matrix k starts at ap + k n(n+1)/2.
@@ -70,11 +89,13 @@ __host__ __device__ constexpr int k1_split(int n) { return n <= 256 ? 4 : (n <= 
 
 // ---------------------------------------------------------------- n == 1
 template <class T>
-__global__ void k_n1(const long L, const int nm, T *a, T *w, const T *ap)
+__global__ void k_n1(const KP<T> p)
 {
-  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < L; k += (long)gridDim.x * blockDim.x) {
-    w[k] = ap ? ap[k] : a[k * nm];
-    a[k * nm] = T(1);
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < p.Lc; k += (long)gridDim.x * blockDim.x) {
+    T *A = mat_ptr(p, k);
+    *val_ptr(p, k) = p.ap ? p.ap[k] : A[0];
+    A[0] = T(1);
+    put_info(p, k, 0);
   }
 }
 
@@ -94,7 +115,7 @@ __global__ void __launch_bounds__(32 * K1W_NW) k1_warp(const KP<T> p)
   T *gram = ubuf + 128;
   WarpTeam tm;
   const int n = p.n, nm = p.nm, r = tm.rank;
-  T *A = p.a + (size_t)k * nm * n;
+  T *A = mat_ptr(p, k);
   const T *Ap = p.ap ? p.ap + (size_t)k * packed_size(n) : nullptr;
   for (int c = 0; c < n; c++)
     if (r <= c) S[r + c * K1W_LD] = Ap ? Ap[packed_at(r, c)] : A[r + (size_t)c * nm];
@@ -126,7 +147,7 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
   const long k = blockIdx.x;
   const int n = p.n, nm = p.nm, t = threadIdx.x, nt = blockDim.x;
   const int B = p.k1b, ld = B | 1;
-  T *A = p.a + (size_t)k * nm * n;
+  T *A = mat_ptr(p, k);
   T *sm = reinterpret_cast<T *>(smem_raw);
   T *red = sm;          // 72
   T *beta_s = sm + 72;  // n
@@ -182,7 +203,7 @@ __global__ void __launch_bounds__(32 * NB * NB, 1) k1_reg(const KP<T> p)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long k = blockIdx.x;
   CtaTeam tm;
-  tridiag_qt_reg<T, NB>(tm, p.a + (size_t)k * p.nm * p.n, p.nm, p.n, p.d + k * p.n, p.e + k * p.n,
+  tridiag_qt_reg<T, NB>(tm, mat_ptr(p, k), p.nm, p.n, p.d + k * p.n, p.e + k * p.n,
                         reinterpret_cast<T *>(smem_raw), p.ap ? p.ap + (size_t)k * packed_size(p.n) : nullptr);
 }
 
@@ -323,14 +344,14 @@ __device__ __forceinline__ void k3w_writeback(const KP<T> &p, K3WSlot<T> &sl, co
       inv = (r < n) ? sl.inv[r] : r;
     }
   }
-  T *A = p.a + (size_t)k * nm * n;
+  T *A = mat_ptr(p, k);
 #pragma unroll
   for (int c = 0; c < 32; c++) {
     const int dst = __shfl_sync(0xffffffffu, inv, c);
     if (c < n && r < n) A[r + (size_t)dst * nm] = z[c];
   }
-  if (r < n) p.w[k * n + inv] = dr;
-  if (p.info && r == 0) p.info[k] = ierr;
+  if (r < n) val_ptr(p, k)[inv] = dr;
+  if (r == 0) put_info(p, k, ierr);
 }
 
 template <class T>
@@ -342,7 +363,7 @@ __global__ void __launch_bounds__(32 * K3W_NW) k3_warp(const KP<T> p)
   if (k >= p.Lc) return;
   K3WSlot<T> &sl = reinterpret_cast<K3WSlot<T> *>(smem_raw)[wid];
   const int n = p.n, nm = p.nm, r = threadIdx.x & 31;
-  const T *A = p.a + (size_t)k * nm * n;
+  const T *A = mat_ptr(p, k);
   // Z = Q: phase 1 left M = Q^T in a, so Z(r, c) = M(c, r) = a[c + r*nm]
   T z[32];
 #pragma unroll
@@ -675,7 +696,7 @@ __global__ void __launch_bounds__(SM ? 256 : 512, 1) k3_cta(const KP<T> p)
     rs = 1;
     cs = n;
   }
-  T *A = p.a + (size_t)k * nm * n;
+  T *A = mat_ptr(p, k);
   const Meta mt = p.meta[k];
   if (!mt.overflow) {  // first chunk of records, copied while Z is loaded
     const Rec<T> *src = p.rec + (size_t)k * p.rcap;
@@ -778,8 +799,8 @@ __global__ void __launch_bounds__(SM ? 256 : 512, 1) k3_cta(const KP<T> p)
       for (int c = 0; c < n; c++) A[r0 + row + (size_t)inv[c] * nm] = Z[row * rs + c * cs];
     }
   if (r0 == 0) {
-    for (int c = t; c < n; c += nt) p.w[k * n + inv[c]] = sd[c];
-    if (p.info && t == 0) p.info[k] = ierr;
+    for (int c = t; c < n; c += nt) val_ptr(p, k)[inv[c]] = sd[c];
+    if (t == 0) put_info(p, k, ierr);
   }
 }
 
@@ -802,7 +823,7 @@ __global__ void __launch_bounds__(32 * K1W_NW) k_jacobi_warp(const KP<T> p)
   T *As = sl.As, *Zs = sl.Zs;
   const int n = p.n, nm = p.nm, r = threadIdx.x & 31;
   const bool own = r < n;
-  T *A = p.a + (size_t)k * nm * n;
+  T *A = mat_ptr(p, k);
   // full symmetric matrix from the upper triangle; Z = I
   for (int c = 0; c < 32; c++) {
     T v = T(0);
@@ -914,8 +935,8 @@ __global__ void __launch_bounds__(32 * K1W_NW) k_jacobi_warp(const KP<T> p)
     const int dst = __shfl_sync(0xffffffffu, inv, c);
     if (own) A[r + (size_t)dst * nm] = Zs[r + c * 33];
   }
-  if (own) p.w[k * n + inv] = wr;
-  if (p.info && r == 0) p.info[k] = ierr;
+  if (own) val_ptr(p, k)[inv] = wr;
+  if (r == 0) put_info(p, k, ierr);
 }
 
 // ---------------------------------------------------------------- check

@@ -15,7 +15,9 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
+#include <vector>
 
 #include "eigb_kernels.cuh"
 #include "eigb_symfunc.cuh"
@@ -245,11 +247,19 @@ template <class T> void launch_k1(const KP<T> &p, unsigned blocks, int nt, size_
   else k1_cta<T, 1><<<blocks, nt, smem, st>>>(p);
 }
 
+// Uneven batches: the L matrices of a call are matrices kid[0..L) of the
+// caller's batch at a + aoff[.], w + woff[.], info[.] (see KP).
+struct Indirect {
+  const int *kid = nullptr;
+  const long long *aoff = nullptr, *woff = nullptr;
+};
+
 // ap: packed upper-triangle input (nullptr: the upper triangle of a); the
-// eigenvectors go to a either way
+// eigenvectors go to a either way.  ix: see Indirect.
 template <class T>
 cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork, int *info,
-                const eigen_GPU_batch_opts *opts, cudaStream_t stream, const T *ap = nullptr)
+                const eigen_GPU_batch_opts *opts, cudaStream_t stream, const T *ap = nullptr,
+                const Indirect &ix = Indirect())
 {
   if (bad_args(L, nm, n, m) || a == nullptr || w == nullptr) return cudaErrorInvalidValue;
   int method = EIGEN_GPU_BATCH_TQL2, sort = 1, max_sweep = 100;
@@ -261,18 +271,25 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   if (method < EIGEN_GPU_BATCH_TQL2 || method > EIGEN_GPU_BATCH_JACOBI) return cudaErrorInvalidValue;
   if (method == EIGEN_GPU_BATCH_JACOBI && n > 32) return cudaErrorInvalidValue;
   cudaError_t err;
+  KP<T> p{};
+  p.n = n;
+  p.nm = nm;
+  p.kid = ix.kid;
+  p.aoff = ix.aoff;
+  p.woff = ix.woff;
   if (n == 1) {
+    p.a = a;
+    p.w = w;
+    p.ap = ap;
+    p.info = info;
+    p.Lc = L;
     const int blocks = (int)std::min<long>((L + 255) / 256, 4096);
-    k_n1<T><<<blocks, 256, 0, stream>>>(L, nm, a, w, ap);
-    if (info) cudaMemsetAsync(info, 0, sizeof(int) * (size_t)L, stream);
+    k_n1<T><<<blocks, 256, 0, stream>>>(p);
     return cudaGetLastError();
   }
   DevProps dp;
   if ((err = dev_props(dp)) != cudaSuccess) return err;
 
-  KP<T> p{};
-  p.n = n;
-  p.nm = nm;
   p.method = (method == EIGEN_GPU_BATCH_IMTQL2) ? QL_IMTQL2 : QL_TQL2;
   p.max_sweep = max_sweep;
   p.sort = sort;
@@ -376,10 +393,18 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   for (long c0 = 0; c0 < L; c0 += pl.Lc) {
     const long lc = std::min(pl.Lc, L - c0);
     const long chunk = c0 / pl.Lc;
-    p.a = a + (size_t)c0 * nm * n;
-    p.w = w + (size_t)c0 * n;
-    p.ap = ap ? ap + (size_t)c0 * packed_size(n) : nullptr;
-    p.info = info ? info + c0 : nullptr;
+    if (ix.kid) {  // the index list advances instead of the pointers
+      p.a = a;
+      p.w = w;
+      p.info = info;
+      p.kid = ix.kid + c0;
+      p.ap = nullptr;
+    } else {
+      p.a = a + (size_t)c0 * nm * n;
+      p.w = w + (size_t)c0 * n;
+      p.ap = ap ? ap + (size_t)c0 * packed_size(n) : nullptr;
+      p.info = info ? info + c0 : nullptr;
+    }
     p.Lc = lc;
     trace(chunk, 0, stream);
     phase1(p, lc, stream);
@@ -391,6 +416,172 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
   }
   return cudaSuccess;
+}
+
+// ---- uneven batches ----
+//
+// Matrix k has order n_k (1 <= n_k <= 1024), column-major with leading
+// dimension n_k at a + sum_{j<k} n_j^2; its eigenvalues at w + sum_{j<k} n_j.
+// The host groups the matrices by order; each group runs the three phases
+// like a uniform batch (reaching its members through an index list) on one
+// of a few streams, groups placed longest-first (cost count * n^3), so that
+// the latency-bound steps of one group overlap the work of others.
+constexpr int kUnevenStreams = 8;
+
+struct UnevenGroup {
+  int n = 0, start = 0, count = 0, stream = 0;
+  eigen_GPU_batch_opts opts{};
+};
+struct UnevenPlan {
+  std::vector<int> kid;  // matrix indices, grouped
+  std::vector<long long> aoff, woff;
+  std::vector<UnevenGroup> groups;
+  int nstreams = 0;
+  size_t off_kid = 0, off_aoff = 0, off_woff = 0, off_slices = 0, slice = 0, bytes = 0;
+};
+
+template <class T>
+cudaError_t make_uneven_plan(long L, const int *n_host, const eigen_GPU_batch_opts *opts, UnevenPlan &up)
+{
+  if (L < 1 || n_host == nullptr) return cudaErrorInvalidValue;
+  const int method = opts ? opts->method : EIGEN_GPU_BATCH_TQL2;
+  std::map<int, std::vector<int>> by_n;
+  up.aoff.resize(L);
+  up.woff.resize(L);
+  long long ao = 0, wo = 0;
+  for (long k = 0; k < L; k++) {
+    const int n = n_host[k];
+    if (n < 1 || n > 1024) return cudaErrorInvalidValue;
+    if (method == EIGEN_GPU_BATCH_JACOBI && n > 32) return cudaErrorInvalidValue;
+    up.aoff[k] = ao;
+    up.woff[k] = wo;
+    ao += (long long)n * n;
+    wo += n;
+    by_n[n].push_back((int)k);
+  }
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  for (auto &g : by_n) {
+    UnevenGroup ug;
+    ug.n = g.first;
+    ug.start = (int)up.kid.size();
+    ug.count = (int)g.second.size();
+    up.kid.insert(up.kid.end(), g.second.begin(), g.second.end());
+    up.groups.push_back(ug);
+  }
+  // longest first onto the least loaded stream
+  std::sort(up.groups.begin(), up.groups.end(), [](const UnevenGroup &x, const UnevenGroup &y) {
+    return (double)x.count * x.n * x.n * x.n > (double)y.count * y.n * y.n * y.n;
+  });
+  up.nstreams = (int)std::min<size_t>(kUnevenStreams, up.groups.size());
+  std::vector<double> load(up.nstreams, 0.0);
+  std::vector<size_t> need(up.nstreams, 0);
+  const size_t cap = kWsBudget / kUnevenStreams;  // workspace per stream
+  for (auto &g : up.groups) {
+    const int s = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    g.stream = s;
+    load[s] += (double)g.count * g.n * g.n * g.n;
+    g.opts = opts ? *opts : eigen_GPU_batch_opts{};
+    if (!opts) g.opts.sort = 1;
+    if (g.n == 1 || method == EIGEN_GPU_BATCH_JACOBI) continue;  // no workspace
+    Plan<T> one;
+    eigen_GPU_batch_opts o1 = g.opts;
+    o1.chunk = 1;
+    if ((err = make_plan<T>(1, g.n, g.n, dp, one, &o1)) != cudaSuccess) return err;
+    const long fit = std::max<long>(1, (long)(cap / one.bytes));
+    g.opts.chunk = (int)std::min<long>(g.count, std::min<long>(fit, 1L << 30));
+    Plan<T> pl;
+    if ((err = make_plan<T>(g.count, g.n, g.n, dp, pl, &g.opts)) != cudaSuccess) return err;
+    need[s] = std::max(need[s], pl.bytes);
+  }
+  up.slice = align256(*std::max_element(need.begin(), need.end()));
+  size_t off = 0;
+  up.off_kid = off;
+  off = align256(off + sizeof(int) * (size_t)L);
+  up.off_aoff = off;
+  off = align256(off + sizeof(long long) * (size_t)L);
+  up.off_woff = off;
+  off = align256(off + sizeof(long long) * (size_t)L);
+  up.off_slices = off;
+  up.bytes = off + up.slice * up.nstreams;
+  return cudaSuccess;
+}
+
+// pool of streams for the groups of uneven batches, created once per device
+cudaStream_t g_ustream[kMaxDev][kUnevenStreams];
+cudaError_t uneven_streams(int count, cudaStream_t *out)
+{
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (int i = 0; i < count; i++) {
+    if (g_ustream[dev][i] == nullptr &&
+        (err = cudaStreamCreateWithFlags(&g_ustream[dev][i], cudaStreamNonBlocking)) != cudaSuccess)
+      return err;
+    out[i] = g_ustream[dev][i];
+  }
+  return cudaSuccess;
+}
+
+template <class T>
+cudaError_t uneven_buffer_size(long L, const int *n_host, const eigen_GPU_batch_opts *opts, size_t *lwork)
+{
+  if (lwork) *lwork = 0;
+  UnevenPlan up;
+  cudaError_t err = make_uneven_plan<T>(L, n_host, opts, up);
+  if (err == cudaSuccess && lwork) *lwork = up.bytes;
+  return err;
+}
+
+template <class T>
+cudaError_t run_uneven(long L, const int *n_host, T *a, T *w, void *wk, size_t lwork, int *info,
+                       const eigen_GPU_batch_opts *opts, cudaStream_t stream)
+{
+  if (a == nullptr || w == nullptr || wk == nullptr) return cudaErrorInvalidValue;
+  UnevenPlan up;
+  cudaError_t err = make_uneven_plan<T>(L, n_host, opts, up);
+  if (err != cudaSuccess) return err;
+  if (lwork < up.bytes) return cudaErrorInvalidValue;
+  char *base = static_cast<char *>(wk);
+  int *d_kid = reinterpret_cast<int *>(base + up.off_kid);
+  long long *d_aoff = reinterpret_cast<long long *>(base + up.off_aoff);
+  long long *d_woff = reinterpret_cast<long long *>(base + up.off_woff);
+  // from pageable host memory: the copies are staged before these calls return
+  if ((err = cudaMemcpyAsync(d_kid, up.kid.data(), sizeof(int) * (size_t)L, cudaMemcpyHostToDevice, stream)) ||
+      (err = cudaMemcpyAsync(d_aoff, up.aoff.data(), sizeof(long long) * (size_t)L, cudaMemcpyHostToDevice,
+                             stream)) ||
+      (err = cudaMemcpyAsync(d_woff, up.woff.data(), sizeof(long long) * (size_t)L, cudaMemcpyHostToDevice,
+                             stream)))
+    return err;
+  cudaStream_t st[kUnevenStreams];
+  if ((err = uneven_streams(up.nstreams, st)) != cudaSuccess) return err;
+  cudaEvent_t ev;
+  if ((err = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return err;
+  cudaEventRecord(ev, stream);  // the index lists and everything before on the caller's stream
+  for (int i = 0; i < up.nstreams; i++) cudaStreamWaitEvent(st[i], ev, 0);
+  cudaEventDestroy(ev);
+  for (const UnevenGroup &g : up.groups) {
+    Indirect ix;
+    ix.kid = d_kid + g.start;
+    ix.aoff = d_aoff;
+    ix.woff = d_woff;
+    void *slice = base + up.off_slices + up.slice * g.stream;
+    err = run<T>(g.count, g.n, g.n, g.n, a, w, slice, up.slice, info, &g.opts, st[g.stream], nullptr, ix);
+    if (err != cudaSuccess) break;
+  }
+  // the caller's stream waits for every group stream
+  for (int i = 0; i < up.nstreams; i++) {
+    cudaEvent_t done;
+    cudaError_t e2 = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
+    if (e2 != cudaSuccess) return e2;
+    cudaEventRecord(done, st[i]);
+    cudaStreamWaitEvent(stream, done, 0);
+    cudaEventDestroy(done);
+  }
+  return err;
 }
 
 template <class T>
@@ -582,6 +773,30 @@ cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap,
 {
   if (ap == nullptr) return cudaErrorInvalidValue;
   return eigb::run<float>(L, ldz, n, n, z, w, wk, lwork, info, opts, stream, ap);
+}
+
+cudaError_t eigen_GPU_batch_uneven_BufferSize_DP(const int L, const int *n, const eigen_GPU_batch_opts *opts,
+                                                 size_t *lwork)
+{
+  return eigb::uneven_buffer_size<double>(L, n, opts, lwork);
+}
+
+cudaError_t eigen_GPU_batch_uneven_BufferSize_FP(const int L, const int *n, const eigen_GPU_batch_opts *opts,
+                                                 size_t *lwork)
+{
+  return eigb::uneven_buffer_size<float>(L, n, opts, lwork);
+}
+
+cudaError_t eigen_GPU_batch_uneven_DP(const int L, const int *n, double *a, double *w, void *wk, const size_t lwork,
+                                      int *info, const eigen_GPU_batch_opts *opts, const cudaStream_t stream)
+{
+  return eigb::run_uneven<double>(L, n, a, w, wk, lwork, info, opts, stream);
+}
+
+cudaError_t eigen_GPU_batch_uneven_FP(const int L, const int *n, float *a, float *w, void *wk, const size_t lwork,
+                                      int *info, const eigen_GPU_batch_opts *opts, const cudaStream_t stream)
+{
+  return eigb::run_uneven<float>(L, n, a, w, wk, lwork, info, opts, stream);
 }
 
 cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, const int m, double *a, double *w,

@@ -64,6 +64,13 @@ def lib():
             f.argtypes = [I, I, I, I, P, P, P, P, P, P, P]
             f.restype = I
         for s_ in ("DP", "FP"):
+            f = getattr(L, "eigen_GPU_batch_uneven_BufferSize_" + s_)
+            f.argtypes = [I, P, ctypes.POINTER(Opts), ctypes.POINTER(SZ)]
+            f.restype = I
+            f = getattr(L, "eigen_GPU_batch_uneven_" + s_)
+            f.argtypes = [I, P, P, P, P, SZ, P, ctypes.POINTER(Opts), P]
+            f.restype = I
+        for s_ in ("DP", "FP"):
             f = getattr(L, "eigen_GPU_batch_packed_" + s_)
             f.argtypes = [I, I, P, P, I, P, P, SZ, P, ctypes.POINTER(Opts), P]
             f.restype = I
@@ -127,6 +134,8 @@ def exported_symbols():
         "eigen_GPU_batch_trace", "eigen_GPU_batch_noalloc_DP",
         "eigen_GPU_batch_symfunc_DP", "eigen_GPU_batch_symfunc_FP",
         "eigen_GPU_batch_packed_DP", "eigen_GPU_batch_packed_FP",
+        "eigen_GPU_batch_uneven_DP", "eigen_GPU_batch_uneven_FP",
+        "eigen_GPU_batch_uneven_BufferSize_DP", "eigen_GPU_batch_uneven_BufferSize_FP",
     ]
 
 
@@ -258,6 +267,32 @@ def solve_packed(ap, n, ldz=None, method=TQL2, sort=True, max_sweep=100, stream=
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_packed failed with cudaError {st}")
     return z, w, info
+
+
+def solve_uneven(a, ns, method=TQL2, sort=True, max_sweep=100, stream=None):
+    """eigen_GPU_batch_uneven: a is a flat CUDA tensor holding matrix k
+    (order ns[k], column-major, leading dimension ns[k]) at offset
+    sum_{j<k} ns[j]^2; solved in place.  Returns (w, info), w flat with the
+    eigenvalues of matrix k at sum_{j<k} ns[j]."""
+    nsa = (ctypes.c_int * len(ns))(*[int(x) for x in ns])
+    L = len(ns)
+    tot = sum(int(x) * int(x) for x in ns)
+    if not a.is_cuda or not a.is_contiguous() or a.numel() != tot:
+        raise EigenGError("a must be a contiguous CUDA tensor of sum(n^2) elements")
+    o = Opts(method, 1 if sort else 0, max_sweep, 0, 0, 0)
+    sfx = _sfx(a.dtype)
+    lw = ctypes.c_size_t(0)
+    st = getattr(lib(), "eigen_GPU_batch_uneven_BufferSize_" + sfx)(L, nsa, ctypes.byref(o), ctypes.byref(lw))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_uneven_BufferSize failed with cudaError {st}")
+    wk = torch.empty(max(lw.value, 16), dtype=torch.uint8, device=a.device)
+    w = torch.empty(sum(int(x) for x in ns), dtype=a.dtype, device=a.device)
+    info = torch.zeros(L, dtype=torch.int32, device=a.device)
+    st = getattr(lib(), "eigen_GPU_batch_uneven_" + sfx)(L, nsa, _ptr(a), _ptr(w), _ptr(wk), lw.value, _ptr(info),
+                                                        ctypes.byref(o), _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_uneven failed with cudaError {st}")
+    return w, info
 
 
 FUNC_DIAG, FUNC_POW, FUNC_EXP = 0, 1, 2

@@ -143,6 +143,28 @@ cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap,
                                       const cudaStream_t stream);
 
 /*
+ * Uneven batches (BASELINE's mixed-size case; the reference API is
+ * uniform-n, so its users group by n and call once per size).  Matrix k has
+ * order n[k] (1..1024, n is a HOST array of L ints) and is stored
+ * column-major with leading dimension n[k] at a + sum_{j<k} n[j]^2; its
+ * eigenvalues go to w + sum_{j<k} n[j] and its status to info[k] (device,
+ * optional).  The matrices are grouped by order and the groups run
+ * concurrently on internal streams; the call is asynchronous with respect to
+ * the host except for three small index copies from host memory, and the
+ * caller's stream waits for all of it.  Results equal eigen_GPU_batch_ex_*
+ * on each matrix.  Options as eigen_GPU_batch_ex_* (chunk is chosen per
+ * group); lwork from eigen_GPU_batch_uneven_BufferSize_*.
+ */
+cudaError_t eigen_GPU_batch_uneven_BufferSize_DP(const int L, const int *n, const eigen_GPU_batch_opts *opts,
+                                                 size_t *lwork);
+cudaError_t eigen_GPU_batch_uneven_BufferSize_FP(const int L, const int *n, const eigen_GPU_batch_opts *opts,
+                                                 size_t *lwork);
+cudaError_t eigen_GPU_batch_uneven_DP(const int L, const int *n, double *a, double *w, void *wk, const size_t lwork,
+                                      int *info, const eigen_GPU_batch_opts *opts, const cudaStream_t stream);
+cudaError_t eigen_GPU_batch_uneven_FP(const int L, const int *n, float *a, float *w, void *wk, const size_t lwork,
+                                      int *info, const eigen_GPU_batch_opts *opts, const cudaStream_t stream);
+
+/*
  * Symmetric matrix function of a solved batch (counterpart of the
  * reference's prototype symdmt.cu:5-80, z = a diag(d) a^T, and of the use
  * its README:171 names: powers such as the square root or the inverse):
