@@ -426,7 +426,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
 // like a uniform batch (reaching its members through an index list) on one
 // of a few streams, groups placed longest-first (cost count * n^3), so that
 // the latency-bound steps of one group overlap the work of others.
-constexpr int kUnevenStreams = 8;
+constexpr int kUnevenStreams = 32;
 
 struct UnevenGroup {
   int n = 0, start = 0, count = 0, stream = 0;
