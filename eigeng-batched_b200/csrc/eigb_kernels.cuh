@@ -939,6 +939,30 @@ __global__ void __launch_bounds__(32 * K1W_NW) k_jacobi_warp(const KP<T> p)
   if (r == 0) put_info(p, k, ierr);
 }
 
+// ---------------------------------------------------------------- layouts
+// Transpose of a rows x cols row-major matrix (in[r*cols + c] ->
+// out[c*rows + r]) through 32 x 33 shared-memory tiles, coalesced on both
+// sides.  Converts between the interleaved layout (element e of all
+// matrices contiguous: x[e*L + k]) and the matrix-by-matrix one
+// (x[k*E + e]), in either direction.
+template <class T>
+__global__ void __launch_bounds__(256) k_transpose(const long rows, const long cols, const T *__restrict__ in,
+                                                   T *__restrict__ out)
+{
+  __shared__ T tile[32][33];
+  const long r0 = (long)blockIdx.y * 32, c0 = (long)blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  for (int y = ty; y < 32; y += 8) {
+    const long r = r0 + y, c = c0 + tx;
+    if (r < rows && c < cols) tile[y][tx] = in[r * cols + c];
+  }
+  __syncthreads();
+  for (int y = ty; y < 32; y += 8) {
+    const long c = c0 + y, r = r0 + tx;
+    if (r < rows && c < cols) out[c * rows + r] = tile[tx][y];
+  }
+}
+
 // ---------------------------------------------------------------- check
 // Residual ||A Z - Z D||_F and orthogonality ||Z^T Z - I||_F (off-diagonal
 // terms twice) in FP64 per matrix, one warp per matrix, following

@@ -418,6 +418,53 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   return cudaSuccess;
 }
 
+// ---- interleaved layout ----
+//
+// Element (i, j) of matrix k at ai[(i + j*n)*L + k], eigenvalue j of matrix
+// k at wi[j*L + k].  Transposed into the workspace, solved there, and
+// transposed back.
+template <class T> cudaError_t transpose(long rows, long cols, const T *in, T *out, cudaStream_t st)
+{
+  const long gx = (cols + 31) / 32, gy = (rows + 31) / 32;
+  if (gx > 0x7fffffffL || gy > 65535) return cudaErrorInvalidValue;
+  k_transpose<T><<<dim3((unsigned)gx, (unsigned)gy), 256, 0, st>>>(rows, cols, in, out);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t interleaved_plan(long L, int n, const eigen_GPU_batch_opts *opts, size_t &off_w, size_t &off_ws,
+                             size_t &bytes)
+{
+  size_t inner = 0;
+  cudaError_t err = buffer_size<T>(L, n, n, n, &inner, opts);
+  if (err != cudaSuccess) return err;
+  off_w = align256(sizeof(T) * (size_t)L * n * n);
+  off_ws = align256(off_w + sizeof(T) * (size_t)L * n);
+  bytes = off_ws + inner;
+  return cudaSuccess;
+}
+
+template <class T>
+cudaError_t run_interleaved(long L, int n, const T *ai, T *zi, T *wi, void *wk, size_t lwork, int *info,
+                            const eigen_GPU_batch_opts *opts, cudaStream_t stream)
+{
+  if (bad_args(L, n, n, n) || ai == nullptr || zi == nullptr || wi == nullptr || wk == nullptr)
+    return cudaErrorInvalidValue;
+  size_t off_w, off_ws, bytes;
+  cudaError_t err = interleaved_plan<T>(L, n, opts, off_w, off_ws, bytes);
+  if (err != cudaSuccess) return err;
+  if (lwork < bytes) return cudaErrorInvalidValue;
+  char *base = static_cast<char *>(wk);
+  T *a = reinterpret_cast<T *>(base);
+  T *w = reinterpret_cast<T *>(base + off_w);
+  const long E = (long)n * n;
+  if ((err = transpose<T>(E, L, ai, a, stream)) != cudaSuccess) return err;  // (E x L) -> (L x E)
+  if ((err = run<T>(L, n, n, n, a, w, base + off_ws, lwork - off_ws, info, opts, stream)) != cudaSuccess)
+    return err;
+  if ((err = transpose<T>(L, E, a, zi, stream)) != cudaSuccess) return err;  // (L x E) -> (E x L)
+  return transpose<T>(L, n, w, wi, stream);
+}
+
 // ---- uneven batches ----
 //
 // Matrix k has order n_k (1 <= n_k <= 1024), column-major with leading
@@ -773,6 +820,38 @@ cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap,
 {
   if (ap == nullptr) return cudaErrorInvalidValue;
   return eigb::run<float>(L, ldz, n, n, z, w, wk, lwork, info, opts, stream, ap);
+}
+
+cudaError_t eigen_GPU_batch_interleaved_BufferSize_DP(const int L, const int n, const eigen_GPU_batch_opts *opts,
+                                                      size_t *lwork)
+{
+  size_t a, b, bytes = 0;
+  const cudaError_t err = eigb::interleaved_plan<double>(L, n, opts, a, b, bytes);
+  if (lwork) *lwork = err == cudaSuccess ? bytes : 0;
+  return err;
+}
+
+cudaError_t eigen_GPU_batch_interleaved_BufferSize_FP(const int L, const int n, const eigen_GPU_batch_opts *opts,
+                                                      size_t *lwork)
+{
+  size_t a, b, bytes = 0;
+  const cudaError_t err = eigb::interleaved_plan<float>(L, n, opts, a, b, bytes);
+  if (lwork) *lwork = err == cudaSuccess ? bytes : 0;
+  return err;
+}
+
+cudaError_t eigen_GPU_batch_interleaved_DP(const int L, const int n, const double *ai, double *zi, double *wi,
+                                           void *wk, const size_t lwork, int *info,
+                                           const eigen_GPU_batch_opts *opts, const cudaStream_t stream)
+{
+  return eigb::run_interleaved<double>(L, n, ai, zi, wi, wk, lwork, info, opts, stream);
+}
+
+cudaError_t eigen_GPU_batch_interleaved_FP(const int L, const int n, const float *ai, float *zi, float *wi,
+                                           void *wk, const size_t lwork, int *info,
+                                           const eigen_GPU_batch_opts *opts, const cudaStream_t stream)
+{
+  return eigb::run_interleaved<float>(L, n, ai, zi, wi, wk, lwork, info, opts, stream);
 }
 
 cudaError_t eigen_GPU_batch_uneven_BufferSize_DP(const int L, const int *n, const eigen_GPU_batch_opts *opts,

@@ -64,6 +64,13 @@ def lib():
             f.argtypes = [I, I, I, I, P, P, P, P, P, P, P]
             f.restype = I
         for s_ in ("DP", "FP"):
+            f = getattr(L, "eigen_GPU_batch_interleaved_BufferSize_" + s_)
+            f.argtypes = [I, I, ctypes.POINTER(Opts), ctypes.POINTER(SZ)]
+            f.restype = I
+            f = getattr(L, "eigen_GPU_batch_interleaved_" + s_)
+            f.argtypes = [I, I, P, P, P, P, SZ, P, ctypes.POINTER(Opts), P]
+            f.restype = I
+        for s_ in ("DP", "FP"):
             f = getattr(L, "eigen_GPU_batch_uneven_BufferSize_" + s_)
             f.argtypes = [I, P, ctypes.POINTER(Opts), ctypes.POINTER(SZ)]
             f.restype = I
@@ -136,6 +143,8 @@ def exported_symbols():
         "eigen_GPU_batch_packed_DP", "eigen_GPU_batch_packed_FP",
         "eigen_GPU_batch_uneven_DP", "eigen_GPU_batch_uneven_FP",
         "eigen_GPU_batch_uneven_BufferSize_DP", "eigen_GPU_batch_uneven_BufferSize_FP",
+        "eigen_GPU_batch_interleaved_DP", "eigen_GPU_batch_interleaved_FP",
+        "eigen_GPU_batch_interleaved_BufferSize_DP", "eigen_GPU_batch_interleaved_BufferSize_FP",
     ]
 
 
@@ -267,6 +276,30 @@ def solve_packed(ap, n, ldz=None, method=TQL2, sort=True, max_sweep=100, stream=
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_packed failed with cudaError {st}")
     return z, w, info
+
+
+def solve_interleaved(ai, n, method=TQL2, sort=True, max_sweep=100, stream=None):
+    """eigen_GPU_batch_interleaved: ai is a CUDA tensor of shape (n*n, L) with
+    element (i, j) of matrix k at ai[i + j*n, k]; returns (zi, wi, info) in
+    the same layout (wi of shape (n, L))."""
+    if not ai.is_cuda or not ai.is_contiguous() or ai.dim() != 2 or ai.shape[0] != n * n:
+        raise EigenGError("ai must be a contiguous CUDA tensor of shape (n*n, L)")
+    L = ai.shape[1]
+    o = Opts(method, 1 if sort else 0, max_sweep, 0, 0, 0)
+    sfx = _sfx(ai.dtype)
+    lw = ctypes.c_size_t(0)
+    st = getattr(lib(), "eigen_GPU_batch_interleaved_BufferSize_" + sfx)(L, n, ctypes.byref(o), ctypes.byref(lw))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_interleaved_BufferSize failed with cudaError {st}")
+    wk = torch.empty(max(lw.value, 16), dtype=torch.uint8, device=ai.device)
+    zi = torch.empty_like(ai)
+    wi = torch.empty((n, L), dtype=ai.dtype, device=ai.device)
+    info = torch.zeros(L, dtype=torch.int32, device=ai.device)
+    st = getattr(lib(), "eigen_GPU_batch_interleaved_" + sfx)(L, n, _ptr(ai), _ptr(zi), _ptr(wi), _ptr(wk), lw.value,
+                                                             _ptr(info), ctypes.byref(o), _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_interleaved failed with cudaError {st}")
+    return zi, wi, info
 
 
 def solve_uneven(a, ns, method=TQL2, sort=True, max_sweep=100, stream=None):

@@ -143,6 +143,27 @@ cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap,
                                       const cudaStream_t stream);
 
 /*
+ * Interleaved layout (the reference's README:166 "flexible interleave data
+ * format", not in its code): element (i, j) of matrix k (0-based) at
+ * ai[(i + j*n)*L + k], i.e. the same element of every matrix contiguous, as
+ * SIMD-per-matrix codes keep them; eigenvector element (i, j) returned the
+ * same way in zi (may equal ai), eigenvalue j of matrix k at wi[j*L + k].
+ * The batch is transposed on the device into the workspace, solved there
+ * (results equal eigen_GPU_batch_ex_* on the same matrices) and transposed
+ * back.  lwork from eigen_GPU_batch_interleaved_BufferSize_*.
+ */
+cudaError_t eigen_GPU_batch_interleaved_BufferSize_DP(const int L, const int n, const eigen_GPU_batch_opts *opts,
+                                                      size_t *lwork);
+cudaError_t eigen_GPU_batch_interleaved_BufferSize_FP(const int L, const int n, const eigen_GPU_batch_opts *opts,
+                                                      size_t *lwork);
+cudaError_t eigen_GPU_batch_interleaved_DP(const int L, const int n, const double *ai, double *zi, double *wi,
+                                           void *wk, const size_t lwork, int *info,
+                                           const eigen_GPU_batch_opts *opts, const cudaStream_t stream);
+cudaError_t eigen_GPU_batch_interleaved_FP(const int L, const int n, const float *ai, float *zi, float *wi,
+                                           void *wk, const size_t lwork, int *info,
+                                           const eigen_GPU_batch_opts *opts, const cudaStream_t stream);
+
+/*
  * Uneven batches (BASELINE's mixed-size case; the reference API is
  * uniform-n, so its users group by n and call once per size).  Matrix k has
  * order n[k] (1..1024, n is a HOST array of L ints) and is stored

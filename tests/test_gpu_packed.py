@@ -1,4 +1,5 @@
-"""Packed upper-triangle input (eigen_GPU_batch_packed_*): the same
+"""Packed upper-triangle input (eigen_GPU_batch_packed_*) and the
+interleaved layout (eigen_GPU_batch_interleaved_*): the same
 eigenpairs, bit for bit, as the full-storage solve of the same matrices,
 for every phase-1 form (warp, registers, shared-memory block with the band
 in global memory) and for Jacobi and n = 1; the packed input is not
@@ -46,3 +47,18 @@ def test_packed_other_methods(oracle_mod, method):
     wf, infof = E().solve(a, n, method=method)
     torch.cuda.synchronize()
     assert torch.equal(w, wf) and torch.equal(z, a) and torch.equal(info, infof)
+
+
+@pytest.mark.parametrize("n,L", [(1, 7), (5, 33), (32, 100), (64, 70), (130, 45), (256, 9)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_interleaved_matches_full(oracle_mod, n, L, dtype):
+    O = oracle_mod
+    a0 = O.sym_uniform(L, n, seed=n + 5).astype(dtype)       # (L, n, n) column-major matrices
+    a = torch.from_numpy(a0.copy()).cuda()
+    ai = a.reshape(L, n * n).t().contiguous()                 # element e of matrix k at ai[e, k]
+    zi, wi, info = E().solve_interleaved(ai, n)
+    wf, infof = E().solve(a, n)
+    torch.cuda.synchronize()
+    assert torch.equal(info, infof) and (info == 0).all()
+    assert torch.equal(wi.t(), wf)
+    assert torch.equal(zi.t().reshape(L, n, n), a)
