@@ -393,7 +393,9 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
-        dist.init_process_group("nccl", device_id=dev)
+        import datetime
+        # short: a rank that fails makes the others' next collective fail too
+        dist.init_process_group("nccl", device_id=dev, timeout=datetime.timedelta(seconds=300))
 
     def barrier():
         if world > 1:
@@ -511,7 +513,7 @@ def main():
         line["e2e"] = {"value": world * L * args.steps / (ems / 1000.0), "unit": "matrices/s",
                        "h2d_bytes_per_step": L * n * n * esize, "d2h_bytes_per_step": L * n * n * esize + L * n * esize}
 
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline is an N=1 figure
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
         nth = os.cpu_count() or 1
