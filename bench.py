@@ -158,7 +158,7 @@ def measured_traffic(kernel, dtype, n):
 
 
 def alg_bytes(n, esize):
-    """Compulsory bytes per matrix: read A, write V and w (SURVEY 8(d) model)."""
+    """Compulsory bytes per matrix: read A, write V and w."""
     return esize * (2 * n * n + n)
 
 

@@ -164,7 +164,7 @@ cudaError_t eigen_GPU_batch_interleaved_FP(const int L, const int n, const float
                                            const eigen_GPU_batch_opts *opts, const cudaStream_t stream);
 
 /*
- * Uneven batches (BASELINE's mixed-size case; the reference API is
+ * Uneven batches (mixed sizes in one call; the reference API is
  * uniform-n, so its users group by n and call once per size).  Matrix k has
  * order n[k] (1..1024, n is a HOST array of L ints) and is stored
  * column-major with leading dimension n[k] at a + sum_{j<k} n[j]^2; its
