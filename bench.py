@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--method", default="tql2", choices=["tql2", "imtql2", "jacobi"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--extra", action="store_true", help="also time n=32 (L=16384) and n=256 (L=2048)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the n=32 (L=16384) and n=256 (L=2048) FP64 figures added to the line")
     ap.add_argument("--uneven", type=int, default=0,
                     help="mixed-size workload: this many matrices, n uniform in [8, 512], A = Q diag(l) Q^T")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
@@ -512,6 +513,35 @@ def main():
             ems = float(tt.item())
         line["e2e"] = {"value": world * L * args.steps / (ems / 1000.0), "unit": "matrices/s",
                        "h2d_bytes_per_step": L * n * n * esize, "d2h_bytes_per_step": L * n * n * esize + L * n * esize}
+
+    if not args.no_extra:
+        # the metric's other sizes, same timing rules (fresh copy per step,
+        # warm-up, CUDA events on the launching stream, max over ranks)
+        sizes = {}
+        for n2, L2 in ((32, 16384), (256, 2048)):
+            if n2 == n and dt == torch.float64:
+                continue
+            b2 = make_batch(torch, "symu", L2, n2, torch.float64, seed=99 + rank, device=dev)
+            cps = [b2.clone() for _ in range(args.steps + args.warmup)]
+            w2 = torch.empty((L2, n2), dtype=torch.float64, device=dev)
+            wk2 = E.workspace(L2, n2, n2, torch.float64, dev)
+            for i in range(args.warmup):
+                E.eigen_GPU_batch_ex(cps[i], w2, wk2, n2, stream=stream)
+            barrier()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for i in range(args.steps):
+                E.eigen_GPU_batch_ex(cps[args.warmup + i], w2, wk2, n2, stream=stream)
+            f1.record(stream)
+            barrier()
+            ms2 = f0.elapsed_time(f1)
+            if world > 1:
+                tt = torch.tensor([ms2], dtype=torch.float64, device=dev)
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                ms2 = float(tt.item())
+            sizes[f"n{n2}_f64_L{L2}"] = world * L2 * args.steps / (ms2 / 1000.0)
+            del cps, wk2
+        line["sizes"] = {"unit": "matrices/s", "data": "synthetic (B + B^T)/2, B iid U[-1,1]", **sizes}
 
     if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline is an N=1 figure
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
