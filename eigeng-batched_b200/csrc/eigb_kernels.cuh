@@ -197,8 +197,15 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
 
 // Register-resident phase 1 for 32 < n <= 32*NB, one CTA of NB*NB warps
 // per matrix (eigb_tridiag_reg.cuh).
+// CTAs of k1_reg wanted per SM: the step chain is latency-bound, so small
+// forms keep several matrices per SM (bounding registers accordingly)
+template <class T> __host__ __device__ constexpr int k1r_min_blocks(int nb)
+{
+  return sizeof(T) == 4 ? (nb == 2 ? 4 : (nb == 3 ? 2 : 1)) : (nb == 2 ? 3 : 1);
+}
+
 template <class T, int NB>
-__global__ void __launch_bounds__(32 * NB * NB, 1) k1_reg(const KP<T> p)
+__global__ void __launch_bounds__(32 * NB * NB, k1r_min_blocks<T>(NB)) k1_reg(const KP<T> p)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const long k = blockIdx.x;
