@@ -197,11 +197,15 @@ __global__ void __launch_bounds__(1024) k1_cta(const KP<T> p)
 
 // Register-resident phase 1 for 32 < n <= 32*NB, one CTA of NB*NB warps
 // per matrix (eigb_tridiag_reg.cuh).
-// CTAs of k1_reg wanted per SM: the step chain is latency-bound, so small
-// forms keep several matrices per SM (bounding registers accordingly)
+// CTAs of k1_reg wanted per SM (registers are bounded accordingly): the
+// step chain is latency-bound, and more matrices per SM pay even where the
+// tighter bound costs spills.  Measured on B200 (phase 1, ms):
+//   FP32 n=64: 18.8 (1 CTA/SM bound) -> 8.5 (8); n=96: 14.7 (2) -> 10.2 (3);
+//   n=128: 5.7 (1) -> 4.1 (2).  FP64 n=64: 6.6 (2) -> 4.4 (4); n=96: 13.0
+//   (1) -> 9.9 (2); n=128: 8.4 (1), 19.9 with 2.
 template <class T> __host__ __device__ constexpr int k1r_min_blocks(int nb)
 {
-  return sizeof(T) == 4 ? (nb == 2 ? 4 : (nb == 3 ? 2 : 1)) : (nb == 2 ? 3 : 1);
+  return sizeof(T) == 4 ? (nb == 2 ? 8 : (nb == 3 ? 3 : 2)) : (nb == 2 ? 4 : (nb == 3 ? 2 : 1));
 }
 
 template <class T, int NB>
