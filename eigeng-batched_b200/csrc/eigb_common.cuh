@@ -227,6 +227,21 @@ struct CtaTeam {
     for (int k = 0; k < nw; k++) s += buf[k];
     return s;
   }
+  // A sum split around a barrier the caller places: post() (called by whole
+  // warps) stores the warp's sum of x in buf[warp]; after the next sync(),
+  // total() adds the slots of warps w0 .. w0+nw-1.  `id` names the buffer
+  // for the host emulation of a team, which keeps one slot per thread.
+  template <class T> __device__ __forceinline__ void post(T x, T *buf, int) const
+  {
+    x = warp_sum(x);
+    if ((rank & 31) == 0) buf[rank >> 5] = x;
+  }
+  template <class T> __device__ __forceinline__ T total(const T *buf, int, const int w0, const int nw) const
+  {
+    T s = T(0);
+    for (int k = 0; k < nw; k++) s += buf[w0 + k];
+    return s;
+  }
 };
 
 }  // namespace eigb

@@ -79,20 +79,15 @@ __host__ __device__ __forceinline__ T reg_symv(const T (&S)[32], const T *Vc, co
   return (a0 + a1) + (a2 + a3);
 }
 
-// S[c] += u_c w2r + p_c ur over the block's 32 columns (pivot as in reg_symv)
-template <class T, bool PIV>
-__host__ __device__ __forceinline__ void reg_rank2(T (&S)[32], const T *Vc, const T *pc, const T ur, const T w2r,
-                                                   const int cp, const T ul)
+// S[c] += u_c w2r + p_c ur over the block's 32 columns
+template <class T>
+__host__ __device__ __forceinline__ void reg_rank2(T (&S)[32], const T *Vc, const T *pc, const T ur, const T w2r)
 {
 #pragma unroll
   for (int c = 0; c < 32; c += 2) {
     T u0, u1, p0, p1;
     ld2(Vc + c, u0, u1);
     ld2(pc + c, p0, p1);
-    if (PIV) {
-      u0 = (c + 0 == cp) ? ul : u0;
-      u1 = (c + 1 == cp) ? ul : u1;
-    }
     S[c] = fma(p0, ur, fma(u0, w2r, S[c]));
     S[c + 1] = fma(p1, ur, fma(u1, w2r, S[c + 1]));
   }
@@ -155,22 +150,59 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   }
   tm.sync();  // the staging area becomes the reflector store
 
-  // ---- reduction, i = n-1 .. 1 ----
-  // The pivot u_{i-1} = ul of step i is kept aside (gram[i], free until
-  // the formation of M) and copied into the reflector after the loop, so
-  // the reflector slot never changes while other warps read it; during
-  // step i the warps of its column block substitute it in registers.
-  for (int i = n - 1; i >= 1; --i) {
-    T *Vi = V + (size_t)i * NR;
+  // ---- reduction, i = n-1 .. 1, two barriers per step ----
+  // Step i applies H_i: u = rows < i of column i with the pivot u_{i-1}
+  // replaced by ul, p = beta A u, alpha = beta/2 u.p, and
+  // A += u w^T + w u^T with w = p + alpha u, i.e.
+  //   a_rk += u_k (p_r + 2 alpha u_r) + p_k u_r = u_k w2_r + p_k u_r.
+  // Schedule of step i:
+  //   top      the warps of column i bring that column up to date (the
+  //            rank-2 update of step i+1 restricted to it: its row i is
+  //            then final, the diagonal d_i) and publish its rows < i with
+  //            their partial sums of u.u;
+  //   barrier  1
+  //   middle   every warp applies step i+1's rank-2 update to its block
+  //            (column i gets a wrong but finite value there: the
+  //            reflector slot holds the raw pivot; nothing reads column i
+  //            or row i of the registers after step i, since every later
+  //            u and p is zero there), forms ul and beta, and its partials
+  //            of A u and of u.(A u);
+  //   barrier  2
+  //   tail     p_r and alpha in every thread; p published for the next
+  //            middle.
+  // The pivot ul of step i is kept aside (gram[i], free until the
+  // formation of M) and copied into the reflector after the loop, so the
+  // reflector slot never changes while other warps read it; the warps of
+  // its column block substitute it in registers.
+  T *sg = red, *al = red + 32;  // posted partial sums: u.u and u.(A u)
+  T ur = T(0), w2r = T(0);  // step i+1's u_r and w2_r (its pivot and beta are in gram, beta_s)
+  for (int i = n - 1;; --i) {
     const int cbi = i >> 5;
-    T u0 = T(0);
-    if (cb == cbi) {  // the warps holding column i publish it
-      const T col = get32(S, i & 31);
-      u0 = (r < i) ? col : T(0);
-      Vi[r] = u0;
-      if (r == i - 1) red[64] = u0;
+    if (cb == cbi) {
+      T pi = T(0), ulp = T(0);  // p_i and the pivot of step i+1
+      if (i < n - 1) {
+        const int nactp = (i + 32) >> 5;
+#pragma unroll
+        for (int q = 0; q < NB; q++)
+          if (q < nactp) pi += part[q * NR + i];
+        pi *= beta_s[i + 1];
+        ulp = gram[i + 1];
+      }
+      const T col = get32(S, i & 31) + fma(ulp, w2r, pi * ur);
+      if (r == i) d_out[i] = col;
+      if (i >= 1) {
+        const T u0 = (r < i) ? col : T(0);
+        V[(size_t)i * NR + r] = u0;
+        if (r == i - 1) red[64] = u0;
+        tm.post(u0 * u0, sg, 0);
+      }
     }
-    const T sig = tm.sum(u0 * u0, red);
+    if (i == 0) break;
+    tm.sync();
+    T *Vi = V + (size_t)i * NR;
+    const bool act = (c0 < i) && (32 * rb < i);
+    if (act && i < n - 1) reg_rank2<T>(S, Vi + NR + c0, pv + c0, ur, w2r);  // step i+1's update
+    const T sig = tm.total(sg, 0, cbi * NB, NB);
     const T ulast = red[64];
     const T anorm = -copysign_t(sqr_t(sig), ulast);
     const T ul = ulast - anorm;
@@ -180,13 +212,17 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
       e_out[i - 1] = anorm;
       beta_s[i] = beta;
     }
-    const bool act = (c0 < i) && (32 * rb < i);
     const int cp = (i - 1) - c0;  // pivot column within this block, if 0 <= cp < 32
     const bool piv = (cb == ((i - 1) >> 5));
-    if (act) {  // partial p_r over this block's columns; u_{i-1} is ul
-      const T a = piv ? reg_symv<T, true>(S, Vi + c0, cp, ul) : reg_symv<T, false>(S, Vi + c0, cp, ul);
-      part[cb * NR + r] = (r < i) ? a : T(0);
+    ur = (r == i - 1) ? ul : Vi[r];  // u_r with the pivot, 0 for r >= i
+    T x = T(0);
+    if (act) {  // partial (A u)_r over this block's columns
+      T a = piv ? reg_symv<T, true>(S, Vi + c0, cp, ul) : reg_symv<T, false>(S, Vi + c0, cp, ul);
+      a = (r < i) ? a : T(0);
+      part[cb * NR + r] = a;
+      x = ur * a;
     }
+    tm.post(x, al, 1);
     tm.sync();
     const int nact = (i + 31) >> 5;
     T pr = T(0);
@@ -196,21 +232,12 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
         if (q < nact) pr += part[q * NR + r];
       pr *= beta;
     }
-    if (cb == 0) pv[r] = pr;                    // 0 for r >= i
-    const T ur = (r == i - 1) ? ul : Vi[r];     // u_r with the pivot, 0 for r >= i
-    const T alpha = tm.sum(cb == 0 ? pr * ur : T(0), red) * (beta * T(0.5));
-    if (act) {
-      // A += u w^T + w u^T with w = p + alpha u, i.e.
-      // a_rk += u_k (p_r + 2 alpha u_r) + p_k u_r
-      const T w2r = fma(alpha + alpha, ur, pr);
-      if (piv) reg_rank2<T, true>(S, Vi + c0, pv + c0, ur, w2r, cp, ul);
-      else reg_rank2<T, false>(S, Vi + c0, pv + c0, ur, w2r, cp, ul);
-    }
-    // the barrier in the next step's first sum() orders pv/part reuse
+    if (cb == 0) pv[r] = pr;  // 0 for r >= i
+    const T alpha = tm.total(al, 1, 0, NB * NB) * (beta * beta * T(0.5));
+    w2r = fma(alpha + alpha, ur, pr);
   }
   tm.sync();
   for (int k = 1 + t; k < n; k += tm.size()) V[(size_t)k * NR + k - 1] = gram[k];
-  if (r < n && cb == rb) d_out[r] = get32(S, r - c0);
   if (t == 0) e_out[n - 1] = T(0);
   tm.sync();
 

@@ -13,7 +13,8 @@
 template <class T> struct HostShared {
   std::barrier<> bar;
   std::vector<T> slots;  // 2 x nthr, alternating halves
-  explicit HostShared(int nthr) : bar(nthr), slots(2 * (size_t)nthr) {}
+  std::vector<T> posted; // 2 x nthr: the buffers of post()/total()
+  explicit HostShared(int nthr) : bar(nthr), slots(2 * (size_t)nthr), posted(2 * (size_t)nthr) {}
 };
 
 template <class T> struct HostTeam {
@@ -29,6 +30,15 @@ template <class T> struct HostTeam {
     sh->bar.arrive_and_wait();
     T s = T(0);
     for (int k = 0; k < nthr; k++) s += buf[k];  // same order in every thread
+    return s;
+  }
+  // one slot per thread; total() adds the threads of warps w0 .. w0+nw-1
+  void post(T x, T *, int id) { sh->posted[(size_t)id * nthr + rank] = x; }
+  T total(const T *, int id, int w0, int nw) const
+  {
+    const T *buf = sh->posted.data() + (size_t)id * nthr;
+    T s = T(0);
+    for (int k = 32 * w0; k < 32 * (w0 + nw) && k < nthr; k++) s += buf[k];
     return s;
   }
 };
