@@ -62,54 +62,74 @@ def peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples nvidia-smi clocks and throttle reasons around the timed
+    region.  Started before the warm-up (nvidia-smi takes a moment to print
+    its first sample), every sample is timestamped, and summary() keeps the
+    samples inside the timed window; a window shorter than the sampling
+    period keeps the nearest samples instead, taken under the same load."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 100
 
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time, csv line)
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.perf_counter() + 5.0
+            while not self.lines and time.perf_counter() < t_end and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
-    def __exit__(self, *exc):
+    def stop(self):
         if self.proc is not None:
+            time.sleep(2.0 * self.PERIOD_MS / 1000.0)  # the samples just after the window
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-        return False
+            self.proc = None
 
-    def summary(self):
+    @staticmethod
+    def _parse(ln):
+        f = [x.strip() for x in ln.split(",")]
+        if len(f) < 9:
+            return None
+        try:
+            return float(f[1]), float(f[2]), f[5:9]
+        except ValueError:
+            return None
+
+    def summary(self, w0=None, w1=None):
+        rows = [(t, r) for t, r in ((t, self._parse(ln)) for t, ln in self.lines) if r is not None]
+        if w0 is not None and w1 is not None and rows:
+            inside = [(t, r) for t, r in rows if w0 <= t <= w1]
+            if not inside:  # window shorter than the period: the nearest samples
+                mid = 0.5 * (w0 + w1)
+                inside = sorted(rows, key=lambda x: abs(x[0] - mid))[:2]
+            rows = inside
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
+        for _, (c, m, flags) in rows:
+            sm.append(c)
+            mx.append(m)
+            for nm, v in zip(names, flags):
                 if v.lower() == "active":
                     reasons.add(nm)
         if not sm:
@@ -420,24 +440,29 @@ def main():
         if st != 0:
             raise RuntimeError(f"solve failed: cudaError {st}")
 
-    for i in range(args.warmup):
-        solve(copies[i])
-    barrier()
-    # correctness of the timed configuration: the reference's gate on copy 0
-    e1, e2, fl = E.check(base, w, copies[args.warmup - 1] if args.warmup else copies[0], n)
-    torch.cuda.synchronize()
-    gate_fail = int((fl != 0).sum().item())
-    info_fail = int((info != 0).sum().item())
-
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    clk = ClockSampler(local).start()
+    try:
+        for i in range(args.warmup):
+            solve(copies[i])
         barrier()
+        # correctness of the timed configuration: the reference's gate on copy 0
+        e1, e2, fl = E.check(base, w, copies[args.warmup - 1] if args.warmup else copies[0], n)
+        torch.cuda.synchronize()
+        gate_fail = int((fl != 0).sum().item())
+        info_fail = int((info != 0).sum().item())
+
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        w0 = time.perf_counter()
         t0.record(stream)
         for i in range(args.steps):
             solve(copies[args.warmup + i])
         t1.record(stream)
         barrier()
+        w1 = time.perf_counter()
+    finally:
+        clk.stop()
     ms = t0.elapsed_time(t1)
     if world > 1:
         tt = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -485,7 +510,7 @@ def main():
                      if traffic else None,
                      "alg_bytes_per_matrix": pb[dom]},
         "hbm_fraction_whole_solve": alg_bytes(n, esize) * value / world / 1e9 / hbm,
-        "clocks": clk.summary(),
+        "clocks": clk.summary(w0, w1),
     }
 
     if not args.no_e2e:

@@ -14,6 +14,8 @@
 //   k3_cta<SM>     phase 3 for n > 32: rows of Z in shared memory (a
 //                  matrix's rows split over CTAs when needed) or, for the
 //                  largest FP64 sizes, Z in the workspace
+//   k3_tmem        phase 3 for n > 32 with rows of up to 512 32-bit
+//                  columns: rows of Z in tensor memory
 //   k_jacobi_warp  cyclic Jacobi for n <= 32 (jac_tiled.hpp:3-152)
 //   k_check        FP64 residual / orthogonality gate (eigen_GPU_check.cu),
 //                  one warp per matrix; k_check_cta the tiled form for n > 32
@@ -23,6 +25,7 @@
 #include "eigb_common.cuh"
 #include "eigb_ql.cuh"
 #include "eigb_symfunc.cuh"
+#include "eigb_tmem.cuh"
 #include "eigb_tridiag.cuh"
 #include "eigb_tridiag_reg.cuh"
 
@@ -688,8 +691,8 @@ __global__ void __launch_bounds__(SM ? 256 : 512, 1) k3_cta(const KP<T> p)
   const int r0 = SM ? (int)(blockIdx.x % zsplit) * p.zrows : 0;
   const int nrow = SM ? min(p.zrows, n - r0) : n;
   const int ch = k3c_chunk(n);
-  Rec<T> *rbuf = reinterpret_cast<Rec<T> *>(smem_raw);
-  T *sd = reinterpret_cast<T *>(rbuf + ch);
+  Rec<T> *rbuf = reinterpret_cast<Rec<T> *>(smem_raw);  // two buffers of ch records
+  T *sd = reinterpret_cast<T *>(rbuf + 2 * ch);
   T *se = sd + n;
   T *sdd = se + n;
   T *red = sdd + n;
@@ -812,6 +815,184 @@ __global__ void __launch_bounds__(SM ? 256 : 512, 1) k3_cta(const KP<T> p)
   if (r0 == 0) {
     for (int c = t; c < n; c += nt) val_ptr(p, k)[inv[c]] = sd[c];
     if (t == 0) put_info(p, k, ierr);
+  }
+}
+
+// ---------------------------------------------------------------- phase 3, Z in tensor memory
+// One part of k3_tmem: rows r0 .. r0+zrows-1 of one matrix, applied by the
+// pn threads pt = 0 .. pn-1 of the part (row r0+pt in tensor memory at z0),
+// with the shared-memory scratch of k3_cta (records double buffer, d, e,
+// sort permutation; no Z) at ps and named barrier id bar.  Same steps and
+// the same arithmetic as k3_cta.
+template <class T>
+__device__ __forceinline__ void k3_tmem_part(const KP<T> &p, const long part, const int pt, const int pn,
+                                             const int bar, unsigned char *ps, const uint32_t z0)
+{
+  const long k = part / p.zsplit;
+  const int n = p.n, nm = p.nm;
+  const int r0 = (int)(part % p.zsplit) * p.zrows;
+  const int nrow = min(p.zrows, n - r0);
+  const int ch = k3c_chunk(n);
+  Rec<T> *rbuf = reinterpret_cast<Rec<T> *>(ps);  // two buffers of ch records
+  T *sd = reinterpret_cast<T *>(rbuf + 2 * ch);
+  T *se = sd + n;
+  T *sdd = se + n;
+  T *red = sdd + n;
+  int *inv = reinterpret_cast<int *>(red + 64);
+  int *pos = inv + n;
+  int *sflag = pos + n;  // [0] nrec, [1] done, [2] ierr
+  T *A = mat_ptr(p, k);
+  const Meta mt = p.meta[k];
+  const Rec<T> *src = p.rec + (size_t)k * p.rcap;
+  if (!mt.overflow) {  // first chunk of records, copied while Z is loaded
+    const int cnt = min(ch, mt.nrec);
+    for (int q = pt; q < cnt; q += pn) cp_async<sizeof(Rec<T>)>(rbuf + q, src + q);
+    cp_async_commit();
+  }
+  // row r0+pt of Q into tensor memory (zeros in lanes past the last row)
+  const bool mine = pt < nrow;
+  {
+    const T *Ar = A + r0 + pt;
+    int c = 0;
+    for (; c + 8 <= n; c += 8) {
+      T v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = mine ? Ar[(size_t)(c + u) * nm] : T(0);
+#pragma unroll
+      for (int u = 0; u < 8; u++) tmem_st1(tmem_at<T>(z0, c + u), v[u]);
+    }
+    for (; c < n; c++) tmem_st1(tmem_at<T>(z0, c), mine ? Ar[(size_t)c * nm] : T(0));
+  }
+  cp_async_wait_all();
+  part_sync(bar, pn);
+
+  if (!mt.overflow) {
+    // double buffer: the next chunk is copied in while this one is applied
+    int base = 0, cur = 0;
+    while (base < mt.nrec) {
+      Rec<T> *rb = rbuf + cur * ch;
+      const int cnt = min(ch, mt.nrec - base);
+      const int used = seg_walk(rb, cnt);
+      const int nb = base + (used > 0 ? used : cnt);  // a segment is at most n records: used > 0
+      if (nb < mt.nrec) {
+        Rec<T> *nx = rbuf + (cur ^ 1) * ch;
+        const int ncnt = min(ch, mt.nrec - nb);
+        for (int q = pt; q < ncnt; q += pn) cp_async<sizeof(Rec<T>)>(nx + q, src + nb + q);
+        cp_async_commit();
+      }
+      apply_segments_tm<T>(rb, used, z0);
+      cp_async_wait_all();
+      part_sync(bar, pn);
+      base = nb;
+      cur ^= 1;
+    }
+    for (int c = pt; c < n; c += pn) sd[c] = p.e[k * n + c];
+    if (pt == 0) sflag[2] = mt.ierr;
+  } else {
+    // capacity exceeded in phase 2: regenerate in chunks (segments are
+    // closed at every chunk end, so each chunk is self-contained)
+    for (int c = pt; c < n; c += pn) {
+      sd[c] = p.d[k * n + c];
+      se[c] = p.e[k * n + c];
+    }
+    part_sync(bar, pn);
+    QLGen<T> g;
+    g.pc = PC_START;
+    while (true) {
+      if (pt == 0) {
+        sflag[0] = ql_run(p.method, g, DEView<T>{sd, se, 1}, n, rbuf, ch, p.max_sweep);
+        sflag[1] = (g.pc == PC_DONE);
+        sflag[2] = g.ierr;
+      }
+      part_sync(bar, pn);
+      const int nr = sflag[0];
+      const int done = sflag[1];
+      apply_segments_tm<T>(rbuf, nr, z0);
+      part_sync(bar, pn);
+      if (done) break;
+    }
+  }
+  part_sync(bar, pn);
+  const int ierr = sflag[2];
+  // sort permutation (inverse: destination column of each source column)
+  bool bad = false;
+  for (int c = pt; c < n; c += pn) {
+    inv[c] = c;
+    if (p.sort && ierr == 0) {
+      const T dc = sd[c];
+      int cnt = 0;
+      bad |= (dc != dc);
+      for (int q = 0; q < n; q++) {
+        const T dq = sd[q];
+        cnt += (dq < dc) ? 1 : 0;
+        bad |= (q != c) && (dq == dc);
+      }
+      inv[c] = cnt;
+    }
+  }
+  if (part_sync_or(bar, pn, bad)) {
+    if (pt == 0) {
+      for (int c = 0; c < n; c++) sdd[c] = sd[c];
+      select_sort_serial(n, sdd, pos);
+      for (int j = 0; j < n; j++) inv[pos[j]] = j;
+    }
+    part_sync(bar, pn);
+  }
+  tmem_wait_st();  // the last segment's stores
+  {
+    T *Ar = A + r0 + pt;
+    int c = 0;
+    for (; c + 8 <= n; c += 8) {
+      T v[8];
+      tmem_ld8(tmem_at<T>(z0, c + 7), v);  // v[u] = column c+7-u
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+        if (mine) Ar[(size_t)inv[c + 7 - u] * nm] = v[u];
+    }
+    for (; c < n; c++) {
+      const T v = tmem_ld1((const T *)nullptr, tmem_at<T>(z0, c));
+      if (mine) Ar[(size_t)inv[c] * nm] = v;
+    }
+  }
+  if (r0 == 0) {
+    for (int c = pt; c < n; c += pn) val_ptr(p, k)[inv[c]] = sd[c];
+    if (pt == 0) put_info(p, k, ierr);
+  }
+}
+
+// Phase 3 with Z in tensor memory (eigb_tmem.cuh), for rows of at most
+// 512 32-bit columns.  A CTA of at most four warps applies blockDim.x /
+// (32 wpp) parts, wpp warps each (two parts of two warps where a part has
+// at most 64 rows, so that all four lane quarters of its columns are in
+// use).  Warp w keeps its 32 rows in the lanes of its sub-partition,
+// 32*(w % 4) .., in the acols columns the CTA allocates.  The host sizes
+// the CTA's shared memory in proportion to acols, so the CTAs that share an
+// SM never hold more than its 512 columns together.
+template <class T>
+__global__ void __launch_bounds__(128, 1) k3_tmem(const KP<T> p, const int wpp, const int acols)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t tbase;
+  const int t = threadIdx.x, w = t >> 5;
+  const int pn = 32 * wpp;  // threads of a part
+  const int parts = blockDim.x / pn;
+  const int g = t / pn;
+  const long part = (long)blockIdx.x * parts + g;
+  if (w == 0) tmem_alloc(&tbase, acols);
+  tmem_fence_before();
+  __syncthreads();
+  tmem_fence_after();
+  const uint32_t z0 = tbase + ((uint32_t)(32 * (w & 3)) << 16);
+  if (part < p.Lc * (long)p.zsplit)  // uniform per part
+    k3_tmem_part<T>(p, part, t - g * pn, pn, parts == 1 ? 0 : 1 + g, smem_raw + (size_t)g * k3c_fixed_bytes<T>(p.n),
+                    z0);
+  // every tensor memory access of the CTA is complete (loads wait in
+  // place, stores before the read-out); the allocating warp frees
+  tmem_fence_before();
+  __syncthreads();
+  if (w == 0) {
+    tmem_fence_after();
+    tmem_dealloc(tbase, acols);
   }
 }
 

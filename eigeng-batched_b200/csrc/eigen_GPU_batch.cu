@@ -33,6 +33,8 @@ constexpr long kMinChunk = 512;
 struct DevProps {
   int sms = 0;
   int smem_optin = 0;
+  int smem_sm = 0;   // shared memory per SM
+  int smem_rsv = 0;  // shared memory the system reserves per block
   int l2 = 0;
   bool ok = false;
 };
@@ -52,6 +54,10 @@ cudaError_t dev_props(DevProps &out)
   if (!p.ok) {
     if ((err = cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return err;
     if ((err = cudaDeviceGetAttribute(&p.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
+      return err;
+    if ((err = cudaDeviceGetAttribute(&p.smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+      return err;
+    if ((err = cudaDeviceGetAttribute(&p.smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess)
       return err;
     if ((err = cudaDeviceGetAttribute(&p.l2, cudaDevAttrL2CacheSize, dev)) != cudaSuccess) return err;
     p.ok = true;
@@ -115,6 +121,7 @@ template <class T> struct Plan {
   int k1b = 0;        // phase 1 (CTA form): leading block held in shared memory
   int zrows = 0;      // phase 3: rows of Z per CTA in shared memory (0: Z in the workspace)
   int zsplit = 1;     // phase 3: CTAs per matrix
+  int ztm = 0;        // phase 3: rows of Z in tensor memory instead of shared memory
   size_t off_d = 0, off_e = 0, off_meta = 0, off_rec = 0, off_z = 0, bytes = 0;
 };
 
@@ -153,6 +160,21 @@ cudaError_t make_plan(long L, int nm, int n, const DevProps &dp, Plan<T> &pl, co
       pl.zrows = (n + split - 1) / split;
     } else if (fixed > optin) {
       return cudaErrorInvalidValue;
+    }
+    // tensor memory holds up to 128 rows of a matrix per part (rows of up
+    // to 512 32-bit columns: FP64 n <= 256, FP32 n <= 512), unless that
+    // takes more parts per matrix than shared memory does: every part reads
+    // all of the matrix's records (measured on B200: FP64 n = 160, two parts
+    // of 80 rows, is slower than one shared-memory CTA of 160 rows)
+    if (pl.zrows > 0 && tmem_cols<T>(n) > 0 && !(opts && opts->zmem == EIGEN_GPU_ZMEM_SHARED)) {
+      int split = (n + 127) / 128;
+      const int want = opts ? opts->split : 0;
+      if (want > split) split = std::min(want, (n + 31) / 32);
+      if (split <= pl.zsplit) {
+        pl.zsplit = split;
+        pl.zrows = (n + split - 1) / split;
+        pl.ztm = 1;
+      }
     }
   }
   const bool zglob = n > 32 && pl.zrows == 0;
@@ -322,8 +344,8 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const size_t k1w_smem = sizeof(T) * k1w_slot<T>() * K1W_NW;
   const size_t k3w_smem = sizeof(K3WSlot<T>) * K3W_NW;
   // phase 3: one row per thread up to 512 rows, two above
-  const bool zsm = pl.zrows > 0;
-  const int k3_nt = zsm ? ((pl.zrows + 31) / 32) * 32
+  bool ztm = pl.ztm != 0 && n > 32;
+  int k3_nt = pl.zrows > 0 ? ((pl.zrows + 31) / 32) * 32
                         : (n > 512 ? (((n + 1) / 2 + 31) / 32) * 32 : ((n + 31) / 32) * 32);
   p.zrows = pl.zrows;
   p.zsplit = pl.zsplit;
@@ -331,7 +353,48 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const int k1c_nt = k1c_threads(n);
   const bool k1_in_regs = reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin;
   const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems(n, k1c_nt, pl.k1b);
-  const size_t k3c_smem = k3c_smem_bytes<T>(n, pl.zrows);
+  size_t k3c_smem = k3c_smem_bytes<T>(n, ztm ? 0 : pl.zrows);
+  int k3_wpp = 0, k3_parts = 0, k3_acols = 0;  // tensor-memory form: warps per part, parts per CTA, columns
+  if (ztm) {
+    // Tensor memory is allocated per CTA, and the CTAs on one SM must never
+    // ask for more than its 512 columns together (an allocation would wait
+    // for another CTA's columns).  Each CTA therefore requests shared memory
+    // in proportion to its columns, acols/512 of the SM's (reserve
+    // included): whatever mix of these CTAs, from any launch or stream,
+    // shares an SM holds at most 512 columns.  A CTA is at most four warps
+    // (one per lane quarter): two parts of two warps where a part has at
+    // most 64 rows, unless the chunk is too small to fill the SMs.
+    k3_acols = tmem_cols<T>(n);
+    k3_wpp = (pl.zrows + 31) / 32;
+    const long spread = (std::min(L, pl.Lc) * pl.zsplit + dp.sms - 1) / dp.sms;
+    k3_parts = (int)std::max(1L, std::min<long>(4 / k3_wpp, spread));
+    // (the kernel's own static shared memory, 16 bytes, is within the 64
+    // left out; that slack cannot add up to another CTA's share)
+    const size_t fixed = k3c_fixed_bytes<T>(n) * (size_t)k3_parts;
+    const size_t foot = (size_t)dp.smem_sm * (size_t)k3_acols / 512;
+    const size_t other = (size_t)dp.smem_rsv + 64;
+    k3c_smem = std::max(fixed, foot > other ? foot - other : 0);
+    int nb = 0;
+    bool ok = k3c_smem + 64 <= (size_t)dp.smem_optin;
+    if (ok) {
+      if ((err = set_smem(k3_tmem<T>, k3c_smem)) != cudaSuccess) return err;
+      if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k3_tmem<T>, 32 * k3_wpp * k3_parts,
+                                                               k3c_smem)) != cudaSuccess)
+        return err;
+      ok = nb >= 1 && nb * k3_acols <= 512;
+    }
+    if (!ok) {  // the shared-memory plan, which uses the same workspace layout
+      eigen_GPU_batch_opts o = opts ? *opts : eigen_GPU_batch_opts{};
+      o.zmem = EIGEN_GPU_ZMEM_SHARED;
+      if ((err = make_plan<T>(L, nm, n, dp, pl, &o)) != cudaSuccess) return err;
+      ztm = false;
+      p.zrows = pl.zrows;
+      p.zsplit = pl.zsplit;
+      k3_nt = ((pl.zrows + 31) / 32) * 32;
+      k3c_smem = k3c_smem_bytes<T>(n, pl.zrows);
+    }
+  }
+  const bool zsm = pl.zrows > 0 && !ztm;
   // phase 2: matrices per warp, then warps per block within the shared
   // memory budget (2n values per matrix)
   p.k2mpw = k2_mpw(std::min(L, pl.Lc), dp.sms);
@@ -358,7 +421,9 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     } else if ((err = set_k1_smem<T>(n, k1c_smem)) != cudaSuccess) {
       return err;
     }
-    if (zsm) {
+    if (ztm) {
+      // attribute set with the launch geometry above
+    } else if (zsm) {
       if ((err = set_smem(k3_cta<T, true, 1>, k3c_smem)) != cudaSuccess) return err;
     } else if ((err = set_smem(n > 512 ? k3_cta<T, false, 2> : k3_cta<T, false, 1>, k3c_smem)) != cudaSuccess) {
       return err;
@@ -382,6 +447,10 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   auto phase3 = [&](const KP<T> &q, long cnt, cudaStream_t st) {
     if (n <= 32) {
       k3_warp<T><<<(unsigned)((cnt + K3W_NW - 1) / K3W_NW), 32 * K3W_NW, k3w_smem, st>>>(q);
+    } else if (ztm) {
+      const long nparts = cnt * pl.zsplit;
+      k3_tmem<T><<<(unsigned)((nparts + k3_parts - 1) / k3_parts), 32 * k3_wpp * k3_parts, k3c_smem, st>>>(
+          q, k3_wpp, k3_acols);
     } else if (zsm) {
       k3_cta<T, true, 1><<<(unsigned)(cnt * pl.zsplit), k3_nt, k3c_smem, st>>>(q);
     } else if (n > 512) {

@@ -21,6 +21,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libeigenGbatch.so")
 
 TQL2, IMTQL2, JACOBI = 0, 1, 2
+ZMEM_AUTO, ZMEM_SHARED = 0, 1  # where the apply phase keeps Z (eigen_GPU_batch_opts.zmem)
 
 _lib = None
 
@@ -33,7 +34,7 @@ class Opts(ctypes.Structure):
     """eigen_GPU_batch_opts of include/eigen_GPU_batch.h."""
     _fields_ = [("method", ctypes.c_int), ("sort", ctypes.c_int), ("max_sweep", ctypes.c_int),
                 ("rec_cap", ctypes.c_int), ("chunk", ctypes.c_int), ("split", ctypes.c_int),
-                ("reserved", ctypes.c_int * 2)]
+                ("zmem", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 def lib():
@@ -211,11 +212,11 @@ def eigen_GPU_batch(a, w, wk, n, nm=None, m=None, stream=None):
 
 
 def eigen_GPU_batch_ex(a, w, wk, n, nm=None, m=None, info=None, method=TQL2, sort=True, max_sweep=100,
-                       stream=None, rec_cap=0, chunk=0, split=0):
+                       stream=None, rec_cap=0, chunk=0, split=0, zmem=ZMEM_AUTO):
     """Extended call; returns the cudaError_t status (0 on success)."""
     L, nm = _dims(a, n, nm)
     m = n if m is None else m
-    o = Opts(method, 1 if sort else 0, max_sweep, rec_cap, chunk, split)
+    o = Opts(method, 1 if sort else 0, max_sweep, rec_cap, chunk, split, zmem)
     lw = 0 if wk is None else wk.numel() * wk.element_size()
     return getattr(lib(), "eigen_GPU_batch_ex_" + _sfx(a.dtype))(
         L, nm, n, m, _ptr(a), _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), _stream(stream))
@@ -232,14 +233,15 @@ def eigen_GPU_batch_noalloc(a, w, n, nm=None, m=None, info=None, stream=None):
 
 
 def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=None, rec_cap=0, chunk=0,
-          split=0):
+          split=0, zmem=ZMEM_AUTO):
     """Convenience wrapper: solves in place, returns (w, info)."""
     L, nm = _dims(a, n, nm)
     w = torch.empty((L, n), dtype=a.dtype, device=a.device)
     info = torch.zeros(L, dtype=torch.int32, device=a.device)
     if wk is None and method != JACOBI:
         wk = workspace(L, nm, n, a.dtype, a.device, rec_cap, chunk)
-    st = eigen_GPU_batch_ex(a, w, wk, n, nm, n, info, method, sort, max_sweep, stream, rec_cap, chunk, split)
+    st = eigen_GPU_batch_ex(a, w, wk, n, nm, n, info, method, sort, max_sweep, stream, rec_cap, chunk, split,
+                            zmem)
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
     return w, info

@@ -55,6 +55,12 @@ cudaError_t eigen_GPU_batch_BufferSize_FP(const int L, const int nm, const int n
 #define EIGEN_GPU_BATCH_IMTQL2 1
 #define EIGEN_GPU_BATCH_JACOBI 2
 
+/* eigen_GPU_batch_opts.zmem: where the apply phase keeps the rows it rotates */
+#define EIGEN_GPU_ZMEM_AUTO 0   /* tensor memory where a row fits (FP64 n <= 256,
+                                   FP32 n <= 512), else shared memory, else the
+                                   workspace */
+#define EIGEN_GPU_ZMEM_SHARED 1 /* never tensor memory (same results, bit for bit) */
+
 typedef struct eigen_GPU_batch_opts {
   int method;    /* EIGEN_GPU_BATCH_TQL2 (default), _IMTQL2 or _JACOBI */
   int sort;      /* 1: ascending eigenvalues (reference DO_SORT 1), 0: as computed */
@@ -70,7 +76,8 @@ typedef struct eigen_GPU_batch_opts {
                     apply phase; <= 0: automatic (the fewest whose rows fit
                     in shared memory).  Larger values trade re-reads of the
                     rotation records for more warps per SM. */
-  int reserved[2];
+  int zmem;      /* EIGEN_GPU_ZMEM_AUTO (0) or EIGEN_GPU_ZMEM_SHARED */
+  int reserved;
 } eigen_GPU_batch_opts;
 
 /* Workspace bytes for eigen_GPU_batch_ex_* with these options (NULL:

@@ -23,10 +23,10 @@ def E():
     return eigeng_b200
 
 
-def gpu_solve(a0, n, nm=None, method=0, sort=True, max_sweep=100, rec_cap=0, chunk=0, split=0):
+def gpu_solve(a0, n, nm=None, method=0, sort=True, max_sweep=100, rec_cap=0, chunk=0, split=0, zmem=0):
     a = torch.from_numpy(np.ascontiguousarray(a0)).cuda()
     w, info = E().solve(a, n, nm, method=method, sort=sort, max_sweep=max_sweep, rec_cap=rec_cap, chunk=chunk,
-                        split=split)
+                        split=split, zmem=zmem)
     torch.cuda.synchronize()
     return w.cpu().numpy(), a.cpu().numpy(), info.cpu().numpy()
 
@@ -338,6 +338,30 @@ def test_apply_row_split_is_bit_identical(oracle_mod, n, nm):
         assert np.array_equal(w1, w2) and np.array_equal(z1, z2) and np.array_equal(i1, i2), split
     w3, z3, i3 = gpu_solve(a0, n, nm, split=3, rec_cap=4 * n)   # records overflow: regenerated per block
     assert np.array_equal(w1, w3) and np.array_equal(z1, z3) and np.array_equal(i1, i3)
+
+
+@pytest.mark.parametrize("n,nm,dtype", [(33, 33, np.float64), (64, 64, np.float64), (100, 103, np.float64),
+                                        (128, 128, np.float64), (129, 130, np.float64), (200, 200, np.float64),
+                                        (256, 256, np.float64), (40, 40, np.float32), (128, 128, np.float32),
+                                        (300, 301, np.float32), (512, 512, np.float32)])
+def test_tensor_memory_apply_is_bit_identical(oracle_mod, n, nm, dtype):
+    """Where a row fits, the apply phase keeps Z in tensor memory (one row
+    per TMEM lane) with the operations of the shared-memory form, in the
+    same order: results agree bit for bit with the shared-memory form, with
+    a row split and with the in-kernel regeneration path too."""
+    O = oracle_mod
+    a0 = np.zeros((5, n, nm), dtype)
+    a0[:, :, :n] = O.sym_uniform(5, n, seed=n + 11).astype(dtype)
+    shared = E().ZMEM_SHARED
+    w1, z1, i1 = gpu_solve(a0, n, nm, zmem=shared)
+    w2, z2, i2 = gpu_solve(a0, n, nm)
+    assert np.array_equal(w1, w2) and np.array_equal(z1, z2) and np.array_equal(i1, i2)
+    w3, z3, i3 = gpu_solve(a0, n, nm, split=3)
+    assert np.array_equal(w1, w3) and np.array_equal(z1, z3) and np.array_equal(i1, i3)
+    w4, z4, i4 = gpu_solve(a0, n, nm, rec_cap=4 * n)   # records overflow: regenerated in the kernel
+    w5, z5, i5 = gpu_solve(a0, n, nm, rec_cap=4 * n, zmem=shared)
+    assert np.array_equal(w4, w5) and np.array_equal(z4, z5) and np.array_equal(i4, i5)
+    assert np.array_equal(w1, w4) and np.array_equal(z1, z4)
 
 
 def test_chunked_batch_and_determinism(oracle_mod):
