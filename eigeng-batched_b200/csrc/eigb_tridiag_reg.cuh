@@ -17,15 +17,25 @@
 
 namespace eigb {
 
-// v[i] for a warp-uniform (or per-lane) dynamic index, by selects, so that
-// the array stays in registers
+// v[i] (0 <= i < 32) for a warp-uniform (or per-lane) dynamic index, by
+// selects, so that the array stays in registers: four interleaved chains
+// (c = 4j + k picked by i >> 2) and a select by i & 3, nine deep with four
+// values live (one chain would be 31 deep on the critical path of every
+// reduction step; a full tree keeps 16 live and spills)
 template <class T>
 __host__ __device__ __forceinline__ T get32(const T (&v)[32], const int i)
 {
-  T r = v[0];
+  const int j = i >> 2;
+  T a0 = v[0], a1 = v[1], a2 = v[2], a3 = v[3];
 #pragma unroll
-  for (int c = 1; c < 32; c++) r = (i == c) ? v[c] : r;
-  return r;
+  for (int c = 1; c < 8; c++) {
+    a0 = (j == c) ? v[4 * c] : a0;
+    a1 = (j == c) ? v[4 * c + 1] : a1;
+    a2 = (j == c) ? v[4 * c + 2] : a2;
+    a3 = (j == c) ? v[4 * c + 3] : a3;
+  }
+  const T b0 = (i & 1) ? a1 : a0, b1 = (i & 1) ? a3 : a2;
+  return (i & 2) ? b1 : b0;
 }
 
 // Two consecutive values from 2-element-aligned shared memory in one load.
