@@ -22,6 +22,7 @@
 #pragma once
 #include <stdio.h>
 
+#include "eigb_apply.cuh"
 #include "eigb_common.cuh"
 #include "eigb_ql.cuh"
 #include "eigb_symfunc.cuh"
@@ -446,11 +447,14 @@ __global__ void __launch_bounds__(32 * K3W_NW) k3_warp(const KP<T> p)
 // ---------------------------------------------------------------- phase 3, n > 32
 // Records staged per buffer in k3_cta (two buffers, one being filled while
 // the other is applied): room for two whole segments.
-__host__ __device__ inline int k3c_chunk(int n) { return ((2 * (n + 1) + 63) / 64) * 64; }
+// Records per buffer: room for `sweeps` whole sweeps (and their headers),
+// since a sweep is applied only once it is complete in the buffer and a
+// group of sweeps (eigb_apply.cuh) only when all of it is.
+__host__ __device__ inline int k3c_chunk(int n, int sweeps = 2) { return ((sweeps * (n + 1) + 63) / 64) * 64; }
 
-template <class T> __host__ __device__ inline size_t k3c_fixed_bytes(int n)
+template <class T> __host__ __device__ inline size_t k3c_fixed_bytes(int n, int sweeps = 2)
 {
-  size_t b = sizeof(Rec<T>) * 2 * (size_t)k3c_chunk(n) + sizeof(T) * (3 * (size_t)n + 64) +
+  size_t b = sizeof(Rec<T>) * 2 * (size_t)k3c_chunk(n, sweeps) + sizeof(T) * (3 * (size_t)n + 64) +
              sizeof(int) * (2 * (size_t)n + 8);
   return (b + 15) & ~(size_t)15;
 }
@@ -557,6 +561,7 @@ template <class T> __host__ __device__ __forceinline__ int seg_walk(const Rec<T>
   }
   return q;
 }
+
 
 #define EIGB_PAIR_STEP(X, RA, RB, OUT)               \
   {                                                  \
@@ -819,12 +824,16 @@ __global__ void __launch_bounds__(SM ? 256 : 512, 1) k3_cta(const KP<T> p)
 }
 
 // ---------------------------------------------------------------- phase 3, Z in tensor memory
+// Sweeps per record buffer of k3_tmem: a full group and the next sweep
+// (shared memory is not what limits that kernel).
+constexpr int K3_TM_SWEEPS = K3_GROUP + 1;
+
 // One part of k3_tmem: rows r0 .. r0+zrows-1 of one matrix, applied by the
 // pn threads pt = 0 .. pn-1 of the part (row r0+pt in tensor memory at z0),
 // with the shared-memory scratch of k3_cta (records double buffer, d, e,
 // sort permutation; no Z) at ps and named barrier id bar.  Same steps and
 // the same arithmetic as k3_cta.
-template <class T>
+template <class T, int KG>
 __device__ __forceinline__ void k3_tmem_part(const KP<T> &p, const long part, const int pt, const int pn,
                                              const int bar, unsigned char *ps, const uint32_t z0)
 {
@@ -832,7 +841,7 @@ __device__ __forceinline__ void k3_tmem_part(const KP<T> &p, const long part, co
   const int n = p.n, nm = p.nm;
   const int r0 = (int)(part % p.zsplit) * p.zrows;
   const int nrow = min(p.zrows, n - r0);
-  const int ch = k3c_chunk(n);
+  const int ch = k3c_chunk(n, K3_TM_SWEEPS);
   Rec<T> *rbuf = reinterpret_cast<Rec<T> *>(ps);  // two buffers of ch records
   T *sd = reinterpret_cast<T *>(rbuf + 2 * ch);
   T *se = sd + n;
@@ -880,7 +889,7 @@ __device__ __forceinline__ void k3_tmem_part(const KP<T> &p, const long part, co
         for (int q = pt; q < ncnt; q += pn) cp_async<sizeof(Rec<T>)>(nx + q, src + nb + q);
         cp_async_commit();
       }
-      apply_segments_tm<T>(rb, used, z0);
+      apply_segments_tm<T, KG>(rb, used, z0);
       cp_async_wait_all();
       part_sync(bar, pn);
       base = nb;
@@ -907,7 +916,7 @@ __device__ __forceinline__ void k3_tmem_part(const KP<T> &p, const long part, co
       part_sync(bar, pn);
       const int nr = sflag[0];
       const int done = sflag[1];
-      apply_segments_tm<T>(rbuf, nr, z0);
+      apply_segments_tm<T, KG>(rbuf, nr, z0);
       part_sync(bar, pn);
       if (done) break;
     }
@@ -968,7 +977,7 @@ __device__ __forceinline__ void k3_tmem_part(const KP<T> &p, const long part, co
 // 32*(w % 4) .., in the acols columns the CTA allocates.  The host sizes
 // the CTA's shared memory in proportion to acols, so the CTAs that share an
 // SM never hold more than its 512 columns together.
-template <class T>
+template <class T, int KG>
 __global__ void __launch_bounds__(128, 1) k3_tmem(const KP<T> p, const int wpp, const int acols)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -984,8 +993,8 @@ __global__ void __launch_bounds__(128, 1) k3_tmem(const KP<T> p, const int wpp, 
   tmem_fence_after();
   const uint32_t z0 = tbase + ((uint32_t)(32 * (w & 3)) << 16);
   if (part < p.Lc * (long)p.zsplit)  // uniform per part
-    k3_tmem_part<T>(p, part, t - g * pn, pn, parts == 1 ? 0 : 1 + g, smem_raw + (size_t)g * k3c_fixed_bytes<T>(p.n),
-                    z0);
+    k3_tmem_part<T, KG>(p, part, t - g * pn, pn, parts == 1 ? 0 : 1 + g,
+                    smem_raw + (size_t)g * k3c_fixed_bytes<T>(p.n, K3_TM_SWEEPS), z0);
   // every tensor memory access of the CTA is complete (loads wait in
   // place, stores before the read-out); the allocating warp frees
   tmem_fence_before();

@@ -14,10 +14,15 @@
 // warp's first lane).  Loads are followed by tcgen05.wait::ld inside the
 // same asm statement, so no register is read before its data arrived;
 // tcgen05.wait::st orders a thread's stores before its later loads of the
-// same columns (the start of every segment, and the final read-out).
+// same columns (the start of every segment, and the final read-out).  The
+// loads and stores touch only tensor memory and registers: their asm
+// statements are volatile (kept in program order among themselves) but do
+// not clobber memory, so the compiler may schedule shared-memory loads
+// (the rotation records) across them.
 #pragma once
 #include <stdint.h>
 
+#include "eigb_apply.cuh"
 #include "eigb_common.cuh"
 
 namespace eigb {
@@ -84,8 +89,7 @@ __device__ __forceinline__ double tmem_ld1(const double *, const uint32_t a)
       "tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];\n\t"
       "tcgen05.wait::ld.sync.aligned;\n"
       : "=r"(lo), "=r"(hi)
-      : "r"(a)
-      : "memory");
+      : "r"(a));
 #endif
   return __hiloint2double((int)hi, (int)lo);
 }
@@ -97,8 +101,7 @@ __device__ __forceinline__ float tmem_ld1(const float *, const uint32_t a)
       "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n\t"
       "tcgen05.wait::ld.sync.aligned;\n"
       : "=r"(v)
-      : "r"(a)
-      : "memory");
+      : "r"(a));
 #endif
   return __uint_as_float(v);
 }
@@ -106,13 +109,13 @@ __device__ __forceinline__ void tmem_st1(const uint32_t a, const double v)
 {
   const uint32_t lo = (uint32_t)__double2loint(v), hi = (uint32_t)__double2hiint(v);
 #if EIGB_TCGEN05
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};\n" ::"r"(a), "r"(lo), "r"(hi) : "memory");
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};\n" ::"r"(a), "r"(lo), "r"(hi));
 #endif
 }
 __device__ __forceinline__ void tmem_st1(const uint32_t a, const float v)
 {
 #if EIGB_TCGEN05
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};\n" ::"r"(a), "r"(__float_as_uint(v)) : "memory");
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};\n" ::"r"(a), "r"(__float_as_uint(v)));
 #endif
 }
 
@@ -136,8 +139,7 @@ __device__ __forceinline__ void tmem_ld8(const uint32_t a, double (&v)[8])
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(a), "r"(a - s), "r"(a - 2 * s), "r"(a - 3 * s), "r"(a - 4 * s), "r"(a - 5 * s), "r"(a - 6 * s),
-        "r"(a - 7 * s)
-      : "memory");
+        "r"(a - 7 * s));
 #endif
 #pragma unroll
   for (int u = 0; u < 8; u++) v[u] = __hiloint2double((int)r[2 * u + 1], (int)r[2 * u]);
@@ -159,8 +161,7 @@ __device__ __forceinline__ void tmem_ld8(const uint32_t a, float (&v)[8])
       "tcgen05.wait::ld.sync.aligned;\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
       : "r"(a), "r"(a - s), "r"(a - 2 * s), "r"(a - 3 * s), "r"(a - 4 * s), "r"(a - 5 * s), "r"(a - 6 * s),
-        "r"(a - 7 * s)
-      : "memory");
+        "r"(a - 7 * s));
 #endif
 #pragma unroll
   for (int u = 0; u < 8; u++) v[u] = __uint_as_float(r[u]);
@@ -232,6 +233,15 @@ __device__ __forceinline__ void seg_apply_tm(const uint32_t z0, const Rec<T> *__
   tmem_st1(tmem_at<T>(z0, c + 1), h);
 }
 
+// Row accessor for seg_apply_group: this thread's row in TMEM
+template <class T> struct RowTM {
+  uint32_t z0;
+  __device__ __forceinline__ T ld(const int c) const { return tmem_ld1((const T *)nullptr, tmem_at<T>(z0, c)); }
+  __device__ __forceinline__ void st(const int c, const T v) const { tmem_st1(tmem_at<T>(z0, c), v); }
+  __device__ __forceinline__ void ld8(const int c, T (&v)[8]) const { tmem_ld8(tmem_at<T>(z0, c), v); }
+  __device__ __forceinline__ void begin() const { tmem_wait_st(); }  // earlier stores land before these loads
+};
+
 // seg_apply_pair on a row in TMEM (bit-identical to the shared-memory form)
 template <class T>
 __device__ __forceinline__ void seg_apply_pair_tm(const uint32_t z0, const Rec<T> *__restrict__ ra,
@@ -278,10 +288,27 @@ __device__ __forceinline__ void seg_apply_pair_tm(const uint32_t z0, const Rec<T
   }
 }
 
-// apply_segments for a row in TMEM
-template <class T>
+// A single sweep on a row in TMEM (functor for apply_grouped)
+template <class T> struct SingleTM {
+  uint32_t z0;
+  __device__ __forceinline__ void operator()(const Rec<T> *rp, const int i0, const int len) const
+  {
+    seg_apply_tm<T>(z0, rp, i0, len);
+  }
+};
+
+// apply_segments for a row in TMEM (bit-identical to the shared-memory
+// form).  KG > 1: groups of up to KG consecutive sweeps go through
+// seg_apply_group; KG = 1: two consecutive sweeps over the same rotations
+// go through seg_apply_pair_tm (measured on B200: groups pay off for rows
+// of 128 or more, the pairs below that).
+template <class T, int KG>
 __device__ __forceinline__ void apply_segments_tm(const Rec<T> *rbuf, const int used, const uint32_t z0)
 {
+  if (KG > 1) {
+    apply_grouped<T, KG>(rbuf, used, RowTM<T>{z0}, SingleTM<T>{z0});
+    return;
+  }
   int q = 0;
   while (q < used) {
     const Rec<T> hd = rbuf[q];
@@ -299,4 +326,5 @@ __device__ __forceinline__ void apply_segments_tm(const Rec<T> *rbuf, const int 
     q = q2;
   }
 }
+
 }  // namespace eigb

@@ -355,6 +355,9 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems(n, k1c_nt, pl.k1b);
   size_t k3c_smem = k3c_smem_bytes<T>(n, ztm ? 0 : pl.zrows);
   int k3_wpp = 0, k3_parts = 0, k3_acols = 0;  // tensor-memory form: warps per part, parts per CTA, columns
+  // sweeps per pass: up to four for rows of 128 or more, pairs of equal
+  // sweeps below (measured on B200, eigb_tmem.cuh)
+  void (*k3t)(const KP<T>, const int, const int) = n >= 128 ? k3_tmem<T, 4> : k3_tmem<T, 1>;
   if (ztm) {
     // Tensor memory is allocated per CTA, and the CTAs on one SM must never
     // ask for more than its 512 columns together (an allocation would wait
@@ -370,15 +373,15 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     k3_parts = (int)std::max(1L, std::min<long>(4 / k3_wpp, spread));
     // (the kernel's own static shared memory, 16 bytes, is within the 64
     // left out; that slack cannot add up to another CTA's share)
-    const size_t fixed = k3c_fixed_bytes<T>(n) * (size_t)k3_parts;
+    const size_t fixed = k3c_fixed_bytes<T>(n, K3_TM_SWEEPS) * (size_t)k3_parts;
     const size_t foot = (size_t)dp.smem_sm * (size_t)k3_acols / 512;
     const size_t other = (size_t)dp.smem_rsv + 64;
     k3c_smem = std::max(fixed, foot > other ? foot - other : 0);
     int nb = 0;
     bool ok = k3c_smem + 64 <= (size_t)dp.smem_optin;
     if (ok) {
-      if ((err = set_smem(k3_tmem<T>, k3c_smem)) != cudaSuccess) return err;
-      if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k3_tmem<T>, 32 * k3_wpp * k3_parts,
+      if ((err = set_smem(k3t, k3c_smem)) != cudaSuccess) return err;
+      if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k3t, 32 * k3_wpp * k3_parts,
                                                                k3c_smem)) != cudaSuccess)
         return err;
       ok = nb >= 1 && nb * k3_acols <= 512;
@@ -449,7 +452,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
       k3_warp<T><<<(unsigned)((cnt + K3W_NW - 1) / K3W_NW), 32 * K3W_NW, k3w_smem, st>>>(q);
     } else if (ztm) {
       const long nparts = cnt * pl.zsplit;
-      k3_tmem<T><<<(unsigned)((nparts + k3_parts - 1) / k3_parts), 32 * k3_wpp * k3_parts, k3c_smem, st>>>(
+      k3t<<<(unsigned)((nparts + k3_parts - 1) / k3_parts), 32 * k3_wpp * k3_parts, k3c_smem, st>>>(
           q, k3_wpp, k3_acols);
     } else if (zsm) {
       k3_cta<T, true, 1><<<(unsigned)(cnt * pl.zsplit), k3_nt, k3c_smem, st>>>(q);

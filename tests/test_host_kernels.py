@@ -38,7 +38,7 @@ def hostlibs():
         f.restype = I
         getattr(libs["tridiag_host"], "host_tridiag" + s).argtypes = [I, I, I, P, I, I, P, P]
         getattr(libs["tridiag_host"], "host_tridiag_reg" + s).argtypes = [I, P, I, P, P]
-        getattr(libs["apply_host"], "host_apply" + s).argtypes = [I, P, P, I, I]
+        getattr(libs["apply_host"], "host_apply" + s).argtypes = [I, P, P, I, I, I]
         getattr(libs["apply_host"], "host_apply" + s).restype = I
     return libs
 
@@ -240,13 +240,15 @@ def test_pipelined_apply_matches_sequential(oracle_mod, hostlibs, n, method, dty
     flat = np.ascontiguousarray(rec)
     eps = np.finfo(dtype).eps
     first = None
-    for ch in (4 * (n + 1), n + 1, 10 ** 6):
-        z = np.ascontiguousarray(q0.copy())
-        segs = f(n, _p(z), _p(flat), flat.shape[0], ch)
-        assert segs > 0
-        assert np.abs(z - ref).max() <= 64 * n * eps * np.abs(ref).max()
-        # chunking changes which sweeps are applied as pairs; the paired
-        # pipeline does the same operations, so the results are identical
-        if first is None:
-            first = z
-        assert np.array_equal(z, first)
+    for kg in (0, 2, 4):
+        for ch in (4 * (n + 1), n + 1, 10 ** 6):
+            z = np.ascontiguousarray(q0.copy())
+            segs = f(n, _p(z), _p(flat), flat.shape[0], ch, kg)
+            assert segs > 0
+            assert np.abs(z - ref).max() <= 64 * n * eps * np.abs(ref).max()
+            # chunking and the group size change which sweeps are applied
+            # together; the pipelines do the same operations in the same
+            # order, so the results are identical
+            if first is None:
+                first = z
+            assert np.array_equal(z, first), (kg, ch)
