@@ -512,13 +512,15 @@ constexpr int K3_U = 8;
 // rotations alternate between two register sets: while one block is
 // applied, the next one's columns and records are already being loaded
 // (they lie below every column the current block stores).
+// seg_apply_h takes z_{i0+1} as the carried value h instead of loading it
+// (a sweep that continues another one's pass).
 template <class T, int CS>
-__host__ __device__ __forceinline__ void seg_apply(T *__restrict__ zr, const int cs_rt,
-                                                   const Rec<T> *__restrict__ rp, const int i0, const int len)
+__host__ __device__ __forceinline__ void seg_apply_h(T *__restrict__ zr, const int cs_rt,
+                                                     const Rec<T> *__restrict__ rp, const int i0, const int len,
+                                                     T h)
 {
   const int cs = CS > 0 ? CS : cs_rt;
   T *p = zr + i0 * cs;  // column of the next rotation's z_i (rotation j of the segment)
-  T h = p[cs];
   int j = 0;
   if (len >= K3_U) {
     T za[K3_U], zb[K3_U];
@@ -546,6 +548,13 @@ __host__ __device__ __forceinline__ void seg_apply(T *__restrict__ zr, const int
   }
   p[cs] = h;
 }
+template <class T, int CS>
+__host__ __device__ __forceinline__ void seg_apply(T *__restrict__ zr, const int cs_rt,
+                                                   const Rec<T> *__restrict__ rp, const int i0, const int len)
+{
+  const int cs = CS > 0 ? CS : cs_rt;
+  seg_apply_h<T, CS>(zr, cs_rt, rp, i0, len, zr[(i0 + 1) * cs]);
+}
 #undef EIGB_LOAD
 #undef EIGB_BLOCK
 #undef EIGB_CHAIN
@@ -572,16 +581,18 @@ template <class T> __host__ __device__ __forceinline__ int seg_walk(const Rec<T>
     OUT = yb_;                                       \
   }
 
-// Two consecutive sweeps over the same rotations i0 .. i0-len+1 (records
-// ra[0..len), rb[0..len)) as a two-stage pipeline on one row: the second
-// sweep trails the first by one column and takes the first's output from
-// registers, so each column is loaded and stored once for both sweeps
-// (half the shared-memory traffic of two seg_apply calls) and the two
-// fma chains are independent within a step.  Same result, rotation by
+// Two consecutive sweeps from the same top i0, the first over rotations
+// i0 .. i0-la+1 (records ra[0..la)), the second over i0 .. i0-len+1
+// (records rb[0..len), len <= la), as a two-stage pipeline on one row: the
+// second sweep trails the first by one column and takes the first's output
+// from registers, so each column they share is loaded and stored once for
+// both (half the shared-memory traffic of two seg_apply calls) and the two
+// fma chains are independent within a step; past the second sweep's end
+// the first continues alone (seg_apply_h).  Same result, rotation by
 // rotation, as seg_apply(ra) followed by seg_apply(rb).
 template <class T, int CS>
 __host__ __device__ __forceinline__ void seg_apply_pair(T *__restrict__ zr, const int cs_rt,
-                                                        const Rec<T> *__restrict__ ra,
+                                                        const Rec<T> *__restrict__ ra, const int la,
                                                         const Rec<T> *__restrict__ rb, const int i0, const int len)
 {
   const int cs = CS > 0 ? CS : cs_rt;
@@ -633,17 +644,26 @@ __host__ __device__ __forceinline__ void seg_apply_pair(T *__restrict__ zr, cons
     const T x0 = p[0];
     EIGB_PAIR_STEP(x0, ra[j], rb[j - 1], p[2 * cs])
   }
-  {  // second sweep, last rotation i0-len+1
+  if (la == len) {  // second sweep, last rotation i0-len+1, on the first's last value
     const Rec<T> r = rb[len - 1];
     p[2 * cs] = fma(r.c, hb, r.s * ha);
     p[cs] = fma(-r.s, hb, r.c * ha);
+  } else {  // the first sweep's rotation i0-len, then the second's last, then the first alone
+    const T x0 = p[0];
+    const Rec<T> a = ra[len], b = rb[len - 1];
+    const T ya = fma(a.c, ha, a.s * x0);
+    ha = fma(-a.s, ha, a.c * x0);
+    p[2 * cs] = fma(b.c, hb, b.s * ya);
+    p[cs] = fma(-b.s, hb, b.c * ya);
+    seg_apply_h<T, CS>(zr, cs_rt, ra + len + 1, i0 - len - 1, la - len - 1, ha);
   }
 }
 #undef EIGB_PAIR_STEP
 
 // Applies the segments of rbuf[0..used) (complete, as found by seg_walk) to
-// one row; two consecutive segments over the same rotations (the sweeps of
-// one QL index) go through seg_apply_pair.
+// one row; two consecutive segments from the same top, the second no
+// longer than the first (consecutive sweeps of the QL recurrence nest this
+// way), go through seg_apply_pair.
 template <class T, int CS>
 __host__ __device__ __forceinline__ void apply_segments(const Rec<T> *rbuf, const int used, T *zr, const int cs)
 {
@@ -654,9 +674,10 @@ __host__ __device__ __forceinline__ void apply_segments(const Rec<T> *rbuf, cons
     const int q2 = q + 1 + L;
     if (L >= 1 && q2 < used) {
       const Rec<T> h2 = rbuf[q2];
-      if (hdr_cnt(h2) == L && hdr_i0(h2) == i0) {
-        seg_apply_pair<T, CS>(zr, cs, rbuf + q + 1, rbuf + q2 + 1, i0, L);
-        q = q2 + 1 + L;
+      const int L2 = hdr_cnt(h2);
+      if (hdr_i0(h2) == i0 && L2 >= 1 && L2 <= L) {  // complete within used (seg_walk)
+        seg_apply_pair<T, CS>(zr, cs, rbuf + q + 1, L, rbuf + q2 + 1, i0, L2);
+        q = q2 + 1 + L2;
         continue;
       }
     }
