@@ -197,13 +197,13 @@ template <class T> __device__ __forceinline__ uint32_t tmem_at(const uint32_t z0
 
 // seg_apply on a row in TMEM: the same operations in the same order, so
 // the results are bit-identical to the shared-memory form.
+// (seg_apply_tm_h takes z_{i0+1} as the carried value h: a sweep that
+// continues another one's pass, whose stores are this thread's own)
 template <class T>
-__device__ __forceinline__ void seg_apply_tm(const uint32_t z0, const Rec<T> *__restrict__ rp, const int i0,
-                                             const int len)
+__device__ __forceinline__ void seg_apply_tm_h(const uint32_t z0, const Rec<T> *__restrict__ rp, const int i0,
+                                               const int len, T h)
 {
-  tmem_wait_st();  // the previous segment's stores land before these loads
-  int c = i0;      // column of the next rotation's z_i
-  T h = tmem_ld1((const T *)nullptr, tmem_at<T>(z0, c + 1));
+  int c = i0;  // column of the next rotation's z_i
   int j = 0;
   for (; j + 8 <= len; j += 8, c -= 8) {
     T z[8];
@@ -232,6 +232,13 @@ __device__ __forceinline__ void seg_apply_tm(const uint32_t z0, const Rec<T> *__
   }
   tmem_st1(tmem_at<T>(z0, c + 1), h);
 }
+template <class T>
+__device__ __forceinline__ void seg_apply_tm(const uint32_t z0, const Rec<T> *__restrict__ rp, const int i0,
+                                             const int len)
+{
+  tmem_wait_st();  // the previous segment's stores land before these loads
+  seg_apply_tm_h<T>(z0, rp, i0, len, tmem_ld1((const T *)nullptr, tmem_at<T>(z0, i0 + 1)));
+}
 
 // Row accessor for seg_apply_group: this thread's row in TMEM
 template <class T> struct RowTM {
@@ -244,7 +251,7 @@ template <class T> struct RowTM {
 
 // seg_apply_pair on a row in TMEM (bit-identical to the shared-memory form)
 template <class T>
-__device__ __forceinline__ void seg_apply_pair_tm(const uint32_t z0, const Rec<T> *__restrict__ ra,
+__device__ __forceinline__ void seg_apply_pair_tm(const uint32_t z0, const Rec<T> *__restrict__ ra, const int la,
                                                   const Rec<T> *__restrict__ rb, const int i0, const int len)
 {
   tmem_wait_st();
@@ -281,10 +288,18 @@ __device__ __forceinline__ void seg_apply_pair_tm(const uint32_t z0, const Rec<T
     hb = fma(-b.s, hb, b.c * ya);
     tmem_st1(tmem_at<T>(z0, c + 2), yb);
   }
-  {
+  if (la == len) {  // second sweep, last rotation, on the first's last value
     const Rec<T> r = rb[len - 1];
     tmem_st1(tmem_at<T>(z0, c + 2), fma(r.c, hb, r.s * ha));
     tmem_st1(tmem_at<T>(z0, c + 1), fma(-r.s, hb, r.c * ha));
+  } else {  // the first sweep's rotation c, the second's last, then the first alone
+    const T x = tmem_ld1((const T *)nullptr, tmem_at<T>(z0, c));
+    const Rec<T> a = ra[len], b = rb[len - 1];
+    const T ya = fma(a.c, ha, a.s * x);
+    ha = fma(-a.s, ha, a.c * x);
+    tmem_st1(tmem_at<T>(z0, c + 2), fma(b.c, hb, b.s * ya));
+    tmem_st1(tmem_at<T>(z0, c + 1), fma(-b.s, hb, b.c * ya));
+    seg_apply_tm_h<T>(z0, ra + len + 1, c - 1, la - len - 1, ha);
   }
 }
 
@@ -299,8 +314,8 @@ template <class T> struct SingleTM {
 
 // apply_segments for a row in TMEM (bit-identical to the shared-memory
 // form).  KG > 1: groups of up to KG consecutive sweeps go through
-// seg_apply_group; KG = 1: two consecutive sweeps over the same rotations
-// go through seg_apply_pair_tm (measured on B200: groups pay off for rows
+// seg_apply_group; KG = 1: two consecutive sweeps from the same top, the
+// second no longer than the first, go through seg_apply_pair_tm (measured on B200: groups pay off for rows
 // of 128 or more, the pairs below that).
 template <class T, int KG>
 __device__ __forceinline__ void apply_segments_tm(const Rec<T> *rbuf, const int used, const uint32_t z0)
@@ -316,9 +331,10 @@ __device__ __forceinline__ void apply_segments_tm(const Rec<T> *rbuf, const int 
     const int q2 = q + 1 + L;
     if (L >= 1 && q2 < used) {
       const Rec<T> h2 = rbuf[q2];
-      if (hdr_cnt(h2) == L && hdr_i0(h2) == i0) {
-        seg_apply_pair_tm<T>(z0, rbuf + q + 1, rbuf + q2 + 1, i0, L);
-        q = q2 + 1 + L;
+      const int L2 = hdr_cnt(h2);
+      if (hdr_i0(h2) == i0 && L2 >= 1 && L2 <= L) {
+        seg_apply_pair_tm<T>(z0, rbuf + q + 1, L, rbuf + q2 + 1, i0, L2);
+        q = q2 + 1 + L2;
         continue;
       }
     }
