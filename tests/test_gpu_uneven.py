@@ -51,3 +51,18 @@ def test_uneven_jacobi_and_errors(oracle_mod):
         E().solve_uneven(zeros(40 * 40 + 4), [40, 2], method=2)
     with pytest.raises(E().EigenGError):      # above the size limit
         E().solve_uneven(zeros(1025 * 1025), [1025])
+
+
+def test_uneven_tensor_memory_bit_identical(oracle_mod):
+    """The apply phase of every order group gives the same bits with the
+    rows of Z in tensor memory (default) as in shared memory."""
+    rng = np.random.default_rng(7)
+    ns = [int(x) for x in rng.integers(33, 300, size=24)] + [64, 96, 128, 200, 256]
+    mats = [oracle_mod.sym_uniform(1, n, seed=int(rng.integers(1 << 30)))[0] for n in ns]
+    flat = np.concatenate([m.reshape(-1) for m in mats])
+    a1 = torch.from_numpy(flat.copy()).cuda()
+    a2 = torch.from_numpy(flat.copy()).cuda()
+    w1, i1 = E().solve_uneven(a1, ns)
+    w2, i2 = E().solve_uneven(a2, ns, zmem=E().ZMEM_SHARED)
+    torch.cuda.synchronize()
+    assert torch.equal(a1, a2) and torch.equal(w1, w2) and torch.equal(i1, i2)
