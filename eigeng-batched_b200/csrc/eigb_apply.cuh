@@ -15,6 +15,11 @@
 // not reached a column yet, or has passed its last rotation, acts as the
 // identity on the wave (its carried value moves on unchanged); the first
 // K-1 steps fill the pipeline and the last K steps drain it.
+//
+// Used by the tensor-memory apply (k3_tmem) for rows of 128 or more; the
+// row accessor below lets the host-side unit tests run the same code on
+// memory.  The shared-memory and workspace forms (k3_cta) keep their
+// pairs of sweeps (seg_apply_pair), measured faster there.
 #pragma once
 #include "eigb_common.cuh"
 
@@ -23,8 +28,8 @@ namespace eigb {
 // Sweeps applied per pass at most.
 constexpr int K3_GROUP = 4;
 
-// Row accessor for Z in shared or global memory: element c at z[c*cs]
-// (CS > 0: the stride known at compile time).
+// Row accessor for a row in memory: element c at z[c*cs] (CS > 0: the
+// stride known at compile time).
 template <class T, int CS> struct RowMem {
   T *z;
   int cs_rt;
