@@ -76,7 +76,8 @@ typedef struct eigen_GPU_batch_opts {
                     apply phase; <= 0: automatic (the fewest whose rows fit
                     in shared memory).  Larger values trade re-reads of the
                     rotation records for more warps per SM. */
-  int zmem;      /* EIGEN_GPU_ZMEM_AUTO (0) or EIGEN_GPU_ZMEM_SHARED */
+  int zmem;      /* EIGEN_GPU_ZMEM_AUTO (0; any other value but
+                    EIGEN_GPU_ZMEM_SHARED means the same) or EIGEN_GPU_ZMEM_SHARED */
   int reserved;
 } eigen_GPU_batch_opts;
 
