@@ -163,14 +163,26 @@ cudaError_t make_plan(long L, int nm, int n, const DevProps &dp, Plan<T> &pl, co
     }
     // tensor memory holds up to 128 rows of a matrix per part (rows of up
     // to 512 32-bit columns: FP64 n <= 256, FP32 n <= 512), unless that
-    // takes more parts per matrix than shared memory does: every part reads
-    // all of the matrix's records (measured on B200: FP64 n = 160, two parts
-    // of 80 rows, is slower than one shared-memory CTA of 160 rows)
+    // takes more parts per matrix than shared memory does and leaves an SM
+    // fewer warps: every part reads all of the matrix's records (measured
+    // on B200: FP64 n = 160, two parts of 80 rows with one CTA per SM, is
+    // slower than one shared-memory CTA of 160 rows; FP32 n = 200, two
+    // parts of 100 rows with two CTAs per SM, is faster than one of 200)
     if (pl.zrows > 0 && tmem_cols<T>(n) > 0 && !(opts && opts->zmem == EIGEN_GPU_ZMEM_SHARED)) {
       int split = (n + 127) / 128;
       const int want = opts ? opts->split : 0;
       if (want > split) split = std::min(want, (n + 31) / 32);
-      if (split <= pl.zsplit) {
+      bool use = split <= pl.zsplit;
+      if (!use) {
+        const int zr_t = (n + split - 1) / split;
+        const long warps_t = (long)(512 / tmem_cols<T>(n)) * ((zr_t + 31) / 32);
+        const size_t foot_s = k3c_smem_bytes<T>(n, pl.zrows) + (size_t)dp.smem_rsv;
+        const long ctas_s = std::max<long>(1, std::min<long>((long)dp.smem_sm / (long)foot_s,
+                                                              2048 / (((pl.zrows + 31) / 32) * 32)));
+        const long warps_s = ctas_s * ((pl.zrows + 31) / 32);
+        use = warps_t >= warps_s;
+      }
+      if (use) {
         pl.zsplit = split;
         pl.zrows = (n + split - 1) / split;
         pl.ztm = 1;
