@@ -103,11 +103,14 @@ template <class T> int k1c_block(int n, size_t optin)
 template <class T> size_t k2_smem_per_thread(int n) { return sizeof(T) * 2 * (size_t)n; }
 
 // Phase 2 matrices per warp: the largest power of two that still gives
-// each SM about three warps (measured on B200: 8 per warp for 4096
-// matrices, 32 for 16384).
+// each SM about three warps; two for batches of 1025 .. 2048 (measured on
+// B200: 8 per warp for 4096 matrices, 32 for 16384, 2 for 2048 at n = 32 ..
+// 256).  Smaller batches, such as the chunks of solve_host that run beside
+// another chunk's solve, keep the rule: one per warp would be faster alone
+// but crowds out the concurrent solve.
 inline int k2_mpw(long L, int sms)
 {
-  const long target = 3L * sms;
+  const long target = (L > 1024 && L <= 2048) ? L / 2 : 3L * sms;
   int m = 32;
   while (m > 1 && (L + m - 1) / m < target) m >>= 1;
   return m;
