@@ -26,7 +26,7 @@
 namespace eigb {
 
 // Sweeps applied per pass at most.
-constexpr int K3_GROUP = 4;
+constexpr int K3_GROUP = 8;
 
 // Row accessor for a row in memory: element c at z[c*cs] (CS > 0: the
 // stride known at compile time).
@@ -166,6 +166,21 @@ __host__ __device__ __forceinline__ int seg_group(const Rec<T> *rbuf, const int 
   return k;
 }
 
+// seg_apply_group for the first K of the sweeps found by seg_group
+template <class T, int K, class Row>
+__host__ __device__ __forceinline__ void group_call(const Row &row, const Rec<T> *const (&rp)[K3_GROUP], const int i0,
+                                                   const int (&L)[K3_GROUP])
+{
+  const Rec<T> *r[K];
+  int l[K];
+#pragma unroll
+  for (int j = 0; j < K; j++) {
+    r[j] = rp[j];
+    l[j] = L[j];
+  }
+  seg_apply_group<T, K>(row, r, i0, l);
+}
+
 // Applies the complete segments of rbuf[0..used) to one row: groups of up
 // to KG sweeps through seg_apply_group, single sweeps through `single`
 // (a functor taking the records, the top index and the length).
@@ -178,20 +193,15 @@ __host__ __device__ __forceinline__ void apply_grouped(const Rec<T> *rbuf, const
     int i0, qn, L[K3_GROUP];
     const Rec<T> *rp[K3_GROUP];
     const int k = seg_group<T, KG>(rbuf, q, used, i0, rp, L, qn);
-    if (k == 1) {
-      single(rp[0], i0, L[0]);
-    } else if (k == 2) {
-      const Rec<T> *const r2[2] = {rp[0], rp[1]};
-      const int l2[2] = {L[0], L[1]};
-      seg_apply_group<T, 2>(row, r2, i0, l2);
-    } else if (KG >= 3 && k == 3) {
-      const Rec<T> *const r3[3] = {rp[0], rp[1], rp[2]};
-      const int l3[3] = {L[0], L[1], L[2]};
-      seg_apply_group<T, 3>(row, r3, i0, l3);
-    } else if (KG >= 4) {
-      const Rec<T> *const r4[4] = {rp[0], rp[1], rp[2], rp[3]};
-      const int l4[4] = {L[0], L[1], L[2], L[3]};
-      seg_apply_group<T, 4>(row, r4, i0, l4);
+    switch (k) {  // k <= KG: the larger cases are compiled only where they can occur
+      case 1: single(rp[0], i0, L[0]); break;
+      case 2: group_call<T, 2>(row, rp, i0, L); break;
+      case 3: if (KG >= 3) group_call<T, (KG >= 3 ? 3 : 2)>(row, rp, i0, L); break;
+      case 4: if (KG >= 4) group_call<T, (KG >= 4 ? 4 : 2)>(row, rp, i0, L); break;
+      case 5: if (KG >= 5) group_call<T, (KG >= 5 ? 5 : 2)>(row, rp, i0, L); break;
+      case 6: if (KG >= 6) group_call<T, (KG >= 6 ? 6 : 2)>(row, rp, i0, L); break;
+      case 7: if (KG >= 7) group_call<T, (KG >= 7 ? 7 : 2)>(row, rp, i0, L); break;
+      default: if (KG >= 8) group_call<T, (KG >= 8 ? 8 : 2)>(row, rp, i0, L); break;
     }
     q = qn;
   }

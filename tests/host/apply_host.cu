@@ -12,7 +12,7 @@ template <class T> struct SingleMem {
 };
 
 // kg = 0: apply_segments (k3_cta's walker, pairs of equal sweeps);
-// kg = 2, 4: apply_grouped with groups of up to kg sweeps (k3_tmem's walker)
+// kg = 2, 4, 8: apply_grouped with groups of up to kg sweeps (k3_tmem's walker)
 template <class T> static int run(int n, T *Z, const T *recs, int nrec, int ch, int kg)
 {
   using namespace eigb;
@@ -24,7 +24,8 @@ template <class T> static int run(int n, T *Z, const T *recs, int nrec, int ch, 
     const int used = seg_walk(rb, cnt);
     for (int r = 0; r < n; r++) {
       T *z = Z + r * n;
-      if (kg == 4) apply_grouped<T, 4>(rb, used, RowMem<T, 1>{z, 1}, SingleMem<T>{z});
+      if (kg == 8) apply_grouped<T, 8>(rb, used, RowMem<T, 1>{z, 1}, SingleMem<T>{z});
+      else if (kg == 4) apply_grouped<T, 4>(rb, used, RowMem<T, 1>{z, 1}, SingleMem<T>{z});
       else if (kg == 2) apply_grouped<T, 2>(rb, used, RowMem<T, 1>{z, 1}, SingleMem<T>{z});
       else apply_segments<T, 1>(rb, used, z, 1);
     }

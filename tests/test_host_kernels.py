@@ -240,7 +240,7 @@ def test_pipelined_apply_matches_sequential(oracle_mod, hostlibs, n, method, dty
     flat = np.ascontiguousarray(rec)
     eps = np.finfo(dtype).eps
     first = None
-    for kg in (0, 2, 4):
+    for kg in (0, 2, 4, 8):
         for ch in (4 * (n + 1), n + 1, 10 ** 6):
             z = np.ascontiguousarray(q0.copy())
             segs = f(n, _p(z), _p(flat), flat.shape[0], ch, kg)
