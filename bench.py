@@ -33,7 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "eigeng-batched_b200"))
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "cusolver"])
     ap.add_argument("--n", type=int, default=128)
@@ -71,7 +71,7 @@ class ClockSampler:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-    PERIOD_MS = 100
+    PERIOD_MS = 50
 
     def __init__(self, gpu):
         self.gpu = gpu

@@ -370,13 +370,14 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems(n, k1c_nt, pl.k1b);
   size_t k3c_smem = k3c_smem_bytes<T>(n, ztm ? 0 : pl.zrows);
   int k3_wpp = 0, k3_parts = 0, k3_acols = 0;  // tensor-memory form: warps per part, parts per CTA, columns
-  // sweeps per pass: up to eight for FP64 rows of 128 or more and FP32 rows
-  // of 256 or more, four for the FP32 rows between, pairs below 128
-  // (measured on B200: the longer groups give each thread more independent
-  // rotation chains, at more registers, which costs the FP32 n < 256 CTAs
-  // that share an SM)
+  // sweeps per pass: up to eight for rows of 256 or more, four for rows of
+  // 128 .. 255, pairs below 128 (measured on B200: the longer groups give
+  // each thread more independent rotation chains, at 254 registers, which
+  // costs the CTAs that share an SM; at FP64 n=128 eight save 0.12 ms of
+  // phase 3 alone but lose 1.7 ms of a host-to-host solve, where the other
+  // chunks' phase-1/2 CTAs run beside phase 3)
   void (*k3t)(const KP<T>, const int, const int) =
-      n < 128 ? k3_tmem<T, 1> : ((sizeof(T) == 8 || n >= 256) ? k3_tmem<T, 8> : k3_tmem<T, 4>);
+      n < 128 ? k3_tmem<T, 1> : (n >= 256 ? k3_tmem<T, 8> : k3_tmem<T, 4>);
   if (ztm) {
     // Tensor memory is allocated per CTA, and the CTAs on one SM must never
     // ask for more than its 512 columns together (an allocation would wait
