@@ -291,14 +291,28 @@ struct Indirect {
   const long long *aoff = nullptr, *woff = nullptr;
 };
 
+// Part of a solve: the phases in `phases` (EIGEN_GPU_STAGE_* bits) for
+// matrices first .. first+count-1 of the batch (count < 0: to its end).
+struct Stage {
+  long first = 0, count = -1;
+  int phases = EIGEN_GPU_STAGE_ALL;
+};
+
 // ap: packed upper-triangle input (nullptr: the upper triangle of a); the
-// eigenvectors go to a either way.  ix: see Indirect.
+// eigenvectors go to a either way.  ix: see Indirect.  sg: a part of the
+// solve; any part but the whole needs a workspace that holds the whole
+// batch (one chunk), whose slot k belongs to matrix k.
 template <class T>
 cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork, int *info,
                 const eigen_GPU_batch_opts *opts, cudaStream_t stream, const T *ap = nullptr,
-                const Indirect &ix = Indirect())
+                const Indirect &ix = Indirect(), const Stage &sg = Stage())
 {
   if (bad_args(L, nm, n, m) || a == nullptr || w == nullptr) return cudaErrorInvalidValue;
+  const long first = sg.first, count = sg.count <= 0 ? L - sg.first : sg.count;
+  if (first < 0 || count < 1 || first + count > L || sg.phases < 1 || sg.phases > EIGEN_GPU_STAGE_ALL)
+    return cudaErrorInvalidValue;
+  const bool ranged = first != 0 || count != L || sg.phases != EIGEN_GPU_STAGE_ALL;
+  if (ranged && ix.kid) return cudaErrorInvalidValue;
   int method = EIGEN_GPU_BATCH_TQL2, sort = 1, max_sweep = 100;
   if (opts) {
     method = opts->method;
@@ -314,13 +328,16 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   p.kid = ix.kid;
   p.aoff = ix.aoff;
   p.woff = ix.woff;
+  // n = 1 and the Jacobi method are one pass each: a part runs it for its
+  // matrices with the apply bit and does nothing for the others
+  if ((n == 1 || method == EIGEN_GPU_BATCH_JACOBI) && !(sg.phases & EIGEN_GPU_STAGE_APPLY)) return cudaSuccess;
   if (n == 1) {
-    p.a = a;
-    p.w = w;
-    p.ap = ap;
-    p.info = info;
-    p.Lc = L;
-    const int blocks = (int)std::min<long>((L + 255) / 256, 4096);
+    p.a = a + (size_t)first * nm * n;
+    p.w = w + (size_t)first * n;
+    p.ap = ap ? ap + (size_t)first * packed_size(n) : nullptr;
+    p.info = info ? info + first : nullptr;
+    p.Lc = count;
+    const int blocks = (int)std::min<long>((count + 255) / 256, 4096);
     k_n1<T><<<blocks, 256, 0, stream>>>(p);
     return cudaGetLastError();
   }
@@ -334,12 +351,12 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   if (method == EIGEN_GPU_BATCH_JACOBI) {
     const size_t smem = sizeof(JacSlot<T>) * K1W_NW;
     if ((err = set_smem(k_jacobi_warp<T>, smem)) != cudaSuccess) return err;
-    p.a = a;
-    p.w = w;
-    p.ap = ap;
-    p.info = info;
-    p.Lc = L;
-    const long blocks = (L + K1W_NW - 1) / K1W_NW;
+    p.a = a + (size_t)first * nm * n;
+    p.w = w + (size_t)first * n;
+    p.ap = ap ? ap + (size_t)first * packed_size(n) : nullptr;
+    p.info = info ? info + first : nullptr;
+    p.Lc = count;
+    const long blocks = (count + K1W_NW - 1) / K1W_NW;
     k_jacobi_warp<T><<<(unsigned)blocks, 32 * K1W_NW, smem, stream>>>(p);
     return cudaGetLastError();
   }
@@ -347,12 +364,13 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   Plan<T> pl;
   if ((err = make_plan<T>(L, nm, n, dp, pl, opts)) != cudaSuccess) return err;
   if (wk == nullptr || (lwork != 0 && lwork < pl.bytes)) return cudaErrorInvalidValue;
+  if (ranged && pl.Lc < L) return cudaErrorInvalidValue;  // a part needs the whole batch's workspace
   char *base = static_cast<char *>(wk);
-  p.d = reinterpret_cast<T *>(base + pl.off_d);
-  p.e = reinterpret_cast<T *>(base + pl.off_e);
-  p.meta = reinterpret_cast<Meta *>(base + pl.off_meta);
-  p.rec = reinterpret_cast<Rec<T> *>(base + pl.off_rec);
-  p.zs = reinterpret_cast<T *>(base + pl.off_z);
+  T *const ws_d = reinterpret_cast<T *>(base + pl.off_d);
+  T *const ws_e = reinterpret_cast<T *>(base + pl.off_e);
+  Meta *const ws_meta = reinterpret_cast<Meta *>(base + pl.off_meta);
+  Rec<T> *const ws_rec = reinterpret_cast<Rec<T> *>(base + pl.off_rec);
+  T *const ws_z = reinterpret_cast<T *>(base + pl.off_z);
   p.rcap = pl.rcap;
 
   // launch geometry
@@ -389,7 +407,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     // most 64 rows, unless the chunk is too small to fill the SMs.
     k3_acols = tmem_cols<T>(n);
     k3_wpp = (pl.zrows + 31) / 32;
-    const long spread = (std::min(L, pl.Lc) * pl.zsplit + dp.sms - 1) / dp.sms;
+    const long spread = (std::min(count, pl.Lc) * pl.zsplit + dp.sms - 1) / dp.sms;
     k3_parts = (int)std::max(1L, std::min<long>(4 / k3_wpp, spread));
     // (the kernel's own static shared memory, 16 bytes, is within the 64
     // left out; that slack cannot add up to another CTA's share)
@@ -420,7 +438,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   const bool zsm = pl.zrows > 0 && !ztm;
   // phase 2: matrices per warp, then warps per block within the shared
   // memory budget (2n values per matrix)
-  p.k2mpw = k2_mpw(std::min(L, pl.Lc), dp.sms);
+  p.k2mpw = k2_mpw(std::min(count, pl.Lc), dp.sms);
   int k2_mpb = 32;  // matrices per block, a multiple of k2mpw
   {
     const size_t per = k2_smem_per_thread<T>(n);
@@ -482,9 +500,17 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
       k3_cta<T, false, 1><<<(unsigned)cnt, k3_nt, k3c_smem, st>>>(q);
     }
   };
-  for (long c0 = 0; c0 < L; c0 += pl.Lc) {
-    const long lc = std::min(pl.Lc, L - c0);
-    const long chunk = c0 / pl.Lc;
+  for (long c0 = first; c0 < first + count; c0 += pl.Lc) {
+    const long lc = std::min(pl.Lc, first + count - c0);
+    const long chunk = (c0 - first) / pl.Lc;
+    // workspace slot of the chunk's first matrix: chunks reuse the
+    // workspace from slot 0; a part of the solve uses the matrices' own
+    const size_t wo = ranged ? (size_t)c0 : 0;
+    p.d = ws_d + wo * n;
+    p.e = ws_e + wo * n;
+    p.meta = ws_meta + wo;
+    p.rec = ws_rec + wo * (size_t)pl.rcap;
+    p.zs = ws_z + wo * (size_t)n * n;
     if (ix.kid) {  // the index list advances instead of the pointers
       p.a = a;
       p.w = w;
@@ -499,11 +525,11 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     }
     p.Lc = lc;
     trace(chunk, 0, stream);
-    phase1(p, lc, stream);
+    if (sg.phases & EIGEN_GPU_STAGE_REDUCE) phase1(p, lc, stream);
     trace(chunk, 1, stream);
-    phase2(p, lc, stream);
+    if (sg.phases & EIGEN_GPU_STAGE_QL) phase2(p, lc, stream);
     trace(chunk, 2, stream);
-    phase3(p, lc, stream);
+    if (sg.phases & EIGEN_GPU_STAGE_APPLY) phase3(p, lc, stream);
     trace(chunk, 3, stream);
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
   }
@@ -880,6 +906,28 @@ cudaError_t eigen_GPU_batch_ex_FP(const int L, const int nm, const int n, const 
                                   const cudaStream_t stream)
 {
   return eigb::run<float>(L, nm, n, m, a, w, wk, lwork, info, opts, stream);
+}
+
+cudaError_t eigen_GPU_batch_stage_DP(const int L, const int nm, const int n, const int m, double *a, double *w,
+                                     void *wk, const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                     const int phases, const int first, const int count, const cudaStream_t stream)
+{
+  eigb::Stage sg;
+  sg.first = first;
+  sg.count = count;
+  sg.phases = phases;
+  return eigb::run<double>(L, nm, n, m, a, w, wk, lwork, info, opts, stream, nullptr, eigb::Indirect(), sg);
+}
+
+cudaError_t eigen_GPU_batch_stage_FP(const int L, const int nm, const int n, const int m, float *a, float *w,
+                                     void *wk, const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                     const int phases, const int first, const int count, const cudaStream_t stream)
+{
+  eigb::Stage sg;
+  sg.first = first;
+  sg.count = count;
+  sg.phases = phases;
+  return eigb::run<float>(L, nm, n, m, a, w, wk, lwork, info, opts, stream, nullptr, eigb::Indirect(), sg);
 }
 
 void eigen_GPU_check_DP(const int L, const int nm, const int n, const int m, double *a, double *w, double *z,

@@ -22,6 +22,8 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libeigenGbatch.so")
 
 TQL2, IMTQL2, JACOBI = 0, 1, 2
 ZMEM_AUTO, ZMEM_SHARED = 0, 1  # where the apply phase keeps Z (eigen_GPU_batch_opts.zmem)
+# phases of eigen_GPU_batch_stage_* (EIGEN_GPU_STAGE_*)
+STAGE_REDUCE, STAGE_QL, STAGE_APPLY, STAGE_ALL = 1, 2, 4, 7
 
 _lib = None
 
@@ -57,6 +59,9 @@ def lib():
             f.restype = I
             f = getattr(L, "eigen_GPU_batch_ex_" + s)
             f.argtypes = [I, I, I, I, P, P, P, SZ, P, ctypes.POINTER(Opts), P]
+            f.restype = I
+            f = getattr(L, "eigen_GPU_batch_stage_" + s)
+            f.argtypes = [I, I, I, I, P, P, P, SZ, P, ctypes.POINTER(Opts), I, I, I, P]
             f.restype = I
             f = getattr(L, "eigen_GPU_check_" + s)
             f.argtypes = [I, I, I, I, P, P, P, P]
@@ -137,6 +142,7 @@ def exported_symbols():
         "eigen_GPU_batch_BufferSize_DP", "eigen_GPU_batch_BufferSize_FP",
         "eigen_GPU_batch_ex_DP", "eigen_GPU_batch_ex_FP",
         "eigen_GPU_batch_ex_BufferSize_DP", "eigen_GPU_batch_ex_BufferSize_FP",
+        "eigen_GPU_batch_stage_DP", "eigen_GPU_batch_stage_FP",
         "eigen_GPU_check_DP", "eigen_GPU_check_FP",
         "eigen_GPU_check_ex_DP", "eigen_GPU_check_ex_FP",
         "eigen_GPU_batch_trace", "eigen_GPU_batch_noalloc_DP",
@@ -220,6 +226,21 @@ def eigen_GPU_batch_ex(a, w, wk, n, nm=None, m=None, info=None, method=TQL2, sor
     lw = 0 if wk is None else wk.numel() * wk.element_size()
     return getattr(lib(), "eigen_GPU_batch_ex_" + _sfx(a.dtype))(
         L, nm, n, m, _ptr(a), _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), _stream(stream))
+
+
+def stage(a, w, wk, n, phases, first=0, count=0, nm=None, m=None, info=None, method=TQL2, sort=True,
+          max_sweep=100, stream=None, rec_cap=0, split=0, zmem=ZMEM_AUTO):
+    """eigen_GPU_batch_stage_*: the phases in ``phases`` (STAGE_* bits) for
+    matrices first .. first+count-1 (count <= 0: to the end) of the batch
+    ``a``; ``wk`` is the whole batch's workspace (``workspace(..., chunk=L)``).
+    Returns the cudaError_t status."""
+    L, nm = _dims(a, n, nm)
+    m = n if m is None else m
+    o = Opts(method, 1 if sort else 0, max_sweep, rec_cap, L, split, zmem)
+    lw = 0 if wk is None else wk.numel() * wk.element_size()
+    return getattr(lib(), "eigen_GPU_batch_stage_" + _sfx(a.dtype))(
+        L, nm, n, m, _ptr(a), _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), phases, first, count,
+        _stream(stream))
 
 
 def eigen_GPU_batch_noalloc(a, w, n, nm=None, m=None, info=None, stream=None):

@@ -107,6 +107,35 @@ cudaError_t eigen_GPU_batch_ex_FP(const int L, const int nm, const int n, const 
                                   const cudaStream_t stream);
 
 /*
+ * One part of an eigen_GPU_batch_ex_* solve (no counterpart in the
+ * reference): the phases selected by `phases` for matrices first ..
+ * first+count-1 of the batch of L (count <= 0: to the end of the batch).
+ * The phases of a matrix must run in order -- reduction, QL, apply --
+ * each after the previous one has completed (same stream, or an event
+ * between streams); parts for disjoint matrices may run concurrently.
+ * Running all three over all matrices, in any split into parts, gives the
+ * results of eigen_GPU_batch_ex_* bit for bit.  The workspace is the
+ * whole batch's: eigen_GPU_batch_ex_BufferSize_* for (L, nm, n, m, opts),
+ * with opts->chunk = 0 or >= L, and a plan that keeps the batch in one
+ * chunk (otherwise cudaErrorInvalidValue; set opts->chunk = L to force
+ * it).  Matrix k keeps its own workspace slot across the calls.  n = 1
+ * and the JACOBI method have a single pass, run by the part that includes
+ * EIGEN_GPU_STAGE_APPLY.  This lets a caller overlap host-device copies
+ * of some matrices with the phases of others and run the latency-bound
+ * QL phase over many matrices at once.
+ */
+#define EIGEN_GPU_STAGE_REDUCE 1 /* Householder tridiagonalization and Q */
+#define EIGEN_GPU_STAGE_QL 2     /* QL iteration, rotation records */
+#define EIGEN_GPU_STAGE_APPLY 4  /* rotations applied to Q, sort, output */
+#define EIGEN_GPU_STAGE_ALL 7
+cudaError_t eigen_GPU_batch_stage_DP(const int L, const int nm, const int n, const int m, double *a, double *w,
+                                     void *wk, const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                     const int phases, const int first, const int count, const cudaStream_t stream);
+cudaError_t eigen_GPU_batch_stage_FP(const int L, const int nm, const int n, const int m, float *a, float *w,
+                                     void *wk, const size_t lwork, int *info, const eigen_GPU_batch_opts *opts,
+                                     const int phases, const int first, const int count, const cudaStream_t stream);
+
+/*
  * Solve without allocating (no counterpart in the reference).  For callers
  * that must not allocate device memory -- a plugin's enqueue that runs
  * under an allocator owned by a framework, a real-time loop where

@@ -396,3 +396,63 @@ def test_solve_host_matches_device_solve(oracle_mod):
     torch.cuda.synchronize()
     w2, _, _ = gpu_solve(a0.astype(np.float32), n, nm)
     assert np.array_equal(wf.numpy(), w2)
+
+
+def _stage_parts(a0, n, nm, dtype, method):
+    """Solves a0 with eigen_GPU_batch_stage_*: the reductions in two parts on
+    two streams, the QL phase over the whole batch, the apply phase in three
+    parts."""
+    e = E()
+    L = a0.shape[0]
+    a = torch.from_numpy(np.ascontiguousarray(a0)).cuda()
+    w = torch.zeros((L, n), dtype=DT[dtype], device="cuda")
+    info = torch.full((L,), -7, dtype=torch.int32, device="cuda")
+    wk = e.workspace(L, nm, n, DT[dtype], chunk=L)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    assert e.stage(a, w, wk, n, e.STAGE_REDUCE, 0, 5, nm=nm, info=info, method=method, stream=s1) == 0
+    assert e.stage(a, w, wk, n, e.STAGE_REDUCE, 5, 0, nm=nm, info=info, method=method, stream=s2) == 0
+    s1.wait_stream(s2)
+    assert e.stage(a, w, wk, n, e.STAGE_QL, 0, 0, nm=nm, info=info, method=method, stream=s1) == 0
+    for c0, c1 in ((0, 2), (2, 9), (9, L)):
+        assert e.stage(a, w, wk, n, e.STAGE_APPLY, c0, c1 - c0, nm=nm, info=info, method=method, stream=s1) == 0
+    torch.cuda.synchronize()
+    return w.cpu().numpy(), a.cpu().numpy(), info.cpu().numpy()
+
+
+@pytest.mark.parametrize("n,nm,method", [(1, 1, 0), (20, 20, 0), (20, 21, 2), (48, 50, 0), (48, 48, 1),
+                                         (128, 128, 0), (200, 201, 0)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_stage_parts_match_whole_solve(oracle_mod, n, nm, method, dtype):
+    """The phases run in parts (eigen_GPU_batch_stage_*), split differently
+    per phase and on two streams, give the one-call solve's results bit for
+    bit (warp, register, shared/tensor-memory paths; Jacobi and n = 1 run at
+    the apply part)."""
+    O = oracle_mod
+    L = 13
+    a0 = np.zeros((L, n, nm), dtype=dtype)
+    a0[:, :, :n] = O.sym_uniform(L, n, seed=n + nm).astype(dtype)
+    w1, z1, i1 = gpu_solve(a0, n, nm, method=method)
+    w2, z2, i2 = _stage_parts(a0, n, nm, dtype, method)
+    assert np.array_equal(w1, w2) and np.array_equal(z1, z2) and np.array_equal(i1, i2)
+
+
+def test_stage_rejects_bad_parts():
+    import ctypes
+    e = E()
+    L, n = 6, 40
+    a = torch.zeros((L, n, n), dtype=torch.float64, device="cuda")
+    w = torch.zeros((L, n), dtype=torch.float64, device="cuda")
+    wk = e.workspace(L, n, n, torch.float64, chunk=L)
+    INVALID = 1  # cudaErrorInvalidValue
+    assert e.stage(a, w, wk, n, e.STAGE_REDUCE, 4, 3) == INVALID     # past the end of the batch
+    assert e.stage(a, w, wk, n, e.STAGE_REDUCE, -1, 2) == INVALID    # negative first
+    assert e.stage(a, w, wk, n, 0, 0, 2) == INVALID                  # no phase
+    assert e.stage(a, w, wk, n, 8, 0, 2) == INVALID                  # unknown phase bit
+    assert e.stage(a, w, wk[:64], n, e.STAGE_REDUCE, 0, 2) == INVALID  # workspace too small
+    # a plan that keeps the batch in several chunks cannot run a part
+    o = e.Opts(0, 1, 100, 0, 2, 0, 0)
+    st = e.lib().eigen_GPU_batch_stage_DP(L, n, n, n, a.data_ptr(), w.data_ptr(), wk.data_ptr(),
+                                          wk.numel(), None, ctypes.byref(o), e.STAGE_REDUCE, 0, 2, None)
+    assert st == INVALID
+    torch.cuda.synchronize()
