@@ -439,6 +439,11 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   // phase 2: matrices per warp, then warps per block within the shared
   // memory budget (2n values per matrix)
   p.k2mpw = k2_mpw(std::min(count, pl.Lc), dp.sms);
+  if (opts && opts->ql_mpw > 0) {
+    const int q = opts->ql_mpw;
+    if (q > 32 || (q & (q - 1)) != 0) return cudaErrorInvalidValue;
+    p.k2mpw = q;
+  }
   int k2_mpb = 32;  // matrices per block, a multiple of k2mpw
   {
     const size_t per = k2_smem_per_thread<T>(n);

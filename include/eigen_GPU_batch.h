@@ -78,7 +78,13 @@ typedef struct eigen_GPU_batch_opts {
                     rotation records for more warps per SM. */
   int zmem;      /* EIGEN_GPU_ZMEM_AUTO (0; any other value but
                     EIGEN_GPU_ZMEM_SHARED means the same) or EIGEN_GPU_ZMEM_SHARED */
-  int reserved;
+  int ql_mpw;    /* QL phase: matrices per warp (one per lane), a power of
+                    two 1..32; <= 0: automatic (about three warps per SM;
+                    fewer per warp spread a small batch over more warps).
+                    Solves that run concurrently on other streams do
+                    better with 4..8: fewer warps then take issue slots
+                    from the other solve's kernels.  Results do not
+                    depend on it. */
 } eigen_GPU_batch_opts;
 
 /* Workspace bytes for eigen_GPU_batch_ex_* with these options (NULL:

@@ -456,3 +456,27 @@ def test_stage_rejects_bad_parts():
                                           wk.numel(), None, ctypes.byref(o), e.STAGE_REDUCE, 0, 2, None)
     assert st == INVALID
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("n,dtype", [(20, np.float64), (64, np.float32), (128, np.float64)])
+def test_ql_matrices_per_warp_bit_identical(oracle_mod, n, dtype):
+    """opts.ql_mpw (QL matrices per warp) changes only the launch: every
+    power of two up to 32 gives the automatic choice's results; other
+    values are rejected."""
+    O = oracle_mod
+    e = E()
+    L = 37
+    a0 = O.sym_uniform(L, n, seed=3 * n).astype(dtype)
+    w1, z1, i1 = gpu_solve(a0, n)
+    for q in (1, 2, 4, 8, 16, 32):
+        a = torch.from_numpy(np.ascontiguousarray(a0)).cuda()
+        w = torch.empty((L, n), dtype=DT[dtype], device="cuda")
+        info = torch.zeros(L, dtype=torch.int32, device="cuda")
+        wk = e.workspace(L, n, n, DT[dtype])
+        assert e.eigen_GPU_batch_ex(a, w, wk, n, info=info, ql_mpw=q) == 0
+        torch.cuda.synchronize()
+        assert np.array_equal(w.cpu().numpy(), w1) and np.array_equal(a.cpu().numpy(), z1), q
+        assert np.array_equal(info.cpu().numpy(), i1)
+    for q in (3, 64):
+        assert e.eigen_GPU_batch_ex(a, w, wk, n, ql_mpw=q) == 1  # cudaErrorInvalidValue
+    torch.cuda.synchronize()
