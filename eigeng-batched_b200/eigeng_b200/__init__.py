@@ -415,11 +415,12 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
     # concurrently, so one chunk's latency-bound QL phase (which occupies
     # few SMs) overlaps the other chunk's reduction or apply phase
     nrun = min(2, nch)
-    # QL phase with four matrices per warp when chunks solve concurrently:
-    # its few lanes' chains then occupy fewer warps beside the other
-    # chunk's kernels (measured on B200 at n=128 FP64, L=4096: 20.3 against
-    # 21.3 ms; one chunk alone keeps the automatic choice)
-    ql_mpw = 4 if nrun > 1 else 0
+    # QL phase with eight matrices per warp when chunks solve concurrently:
+    # its lanes' chains then occupy fewer warps beside the other chunk's
+    # kernels (measured on B200 at n=128 FP64, L=4096, interleaved: 19.8 ms
+    # against 20.8 with four, 21.1 with two, 21.3 automatic; one chunk
+    # alone keeps the automatic choice)
+    ql_mpw = 8 if nrun > 1 else 0
     info = [torch.zeros(C, dtype=torch.int32, device=dev) for _ in range(nrun)]
     wk = [workspace(C, nm, n, dt, dev) if method != JACOBI else None for _ in range(nrun)]
     s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
