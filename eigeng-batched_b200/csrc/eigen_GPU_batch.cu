@@ -654,6 +654,10 @@ cudaError_t make_uneven_plan(long L, const int *n_host, const eigen_GPU_batch_op
     load[s] += (double)g.count * g.n * g.n * g.n;
     g.opts = opts ? *opts : eigen_GPU_batch_opts{};
     if (!opts) g.opts.sort = 1;
+    // groups solve concurrently: the QL phase at four matrices per warp
+    // leaves the other groups' kernels their issue slots (measured on B200,
+    // 10000 matrices of n ~ U[8,512] FP64: 1.40 s against 1.46 s)
+    if (g.opts.ql_mpw <= 0 && up.nstreams > 1) g.opts.ql_mpw = 4;
     if (g.n == 1 || method == EIGEN_GPU_BATCH_JACOBI) continue;  // no workspace
     Plan<T> one;
     eigen_GPU_batch_opts o1 = g.opts;

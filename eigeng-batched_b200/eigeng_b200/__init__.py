@@ -325,7 +325,7 @@ def solve_interleaved(ai, n, method=TQL2, sort=True, max_sweep=100, stream=None)
     return zi, wi, info
 
 
-def solve_uneven(a, ns, method=TQL2, sort=True, max_sweep=100, stream=None, zmem=ZMEM_AUTO):
+def solve_uneven(a, ns, method=TQL2, sort=True, max_sweep=100, stream=None, zmem=ZMEM_AUTO, ql_mpw=0):
     """eigen_GPU_batch_uneven: a is a flat CUDA tensor holding matrix k
     (order ns[k], column-major, leading dimension ns[k]) at offset
     sum_{j<k} ns[j]^2; solved in place.  Returns (w, info), w flat with the
@@ -335,7 +335,7 @@ def solve_uneven(a, ns, method=TQL2, sort=True, max_sweep=100, stream=None, zmem
     tot = sum(int(x) * int(x) for x in ns)
     if not a.is_cuda or not a.is_contiguous() or a.numel() != tot:
         raise EigenGError("a must be a contiguous CUDA tensor of sum(n^2) elements")
-    o = Opts(method, 1 if sort else 0, max_sweep, 0, 0, 0, zmem)
+    o = Opts(method, 1 if sort else 0, max_sweep, 0, 0, 0, zmem, ql_mpw)
     sfx = _sfx(a.dtype)
     lw = ctypes.c_size_t(0)
     st = getattr(lib(), "eigen_GPU_batch_uneven_BufferSize_" + sfx)(L, nsa, ctypes.byref(o), ctypes.byref(lw))
