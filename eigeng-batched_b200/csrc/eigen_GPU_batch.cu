@@ -541,6 +541,50 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   return cudaSuccess;
 }
 
+// Launch geometry of phase 1 (the matrix-parallel reduction) for the first
+// chunk of a default solve, as run() launches it; the counterpart of the
+// reference's eigen_GPU_batch_get_Launch_params (eigen_GPU_batch.hpp:23-102).
+template <class T>
+cudaError_t launch_params(long L, int n, int *grp, int *tb, int *gr, int *th, int *sh, int *l2)
+{
+  if (!grp || !tb || !gr || !th || !sh || !l2) return cudaErrorInvalidValue;
+  *grp = *tb = *gr = *th = *sh = *l2 = 0;
+  if (bad_args(L, n, n, n)) return cudaErrorInvalidValue;
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  *l2 = dp.l2;
+  if (n == 1) {  // k_n1: one thread per matrix
+    *grp = 1;
+    *gr = 256;
+    *th = 256;
+    *tb = (int)std::min<long>((L + 255) / 256, 4096);
+    return cudaSuccess;
+  }
+  Plan<T> pl;
+  if ((err = make_plan<T>(L, n, n, dp, pl, nullptr)) != cudaSuccess) return err;
+  const long lc = std::min(L, pl.Lc);
+  if (n <= 32) {  // k1_warp: one warp per matrix
+    *grp = 32;
+    *gr = K1W_NW;
+    *th = 32 * K1W_NW;
+    *tb = (int)((lc + K1W_NW - 1) / K1W_NW);
+    *sh = (int)(sizeof(T) * k1w_slot<T>() * K1W_NW);
+  } else if (reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin) {  // k1_reg: NB x NB warps
+    const int nb = reg_nb(n);
+    *grp = *th = 32 * nb * nb;
+    *gr = 1;
+    *tb = (int)lc;
+    *sh = (int)k1r_smem_bytes<T>(n);
+  } else {  // k1_cta
+    *grp = *th = k1c_threads(n);
+    *gr = 1;
+    *tb = (int)lc;
+    *sh = (int)(sizeof(T) * k1c_smem_elems(n, k1c_threads(n), pl.k1b));
+  }
+  return cudaSuccess;
+}
+
 // ---- interleaved layout ----
 //
 // Element (i, j) of matrix k at ai[(i + j*n)*L + k], eigenvalue j of matrix
@@ -1043,6 +1087,18 @@ cudaError_t eigen_GPU_batch_symfunc_FP(const int L, const int nm, const int n, c
                                        float *z, const int func, const double p, const cudaStream_t stream)
 {
   return eigb::symfunc_run<float>(L, nm, n, v, w, z, func, p, stream);
+}
+
+cudaError_t eigen_GPU_batch_launch_params_DP(const int L, const int n, int *grpSZ, int *numTB, int *numGR,
+                                             int *numTH, int *sizeSH, int *sizeL2)
+{
+  return eigb::launch_params<double>(L, n, grpSZ, numTB, numGR, numTH, sizeSH, sizeL2);
+}
+
+cudaError_t eigen_GPU_batch_launch_params_FP(const int L, const int n, int *grpSZ, int *numTB, int *numGR,
+                                             int *numTH, int *sizeSH, int *sizeL2)
+{
+  return eigb::launch_params<float>(L, n, grpSZ, numTB, numGR, numTH, sizeSH, sizeL2);
 }
 
 cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents)

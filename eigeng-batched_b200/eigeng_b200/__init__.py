@@ -91,6 +91,10 @@ def lib():
             f = getattr(L, "eigen_GPU_batch_symfunc_" + s_)
             f.argtypes = [I, I, I, P, P, P, I, ctypes.c_double, P]
             f.restype = I
+        for s_ in ("DP", "FP"):
+            f = getattr(L, "eigen_GPU_batch_launch_params_" + s_)
+            f.argtypes = [I, I] + [ctypes.POINTER(I)] * 6
+            f.restype = I
         L.eigen_GPU_batch_noalloc_DP.argtypes = [I, I, I, I, P, P, P, P]
         L.eigen_GPU_batch_noalloc_DP.restype = I
         L.eigen_GPU_batch_trace.argtypes = [P, I]
@@ -146,6 +150,7 @@ def exported_symbols():
         "eigen_GPU_check_DP", "eigen_GPU_check_FP",
         "eigen_GPU_check_ex_DP", "eigen_GPU_check_ex_FP",
         "eigen_GPU_batch_trace", "eigen_GPU_batch_noalloc_DP",
+        "eigen_GPU_batch_launch_params_DP", "eigen_GPU_batch_launch_params_FP",
         "eigen_GPU_batch_symfunc_DP", "eigen_GPU_batch_symfunc_FP",
         "eigen_GPU_batch_packed_DP", "eigen_GPU_batch_packed_FP",
         "eigen_GPU_batch_uneven_DP", "eigen_GPU_batch_uneven_FP",
@@ -195,6 +200,17 @@ def buffer_size(L, nm, n, m=None, dtype=torch.float64, rec_cap=0, method=TQL2, c
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_BufferSize failed with cudaError {st}")
     return out.value
+
+
+def launch_params(L, n, dtype=torch.float64):
+    """eigen_GPU_batch_get_Launch_params<T>: the reduction phase's launch
+    geometry on the current device, as a dict (grpSZ, numTB, numGR, numTH,
+    sizeSH, sizeL2)."""
+    v = [ctypes.c_int(0) for _ in range(6)]
+    st = getattr(lib(), "eigen_GPU_batch_launch_params_" + _sfx(dtype))(L, n, *[ctypes.byref(x) for x in v])
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_launch_params failed with cudaError {st}")
+    return dict(zip(("grpSZ", "numTB", "numGR", "numTH", "sizeSH", "sizeL2"), (x.value for x in v)))
 
 
 def query_lwork(L, nm, n, m=None, dtype=torch.float64):
@@ -368,7 +384,7 @@ def symfunc(v, w, n, func=FUNC_POW, p=0.5, nm=None, z=None, stream=None):
 
 
 def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True, max_sweep=100,
-               stream=None, device=None, z_host=None):
+               stream=None, device=None, z_host=None, info_host=None):
     """Solves a batch held in host memory (pinned for the copies to be
     asynchronous): eigenvectors overwrite ``a_host`` (or go to ``z_host``,
     same shape, leaving ``a_host`` intact), eigenvalues go to ``w_host``
@@ -381,7 +397,11 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
     already queued on ``stream`` (default: the current stream) and
     ``stream`` waits for all of it, so events recorded there bracket the
     whole transfer and solve.  Results equal eigen_GPU_batch_ex's on the
-    same matrices."""
+    same matrices.  ``info_host`` (optional host int32 tensor of L entries,
+    pinned for an asynchronous copy) receives each matrix's status as
+    eigen_GPU_batch_ex reports it: 0, or the index at which QL exceeded
+    max_sweep (NaN or Inf input shows up there too); read it after the
+    caller's stream has completed."""
     nm = n if nm is None else nm
     if a_host.is_cuda or not a_host.is_contiguous() or a_host.numel() % (nm * n):
         raise EigenGError("a_host must be a contiguous host tensor of L*nm*n elements")
@@ -421,7 +441,12 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
     # against 20.8 with four, 21.1 with two, 21.3 automatic; one chunk
     # alone keeps the automatic choice)
     ql_mpw = 8 if nrun > 1 else 0
-    info = [torch.zeros(C, dtype=torch.int32, device=dev) for _ in range(nrun)]
+    if info_host is not None and (info_host.is_cuda or info_host.numel() != L or info_host.dtype != torch.int32):
+        raise EigenGError("info_host must be a host int32 tensor of L entries")
+    # per-matrix status, one buffer per device buffer: reused, like the
+    # buffer itself, only after its copy-out (the chain s_in -> solve waits
+    # for freed[b])
+    info = [torch.zeros(C, dtype=torch.int32, device=dev) for _ in range(nbuf)]
     wk = [workspace(C, nm, n, dt, dev) if method != JACOBI else None for _ in range(nrun)]
     s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     s_runs = [torch.cuda.Stream(dev) for _ in range(nrun)]
@@ -442,7 +467,7 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
         loaded.record(s_in)
         s_run = s_runs[i % nrun]
         s_run.wait_event(loaded)
-        st = eigen_GPU_batch_ex(da[b][:cnt], dw[b][:cnt], wk[i % nrun], n, nm, n, info[i % nrun][:cnt], method,
+        st = eigen_GPU_batch_ex(da[b][:cnt], dw[b][:cnt], wk[i % nrun], n, nm, n, info[b][:cnt], method,
                                 sort, max_sweep, s_run, ql_mpw=ql_mpw)
         if st != 0:
             raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
@@ -452,6 +477,8 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
         with torch.cuda.stream(s_out):
             z_host[c0:c1].copy_(da[b][:cnt], non_blocking=True)
             w_host[c0:c1].copy_(dw[b][:cnt], non_blocking=True)
+            if info_host is not None:
+                info_host[c0:c1].copy_(info[b][:cnt], non_blocking=True)
         freed[b] = torch.cuda.Event()
         freed[b].record(s_out)
     done = torch.cuda.Event()

@@ -156,6 +156,10 @@ cudaError_t eigen_GPU_batch_stage_FP(const int L, const int nm, const int n, con
  * Limits and behaviour:
  *  - the first call on a device looks the array's address up
  *    (cudaGetSymbolAddress); make that first call before any stream capture;
+ *    the address is then cached per device for the life of the process and
+ *    stays valid only while that device's primary context lives -- after a
+ *    cudaDeviceReset the next call would use a stale address, so do not call
+ *    it after resetting a device;
  *  - every call uses the same array: calls that may overlap on the GPU
  *    (different streams, or different host threads without ordering) race
  *    and corrupt each other's results -- serialize them;
@@ -218,6 +222,10 @@ cudaError_t eigen_GPU_batch_interleaved_FP(const int L, const int n, const float
  * caller's stream waits for all of it.  Results equal eigen_GPU_batch_ex_*
  * on each matrix.  Options as eigen_GPU_batch_ex_* (chunk is chosen per
  * group); lwork from eigen_GPU_batch_uneven_BufferSize_*.
+ * Limits: the index lists are copied from pageable host memory, so a call
+ * cannot be captured in a CUDA graph; the group streams are a pool per
+ * device shared by every caller of the library, so concurrent uneven calls
+ * (from other streams or host threads) serialize on them.
  */
 cudaError_t eigen_GPU_batch_uneven_BufferSize_DP(const int L, const int *n, const eigen_GPU_batch_opts *opts,
                                                  size_t *lwork);
@@ -250,6 +258,22 @@ cudaError_t eigen_GPU_batch_symfunc_FP(const int L, const int nm, const int n, c
                                        float *z, const int func, const double p, const cudaStream_t stream);
 
 /*
+ * Launch geometry of the reduction phase (phase 1, the matrix-parallel
+ * kernel) of a default solve of L matrices of order n on the current
+ * device, for the first chunk of the batch; counterpart of the reference's
+ * header-only eigen_GPU_batch_get_Launch_params (eigen_GPU_batch.hpp:23-102),
+ * which include/eigen_GPU_batch.hpp forwards here.  grpSZ: threads that own
+ * one matrix; numGR: matrices per thread block; numTH: threads per block;
+ * numTB: thread blocks of the launch; sizeSH: dynamic shared memory bytes
+ * per block; sizeL2: the device's L2 bytes.  cudaErrorInvalidValue for
+ * L < 1, n < 1 or n > 1024.
+ */
+cudaError_t eigen_GPU_batch_launch_params_DP(const int L, const int n, int *grpSZ, int *numTB, int *numGR,
+                                             int *numTH, int *sizeSH, int *sizeL2);
+cudaError_t eigen_GPU_batch_launch_params_FP(const int L, const int n, int *grpSZ, int *numTB, int *numGR,
+                                             int *numTH, int *sizeSH, int *sizeL2);
+
+/*
  * Phase timing (counterpart of the reference's compile-time TIMER,
  * eigen_GPU_batch.cu:157-244, which prints per-phase times from warp 0).
  * When set, every later solve on the calling process records, for chunk c
@@ -257,7 +281,9 @@ cudaError_t eigen_GPU_batch_symfunc_FP(const int L, const int nm, const int n, c
  * events[4c+1] after it, events[4c+2] after phase 2 (QL) and events[4c+3]
  * after phase 3 (rotation apply + sort), on the call's stream, for the
  * chunks whose four events fit in nevents.  events == NULL turns it off.
- * The events are created and owned by the caller.
+ * The events are created and owned by the caller.  The setting is global
+ * to the process: while it is on, every solve from any host thread or
+ * stream records into the same events, so trace one solve at a time.
  */
 cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents);
 

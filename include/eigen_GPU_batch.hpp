@@ -17,39 +17,24 @@
 #include "eigen_GPU_batch.h"
 
 /*
- * Launch geometry of the solver's matrix-parallel phases on the current
- * device (reference: eigen_GPU_batch.hpp:23-102).  grpSZ: threads that own
- * one matrix (a warp for n <= 32, a CTA of ceil(n/32)*32 threads above);
- * numGR: matrices per thread block; numTH: threads per block; numTB: blocks
- * per launch; sizeSH: 0 (dynamic shared memory is sized internally);
- * sizeL2: the device's L2 size.
+ * Launch geometry of the solver's matrix-parallel reduction phase on the
+ * current device (reference: eigen_GPU_batch.hpp:23-102), exactly as the
+ * library launches it: grpSZ threads own one matrix (a warp for n <= 32,
+ * a CTA of 32*NB*NB threads for the register form at 32 < n <= 128, NB =
+ * ceil(n/32), else the CTA form), numGR matrices per block of numTH
+ * threads, numTB blocks for the first chunk of the batch, sizeSH bytes of
+ * dynamic shared memory per block, sizeL2 the device's L2 size.
  */
 template <class T>
 cudaError_t eigen_GPU_batch_get_Launch_params(const int L, const int n, int &grpSZ_, int &numTB_, int &numGR_,
                                               int &numTH_, int &sizeSH_, int &sizeL2_)
 {
+  if (std::is_same<T, double>::value)
+    return eigen_GPU_batch_launch_params_DP(L, n, &grpSZ_, &numTB_, &numGR_, &numTH_, &sizeSH_, &sizeL2_);
+  if (std::is_same<T, float>::value)
+    return eigen_GPU_batch_launch_params_FP(L, n, &grpSZ_, &numTB_, &numGR_, &numTH_, &sizeSH_, &sizeL2_);
   grpSZ_ = numTB_ = numGR_ = numTH_ = sizeSH_ = sizeL2_ = 0;
-  if (L < 1 || n < 1) return cudaErrorInvalidValue;
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
-  if (err != cudaSuccess) return err;
-  int l2 = 0;
-  err = cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
-  if (err != cudaSuccess) return err;
-  if (n <= 32) {
-    grpSZ_ = 32;
-    numGR_ = 4;
-    numTH_ = 128;
-    numTB_ = (L + 3) / 4;
-  } else {
-    grpSZ_ = std::min(1024, ((n + 31) / 32) * 32);
-    numGR_ = 1;
-    numTH_ = grpSZ_;
-    numTB_ = L;
-  }
-  sizeSH_ = 0;
-  sizeL2_ = l2;
-  return cudaSuccess;
+  return cudaErrorInvalidValue;
 }
 
 /* Workspace size in bytes (reference: eigen_GPU_batch.hpp:104-118). */

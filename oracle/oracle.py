@@ -18,6 +18,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
+_LIBS = {}
 
 METHOD_TQL2, METHOD_IMTQL2, METHOD_JACOBI = 0, 1, 2
 
@@ -26,29 +27,41 @@ def build():
     subprocess.check_call(["make", "-s", "-C", _HERE])
 
 
-def lib():
+def lib(fast=False):
+    """The parity build (liboracle.so), or with fast=True the timed CPU
+    baseline build (liboracle_fast.so, -O3 -march=native), compiled here
+    for this machine's CPU on first use."""
     global _LIB
+    if fast:
+        if "fast" not in _LIBS:
+            subprocess.check_call(["make", "-s", "-C", _HERE, "fast"])
+            _LIBS["fast"] = _load(os.path.join(_HERE, "liboracle_fast.so"))
+        return _LIBS["fast"]
     if _LIB is None:
         path = os.path.join(_HERE, "liboracle.so")
         if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(path)
-        P = ctypes.c_void_p
-        I = ctypes.c_int
-        for sfx in ("_d", "_f"):
-            getattr(L, "oracle_eigen_batch" + sfx).argtypes = [I, I, I, I, P, P, I, I, I, P, I]
-            getattr(L, "oracle_eigen_batch" + sfx).restype = ctypes.c_long
-            getattr(L, "oracle_check" + sfx).argtypes = [I, I, I, I, P, P, P, P, P, P]
-            getattr(L, "oracle_set_mat" + sfx).argtypes = [P, I, I, I, I]
-            getattr(L, "oracle_tred1" + sfx).argtypes = [I, I, P, P, P]
-            getattr(L, "oracle_tql2" + sfx).argtypes = [I, I, P, P, P, I, P]
-            getattr(L, "oracle_tql2" + sfx).restype = I
-            getattr(L, "oracle_imtql2" + sfx).argtypes = [I, I, P, P, P, I, P]
-            getattr(L, "oracle_imtql2" + sfx).restype = I
-            getattr(L, "oracle_select_sort" + sfx).argtypes = [I, P, P]
-        L.oracle_num_threads.restype = I
-        _LIB = L
+        _LIB = _load(path)
     return _LIB
+
+
+def _load(path):
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    I = ctypes.c_int
+    for sfx in ("_d", "_f"):
+        getattr(L, "oracle_eigen_batch" + sfx).argtypes = [I, I, I, I, P, P, I, I, I, P, I]
+        getattr(L, "oracle_eigen_batch" + sfx).restype = ctypes.c_long
+        getattr(L, "oracle_check" + sfx).argtypes = [I, I, I, I, P, P, P, P, P, P]
+        getattr(L, "oracle_set_mat" + sfx).argtypes = [P, I, I, I, I]
+        getattr(L, "oracle_tred1" + sfx).argtypes = [I, I, P, P, P]
+        getattr(L, "oracle_tql2" + sfx).argtypes = [I, I, P, P, P, I, P]
+        getattr(L, "oracle_tql2" + sfx).restype = I
+        getattr(L, "oracle_imtql2" + sfx).argtypes = [I, I, P, P, P, I, P]
+        getattr(L, "oracle_imtql2" + sfx).restype = I
+        getattr(L, "oracle_select_sort" + sfx).argtypes = [I, P, P]
+    L.oracle_num_threads.restype = I
+    return L
 
 
 def _sfx(dtype):
@@ -64,7 +77,7 @@ def _ptr(x):
     return ctypes.c_void_p(x.ctypes.data)
 
 
-def eigen_batch(a, n, nm=None, method=METHOD_TQL2, sort=True, max_sweep=100, nthreads=0):
+def eigen_batch(a, n, nm=None, method=METHOD_TQL2, sort=True, max_sweep=100, nthreads=0, fast=False):
     """Solve a batch in place on the CPU.
 
     ``a``: contiguous array of L column-major nm x n matrices (shape (L, n, nm)
@@ -76,7 +89,7 @@ def eigen_batch(a, n, nm=None, method=METHOD_TQL2, sort=True, max_sweep=100, nth
     L = a.size // (nm * n)
     w = np.zeros((L, n), dtype=a.dtype)
     info = np.zeros(L, dtype=np.int32)
-    f = getattr(lib(), "oracle_eigen_batch" + _sfx(a.dtype))
+    f = getattr(lib(fast), "oracle_eigen_batch" + _sfx(a.dtype))
     rots = f(L, nm, n, n, _ptr(a), _ptr(w), method, int(bool(sort)), max_sweep, _ptr(info), nthreads)
     return w, info, rots
 
@@ -163,6 +176,38 @@ def clustered_spectrum(L, n, seed, dtype=np.float64, cluster=8, sep=1e-8, gap=1e
     a = np.einsum("lij,j,lkj->lik", q, lam, q)
     a = 0.5 * (a + a.transpose(0, 2, 1))
     return np.ascontiguousarray(a.astype(dtype))
+
+
+THETA_DIM = 4
+
+
+def theta_family_basis(n=64, family_seed=2024):
+    """The fixed members of the parameterised family A(theta) = A0 +
+    sum_j theta_j E_j (j = 1..4): A0 = (G + G^T)/sqrt(2n), G iid N(0,1)
+    (a Wigner matrix, spectrum close to [-2, 2]); E_j = (H_j + H_j^T)
+    scaled to unit Frobenius norm, H_j iid N(0,1).  Returns (A0, E) with
+    E of shape (4, n, n), all float64 and symmetric."""
+    rng = np.random.default_rng(family_seed)
+    g = rng.standard_normal((n, n))
+    a0 = (g + g.T) / np.sqrt(2.0 * n)
+    e = np.empty((THETA_DIM, n, n))
+    for j in range(THETA_DIM):
+        h = rng.standard_normal((n, n))
+        h = h + h.T
+        e[j] = h / np.linalg.norm(h)
+    return a0, e
+
+
+def theta_family(L, n=64, seed=0, dtype=np.float32, family_seed=2024, return_theta=False):
+    """L matrices A(theta) = A0 + sum_j theta_j E_j, theta iid U[-0.1, 0.1]^4
+    (A0, E_j from theta_family_basis).  (L, n, n) C-order holding the
+    symmetric matrices; with return_theta also the (L, 4) parameters."""
+    a0, e = theta_family_basis(n, family_seed)
+    rng = np.random.default_rng(seed)
+    th = rng.uniform(-0.1, 0.1, size=(L, THETA_DIM))
+    a = a0[None] + np.einsum("lj,jik->lik", th, e)
+    a = np.ascontiguousarray(a.astype(dtype))
+    return (a, th) if return_theta else a
 
 
 def frank(L, n, dtype=np.float64):

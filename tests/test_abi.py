@@ -54,3 +54,62 @@ def test_cpp_header_compiles():
         cmd = ["/usr/bin/g++", "-std=c++14", "-fsyntax-only", "-I" + os.path.join(ROOT, "include"),
                "-I/usr/local/cuda/include", f]
         subprocess.check_call(cmd)
+
+
+def _cpp_launch_params_program(td):
+    src = ('#include <stdio.h>\n#include "eigen_GPU_batch.hpp"\n'
+           "int main(){ const int ns[] = {1, 5, 32, 33, 64, 96, 128, 129, 200, 256, 512, 1024};\n"
+           " for (int i = 0; i < 12; i++) { int g,b,r,t,s,l;\n"
+           "  if (eigen_GPU_batch_get_Launch_params<double>(4096, ns[i], g, b, r, t, s, l) != cudaSuccess) return 1;\n"
+           "  printf(\"%d %d %d %d %d %d %d\\n\", ns[i], g, b, r, t, s, l); }\n"
+           " int g,b,r,t,s,l; return eigen_GPU_batch_get_Launch_params<double>(0, 8, g, b, r, t, s, l) == cudaSuccess;}\n")
+    f = os.path.join(td, "lp.cpp")
+    open(f, "w").write(src)
+    exe = os.path.join(td, "lp")
+    import subprocess
+    subprocess.check_call(["/usr/bin/g++", "-std=c++14", "-I" + os.path.join(ROOT, "include"),
+                           "-I/usr/local/cuda/include", f, "-o", exe, "-L" + os.path.dirname(LIB),
+                           "-Wl,-rpath," + os.path.dirname(LIB), "-leigenGbatch", "-L/usr/local/cuda/lib64",
+                           "-lcudart"])
+    return exe
+
+
+def test_cpp_launch_params_program_builds(tmp_path):
+    """The C++ template links against the library (its geometry query is an
+    exported C function)."""
+    _cpp_launch_params_program(str(tmp_path))
+
+
+import pytest  # noqa: E402
+
+
+@pytest.mark.gpu
+def test_launch_params_report_the_launched_geometry(tmp_path):
+    """eigen_GPU_batch_get_Launch_params<T> reports phase 1 as run() launches
+    it: one thread per matrix for n = 1, a warp per matrix (four per block)
+    for n <= 32, a CTA of 32*NB*NB threads (NB = ceil(n/32)) in the
+    register form for 32 < n <= 128, and the CTA form's
+    min(1024, ceil(n/32)*32*split) threads above (split 4 up to n = 256, 2
+    up to 512, then 1), one block per matrix."""
+    import subprocess
+    out = subprocess.check_output([_cpp_launch_params_program(str(tmp_path))], text=True)
+    rows = {int(x.split()[0]): [int(v) for v in x.split()[1:]] for x in out.strip().splitlines()}
+    import math
+    for n, (g, b, r, t, s, l) in rows.items():
+        assert l > 0
+        if n == 1:
+            assert (g, b, r, t) == (1, 16, 256, 256)
+        elif n <= 32:
+            assert (g, b, r, t) == (32, 1024, 4, 128)
+            assert s > 0
+        elif n <= 128:
+            nb = math.ceil(n / 32)
+            assert (g, r, t) == (32 * nb * nb, 1, 32 * nb * nb), n
+            assert 0 < b <= 4096
+        else:
+            split = 4 if n <= 256 else (2 if n <= 512 else 1)
+            th = min(1024, math.ceil(n / 32) * 32 * split)
+            assert (g, r, t) == (th, 1, th), n
+            assert 0 < b <= 4096
+    import eigeng_b200 as E
+    assert E.launch_params(4096, 128)["numTH"] == rows[128][3]

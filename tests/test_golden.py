@@ -83,3 +83,57 @@ def test_cuda_library_matches_reference_gpu_build(fixtures):
         torch.cuda.synchronize()
         assert (info.cpu().numpy() == 0).all(), key
         _check_against(fixtures[key + "__w"], fixtures[key + "__z"], w.cpu().numpy(), a.cpu().numpy(), n, a0.dtype)
+
+
+# ---------------------------------------------------------------------------
+# The "ext" set: the reference's USE_IMTQL 1 build (imtql2 + DO_SORT) at
+# n = 3 .. 256, and its default build at n = 256 (the warp-per-matrix
+# hhsy2tr_ / tql2_ / hhtr2sy_ path, eigen_GPU_batch.cu:138-245).
+
+FIX_EXT = os.path.join(HERE, "golden", "ref_gpu_golden_ext.npz")
+EXT = None
+
+
+def ext_cases():
+    global EXT
+    if EXT is None:
+        EXT = list(_mk().ext_cases())
+    return EXT
+
+
+@pytest.fixture(scope="module")
+def fixtures_ext():
+    if not os.path.exists(FIX_EXT):
+        pytest.skip("ref_gpu_golden_ext.npz not generated (tests/golden/make_ref_golden.py ext, on a GPU)")
+    return np.load(FIX_EXT)
+
+
+def test_ext_fixture_inputs_regenerate_exactly(fixtures_ext):
+    m = _mk()
+    for key, n, a0, _ in ext_cases():
+        assert str(fixtures_ext[key + "__sha"]) == m.sha(a0), key
+
+
+@pytest.mark.parametrize("idx", range(52))
+def test_oracle_matches_reference_ext(oracle_mod, fixtures_ext, idx):
+    key, n, a0, meth = ext_cases()[idx]
+    O = oracle_mod
+    a = a0.copy()
+    w, info, _ = O.eigen_batch(a, n, method=O.METHOD_IMTQL2 if meth == "imtql2" else O.METHOD_TQL2)
+    assert (info == 0).all()
+    _check_against(fixtures_ext[key + "__w"], fixtures_ext[key + "__z"], w, a, n, a0.dtype)
+    e1, e2, fl = O.check(a0, fixtures_ext[key + "__w"], fixtures_ext[key + "__z"], n)
+    assert (fl == 0).all(), (key, e1, e2)
+
+
+@pytest.mark.gpu
+def test_cuda_library_matches_reference_ext(fixtures_ext):
+    import torch
+    import eigeng_b200 as E
+    for key, n, a0, meth in ext_cases():
+        a = torch.from_numpy(a0.copy()).cuda()
+        w, info = E.solve(a, n, method=E.IMTQL2 if meth == "imtql2" else E.TQL2)
+        torch.cuda.synchronize()
+        assert (info.cpu().numpy() == 0).all(), key
+        _check_against(fixtures_ext[key + "__w"], fixtures_ext[key + "__z"], w.cpu().numpy(), a.cpu().numpy(), n,
+                       a0.dtype)

@@ -398,6 +398,29 @@ def test_solve_host_matches_device_solve(oracle_mod):
     assert np.array_equal(wf.numpy(), w2)
 
 
+@pytest.mark.parametrize("n,L,chunk", [(48, 37, 5), (16, 4096, 0)])
+def test_solve_host_buffer_reuse_and_status(oracle_mod, n, L, chunk):
+    """More chunks than the four device buffers (each buffer, and its
+    status buffer, reused after its copy-out), and the default six-chunk
+    schedule of a batch of 2048 or more with the QL phase at eight matrices
+    per warp: bit for bit the device solve, status copied back per matrix.
+    One matrix carries a NaN, which QL reports in its status."""
+    O = oracle_mod
+    a0 = O.sym_uniform(L, n, seed=23)
+    bad = L // 3
+    a0[bad, 1, 0] = a0[bad, 0, 1] = np.nan
+    w1, z1, i1 = gpu_solve(a0, n)
+    ah = torch.from_numpy(a0.copy()).pin_memory()
+    ih = torch.full((L,), -5, dtype=torch.int32).pin_memory()
+    wh = E().solve_host(ah, n, chunk=chunk, info_host=ih)
+    torch.cuda.synchronize()
+    ok = np.arange(L) != bad
+    assert np.array_equal(ih.numpy(), i1)
+    assert i1[bad] != 0 and (i1[ok] == 0).all()
+    assert np.array_equal(wh.numpy()[ok], w1[ok])
+    assert np.array_equal(ah.numpy()[ok], z1[ok])
+
+
 def _stage_parts(a0, n, nm, dtype, method):
     """Solves a0 with eigen_GPU_batch_stage_*: the reductions in two parts on
     two streams, the QL phase over the whole batch, the apply phase in three

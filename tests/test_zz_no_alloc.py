@@ -62,6 +62,24 @@ def test_noalloc_matches_regular_entry_point_twice():
         _close(_regular(a0, n), _noalloc(a0, n), n)
 
 
+def test_noalloc_largest_matrix_fits():
+    """One matrix of the largest supported order, n = 1024, fits the static
+    workspace on its own (two calls of one matrix each, then one of two,
+    which the library runs one matrix per piece): results match the
+    regular entry point and FP64 LAPACK."""
+    from scipy.linalg import lapack
+    n = 1024
+    a0 = _inputs(2, n, 5)
+    ref = _regular(a0, n)
+    for k in range(2):
+        got = _noalloc(a0[k:k + 1], n)
+        _close(tuple(x[k:k + 1] for x in ref), got, n)
+    _close(ref, _noalloc(a0, n), n)
+    wl, _, inf = lapack.dsyev(np.asfortranarray(a0[0].T), compute_v=0)
+    assert inf == 0
+    assert np.abs(ref[0][0] - wl).max() <= 64 * n * np.finfo(np.float64).eps * np.abs(wl).max()
+
+
 def test_noalloc_rejects_sizes_beyond_limit():
     import eigeng_b200 as E
     a = torch.zeros((1, 4, 4), dtype=torch.float64, device="cuda")
