@@ -21,6 +21,7 @@
 
 #include "eigb_kernels.cuh"
 #include "eigb_symfunc.cuh"
+#include "eigb_refine.cuh"
 #include "../../include/eigen_GPU_batch.h"
 
 namespace eigb {
@@ -875,6 +876,450 @@ cudaError_t run_noalloc(long L, int nm, int n, int m, T *a, T *w, int *info, cud
   return run<T>(L, nm, n, m, a, w, scratch, kNoallocScratchBytes, info, &o, stream);
 }
 
+// ---- mixed precision with refinement (eigb_refine.cuh) ----
+//
+// Workspace: one chunk of Lc matrices (the FP32 solve and its workspace,
+// the FP64 matrices of the refinement, the slices of the tensor-core
+// products and the per-matrix state), then a batch-wide tail (the
+// fallback's index list and offsets, counters).  The fallback's plain FP64
+// solve reuses the chunk area.
+struct RefLayout {
+  long Lc = 0;
+  int n = 0, Rp = 0, Kp = 0, KB = 0;
+  size_t a32 = 0, w32 = 0, i32 = 0, ws32 = 0, ws32_bytes = 0;
+  size_t af = 0, x0 = 0, x1 = 0, pe = 0, sm = 0, gm = 0;
+  size_t as = 0, xs = 0, ps = 0, xr = 0, es = 0;
+  size_t ea = 0, ex = 0, ep = 0, exr = 0, ee = 0;
+  size_t lam = 0, sig = 0, act0 = 0, act1 = 0, conv = 0, fail = 0, emax = 0, ord = 0, cl = 0, W = 0;
+  size_t chunk_bytes = 0;
+  size_t fb = 0, aoff = 0, woff = 0, cnt = 0, bytes = 0;
+};
+
+constexpr int REF_S = 8;                   // slices of the FP64-accurate products
+constexpr int REF_SX = 5, REF_SE = 4;      // slices of X and E in X E
+constexpr int REF_DMAX = 9, REF_DMAX_XE = 8;
+
+struct RefOpts {
+  int max_iter = 3;
+  double tol = 1e-7;
+  int fallback = 1;
+  int chunk = 0;
+};
+
+inline RefOpts ref_opts(const eigen_GPU_refine_opts *o)
+{
+  RefOpts r;
+  if (o) {
+    if (o->max_iter > 0) r.max_iter = o->max_iter;
+    if (o->tol > 0) r.tol = o->tol;
+    r.fallback = o->fallback ? 1 : 0;
+    r.chunk = o->chunk;
+  }
+  return r;
+}
+
+inline eigen_GPU_batch_opts ref_opts32(long Lc)
+{
+  eigen_GPU_batch_opts o{};
+  o.method = EIGEN_GPU_BATCH_TQL2;
+  o.sort = 1;
+  o.max_sweep = 100;
+  o.chunk = (int)Lc;
+  return o;
+}
+
+inline size_t ref_chunk_layout(long Lc, int nm, int n, const DevProps &dp, RefLayout &ly)
+{
+  ly.Lc = Lc;
+  ly.n = n;
+  ly.Rp = oz_rp(n);
+  ly.Kp = oz_kp(n);
+  ly.KB = oz_kb(n);
+  const size_t nn = (size_t)n * n, sl = oz_slice_bytes(n), rp = (size_t)ly.Rp;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = align256(o + bytes);
+    return at;
+  };
+  ly.a32 = take(sizeof(float) * nn * Lc);
+  ly.w32 = take(sizeof(float) * n * Lc);
+  ly.i32 = take(sizeof(int) * Lc);
+  Plan<float> pf;
+  eigen_GPU_batch_opts o32 = ref_opts32(Lc);
+  if (make_plan<float>(Lc, n, n, dp, pf, &o32) != cudaSuccess) return 0;
+  ly.ws32_bytes = pf.bytes;
+  ly.ws32 = take(pf.bytes);
+  ly.af = take(sizeof(double) * nn * Lc);
+  ly.x0 = take(sizeof(double) * nn * Lc);
+  ly.x1 = take(sizeof(double) * nn * Lc);
+  ly.pe = take(sizeof(double) * nn * Lc);
+  ly.sm = take(sizeof(double) * nn * Lc);
+  ly.gm = take(sizeof(double) * nn * Lc);
+  ly.as = take(sl * REF_S * Lc);
+  ly.xs = take(sl * REF_S * Lc);
+  ly.ps = take(sl * REF_S * Lc);
+  ly.xr = take(sl * REF_SX * Lc);
+  ly.es = take(sl * REF_SE * Lc);
+  ly.ea = take(sizeof(int) * rp * Lc);
+  ly.ex = take(sizeof(int) * rp * Lc);
+  ly.ep = take(sizeof(int) * rp * Lc);
+  ly.exr = take(sizeof(int) * rp * Lc);
+  ly.ee = take(sizeof(int) * rp * Lc);
+  ly.lam = take(sizeof(double) * n * Lc);
+  ly.sig = take(sizeof(double) * Lc);
+  ly.act0 = take(sizeof(int) * Lc);
+  ly.act1 = take(sizeof(int) * Lc);
+  ly.conv = take(sizeof(int) * Lc);
+  ly.fail = take(sizeof(int) * Lc);
+  ly.emax = take(sizeof(double) * Lc);
+  ly.ord = take(sizeof(int) * n * Lc);
+  ly.cl = take(sizeof(int) * n * Lc);
+  ly.W = take(sizeof(double) * (size_t)n * REF_CL_MAX * Lc);
+  // the fallback's plain FP64 solve of up to Lc matrices reuses the area
+  Plan<double> pd;
+  eigen_GPU_batch_opts o64{};
+  o64.chunk = (int)Lc;
+  if (make_plan<double>(Lc, nm, n, dp, pd, &o64) != cudaSuccess) return 0;
+  return std::max(o, pd.bytes);
+}
+
+inline cudaError_t ref_plan(long L, int nm, int n, const DevProps &dp, const RefOpts &ro, RefLayout &ly)
+{
+  long Lc = ro.chunk > 0 ? std::min<long>(L, ro.chunk) : L;
+  size_t cb = 0;
+  for (;;) {
+    cb = ref_chunk_layout(Lc, nm, n, dp, ly);
+    if (cb == 0) return cudaErrorInvalidValue;
+    if (ro.chunk > 0 || cb <= kWsBudget || Lc <= 64) break;
+    Lc = std::max<long>(64, (long)((double)Lc * (double)kWsBudget / (double)cb * 0.98));
+    const long nch = (L + Lc - 1) / Lc;  // equal chunks
+    Lc = (L + nch - 1) / nch;
+  }
+  ly.chunk_bytes = align256(cb);
+  size_t o = ly.chunk_bytes;
+  ly.fb = o;
+  o = align256(o + sizeof(int) * L);
+  ly.aoff = o;
+  o = align256(o + sizeof(long long) * L);
+  ly.woff = o;
+  o = align256(o + sizeof(long long) * L);
+  ly.cnt = o;  // fallback count, then the products' error flag
+  o = align256(o + 2 * sizeof(int));
+  ly.bytes = o;
+  return cudaSuccess;
+}
+
+inline bool ref_bad_args(long L, int nm, int n) { return L < 1 || nm < n || n < 1 || n > 256; }
+
+cudaError_t ref_buffer_size(long L, int nm, int n, const eigen_GPU_refine_opts *opts, size_t *lwork)
+{
+  if (lwork == nullptr) return cudaErrorInvalidValue;
+  *lwork = 0;
+  if (ref_bad_args(L, nm, n)) return cudaErrorInvalidValue;
+  if (n == 1) return cudaSuccess;
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  RefLayout ly;
+  if ((err = ref_plan(L, nm, n, dp, ref_opts(opts), ly)) != cudaSuccess) return err;
+  *lwork = ly.bytes;
+  return cudaSuccess;
+}
+
+// one product of the refinement
+inline void ref_gemm(const RefLayout &ly, long lc, const int8_t *Ls, const int *eL, int sL, const int8_t *Rs,
+                     const int *eR, int sR, int dmax, double *out, const void *add, int add_f32, const int *act,
+                     int *errf, size_t smem, cudaStream_t st)
+{
+  OzGemm g{};
+  g.Ls = Ls;
+  g.Rs = Rs;
+  g.eL = eL;
+  g.eR = eR;
+  g.RpL = g.RpR = ly.Rp;
+  g.Kp = ly.Kp;
+  g.KB = ly.KB;
+  g.sL = sL;
+  g.sR = sR;
+  g.dmax = dmax;
+  g.n = ly.n;
+  g.mtiles = ly.Rp / OZ_MT;
+  g.ntiles = (ly.n + OZ_NT - 1) / OZ_NT;
+  g.out = out;
+  g.ob = (long long)ly.n * ly.n;
+  g.ldo = ly.n;
+  g.add = add;
+  g.add_f32 = add_f32;
+  g.ab = (long long)ly.n * ly.n;
+  g.lda = ly.n;
+  g.active = act;
+  g.err = errf;
+  const long tiles = lc * g.mtiles * g.ntiles;
+  k_oz_gemm<<<(unsigned)tiles, OZ_THREADS, smem, st>>>(g);
+}
+
+inline void ref_slice(const RefLayout &ly, long lc, const void *src, int f32, int rs, int ks, int s, int8_t *out,
+                      int *e, const int *act, cudaStream_t st)
+{
+  OzSlice q{};
+  q.src = src;
+  q.src_f32 = f32;
+  q.bs = (long long)ly.n * ly.n;
+  q.rs = rs;
+  q.ks = ks;
+  q.R = ly.n;
+  q.K = ly.n;
+  q.Rp = ly.Rp;
+  q.Kp = ly.Kp;
+  q.KB = ly.KB;
+  q.s = s;
+  q.out = out;
+  q.e = e;
+  q.active = act;
+  const int rpb = 256 / (ly.Kp / 16);
+  dim3 grid((unsigned)lc, (unsigned)((ly.Rp + rpb - 1) / rpb));
+  k_oz_slice<><<<grid, 256, 0, st>>>(q);
+}
+
+cudaError_t run_refine(long L, int nm, int n, double *a, double *w, void *wk, size_t lwork, int *info, int *iters,
+                       const eigen_GPU_refine_opts *opts, cudaStream_t stream)
+{
+  if (ref_bad_args(L, nm, n) || a == nullptr || w == nullptr) return cudaErrorInvalidValue;
+  if (n == 1) {
+    cudaError_t e1 = run<double>(L, nm, n, n, a, w, nullptr, 0, info, nullptr, stream);
+    if (e1 == cudaSuccess && iters) e1 = cudaMemsetAsync(iters, 0, sizeof(int) * L, stream);
+    return e1;
+  }
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  const RefOpts ro = ref_opts(opts);
+  RefLayout ly;
+  if ((err = ref_plan(L, nm, n, dp, ro, ly)) != cudaSuccess) return err;
+  if (wk == nullptr || (lwork != 0 && lwork < ly.bytes)) return cudaErrorInvalidValue;
+  char *base = static_cast<char *>(wk);
+  auto P = [&](size_t off) { return static_cast<void *>(base + off); };
+  int *fb_list = static_cast<int *>(P(ly.fb));
+  int *cnt = static_cast<int *>(P(ly.cnt));
+  int *errf = cnt + 1;
+  if ((err = cudaMemsetAsync(cnt, 0, 2 * sizeof(int), stream)) != cudaSuccess) return err;
+  // shared memory of the products: their operands, and at least half of
+  // the SM so that no two of these CTAs (512 TMEM columns each) share an SM
+  const size_t need = std::max(oz_gemm_smem(REF_S, REF_S, ly.KB), oz_gemm_smem(REF_SX, REF_SE, ly.KB));
+  const size_t half = (size_t)dp.smem_sm / 2 + 1024;
+  const size_t gsm = std::min<size_t>(std::max(need, half), (size_t)dp.smem_optin);
+  if (need > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
+  if ((err = set_smem(k_oz_gemm, gsm)) != cudaSuccess) return err;
+  const size_t usm = ref_update_smem(n);
+  if ((err = set_smem(k_oa_update, usm)) != cudaSuccess) return err;
+  const size_t fsm = (sizeof(double) + sizeof(int)) * (size_t)n + 64;
+  const eigen_GPU_batch_opts o32 = ref_opts32(ly.Lc);
+  float *A32 = static_cast<float *>(P(ly.a32));
+  double *Af = static_cast<double *>(P(ly.af));
+  double *XB[2] = {static_cast<double *>(P(ly.x0)), static_cast<double *>(P(ly.x1))};
+  double *PE = static_cast<double *>(P(ly.pe));
+  double *Sm = static_cast<double *>(P(ly.sm));
+  double *Gm = static_cast<double *>(P(ly.gm));
+  int8_t *AS = static_cast<int8_t *>(P(ly.as)), *XS = static_cast<int8_t *>(P(ly.xs));
+  int8_t *PS = static_cast<int8_t *>(P(ly.ps)), *XR = static_cast<int8_t *>(P(ly.xr));
+  int8_t *ES = static_cast<int8_t *>(P(ly.es));
+  int *eA = static_cast<int *>(P(ly.ea)), *eX = static_cast<int *>(P(ly.ex)), *eP = static_cast<int *>(P(ly.ep));
+  int *eXR = static_cast<int *>(P(ly.exr)), *eE = static_cast<int *>(P(ly.ee));
+  int *act[2] = {static_cast<int *>(P(ly.act0)), static_cast<int *>(P(ly.act1))};
+  int *conv = static_cast<int *>(P(ly.conv)), *fail = static_cast<int *>(P(ly.fail));
+  for (long c0 = 0; c0 < L; c0 += ly.Lc) {
+    const long lc = std::min(ly.Lc, L - c0);
+    k_ref_prep<<<(unsigned)lc, 256, 0, stream>>>(a + (size_t)c0 * nm * n, nm, n, Af, A32,
+                                                 static_cast<double *>(P(ly.sig)), 1);
+    if ((err = run<float>(lc, n, n, n, A32, static_cast<float *>(P(ly.w32)), P(ly.ws32), ly.ws32_bytes,
+                          static_cast<int *>(P(ly.i32)), &o32, stream)) != cudaSuccess)
+      return err;
+    k_ref_init<<<(unsigned)((lc + 255) / 256), 256, 0, stream>>>(lc, static_cast<int *>(P(ly.i32)), act[0], conv,
+                                                                 fail);
+    ref_slice(ly, lc, Af, 0, n, 1, REF_S, AS, eA, act[0], stream);
+    for (int it = 1; it <= ro.max_iter; it++) {
+      const int *ain = act[(it - 1) & 1];
+      int *aout = act[it & 1];
+      const void *Xs = it == 1 ? static_cast<const void *>(A32) : static_cast<const void *>(XB[it & 1]);
+      const int xf32 = it == 1 ? 1 : 0;
+      double *Xd = XB[(it - 1) & 1];
+      ref_slice(ly, lc, Xs, xf32, n, 1, REF_S, XS, eX, ain, stream);             // columns of X
+      ref_gemm(ly, lc, AS, eA, REF_S, XS, eX, REF_S, REF_DMAX, PE, nullptr, 0, ain, errf, gsm, stream);  // P = Af X
+      ref_slice(ly, lc, PE, 0, n, 1, REF_S, PS, eP, ain, stream);
+      ref_gemm(ly, lc, XS, eX, REF_S, PS, eP, REF_S, REF_DMAX, Sm, nullptr, 0, ain, errf, gsm, stream);  // S = X^T P
+      ref_gemm(ly, lc, XS, eX, REF_S, XS, eX, REF_S, REF_DMAX, Gm, nullptr, 0, ain, errf, gsm, stream);  // G = X^T X
+      RefP rp{};
+      rp.n = n;
+      rp.S = Sm;
+      rp.G = Gm;
+      rp.E = PE;
+      rp.lam = static_cast<double *>(P(ly.lam));
+      rp.order = static_cast<int *>(P(ly.ord));
+      rp.cl = static_cast<int *>(P(ly.cl));
+      rp.W = static_cast<double *>(P(ly.W));
+      rp.act_in = ain;
+      rp.act_out = aout;
+      rp.conv_it = conv;
+      rp.fail = fail;
+      rp.emax = static_cast<double *>(P(ly.emax));
+      rp.tol = ro.tol;
+      rp.it = it;
+      rp.last = it == ro.max_iter;
+      k_oa_update<<<(unsigned)lc, 256, usm, stream>>>(rp);
+      ref_slice(ly, lc, Xs, xf32, 1, n, REF_SX, XR, eXR, ain, stream);           // rows of X
+      ref_slice(ly, lc, PE, 0, n, 1, REF_SE, ES, eE, ain, stream);               // columns of E
+      ref_gemm(ly, lc, XR, eXR, REF_SX, ES, eE, REF_SE, REF_DMAX_XE, Xd, Xs, xf32, ain, errf, gsm, stream);
+      k_cluster_apply<<<(unsigned)lc, 256, 0, stream>>>(n, Xd, ain, fail, rp.order, rp.cl, rp.W);
+      if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    }
+    k_ref_final<<<(unsigned)lc, 256, fsm, stream>>>(n, nm, a, w, info, XB[0], XB[1],
+                                                     static_cast<double *>(P(ly.lam)),
+                                                     static_cast<double *>(P(ly.sig)), conv, fail, iters, fb_list,
+                                                     cnt, c0);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  }
+  // the fallback: its size is read back (one synchronisation of the stream)
+  int hc[2] = {0, 0};
+  if ((err = cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return err;
+  if ((err = cudaStreamSynchronize(stream)) != cudaSuccess) return err;
+  if (hc[1] != 0) return cudaErrorLaunchFailure;  // a product's wait gave up
+  if (hc[0] > 0) {
+    if (!ro.fallback) {
+      k_ref_mark<<<(unsigned)((hc[0] + 255) / 256), 256, 0, stream>>>(hc[0], fb_list, info);
+      return cudaGetLastError();
+    }
+    long long *aoff = static_cast<long long *>(P(ly.aoff)), *woff = static_cast<long long *>(P(ly.woff));
+    k_ref_offsets<<<(unsigned)std::min<long>((L + 255) / 256, 4096), 256, 0, stream>>>(L, nm, n, aoff, woff);
+    eigen_GPU_batch_opts o64{};
+    o64.chunk = (int)ly.Lc;
+    Indirect ix;
+    ix.kid = fb_list;
+    ix.aoff = aoff;
+    ix.woff = woff;
+    if ((err = run<double>(hc[0], nm, n, n, a, w, wk, ly.chunk_bytes, info, &o64, stream, nullptr, ix)) !=
+        cudaSuccess)
+      return err;
+  }
+  return cudaSuccess;
+}
+
+// ---- Rayleigh products S = X^T A X, G = X^T X on the int8 tensor cores ----
+struct RayLayout {
+  long Lc = 0;
+  size_t af = 0, p = 0, as = 0, xs = 0, ps = 0, ea = 0, ex = 0, ep = 0, err = 0, bytes = 0;
+};
+
+inline void ray_layout(long Lc, int n, RayLayout &ly)
+{
+  const size_t nn = (size_t)n * n, sl = oz_slice_bytes(n), rp = (size_t)oz_rp(n);
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = align256(o + bytes);
+    return at;
+  };
+  ly.Lc = Lc;
+  ly.af = take(sizeof(double) * nn * Lc);
+  ly.p = take(sizeof(double) * nn * Lc);
+  ly.as = take(sl * REF_S * Lc);
+  ly.xs = take(sl * REF_S * Lc);
+  ly.ps = take(sl * REF_S * Lc);
+  ly.ea = take(sizeof(int) * rp * Lc);
+  ly.ex = take(sizeof(int) * rp * Lc);
+  ly.ep = take(sizeof(int) * rp * Lc);
+  ly.err = take(sizeof(int));
+  ly.bytes = o;
+}
+
+inline cudaError_t ray_plan(long L, int n, RayLayout &ly)
+{
+  long Lc = L;
+  ray_layout(Lc, n, ly);
+  if (ly.bytes > kWsBudget) {
+    const size_t per = ly.bytes / (size_t)L + 1;
+    Lc = std::max<long>(1, (long)(kWsBudget / per));
+    ray_layout(Lc, n, ly);
+  }
+  return cudaSuccess;
+}
+
+cudaError_t ray_buffer_size(long L, int nm, int n, size_t *lwork)
+{
+  if (lwork == nullptr) return cudaErrorInvalidValue;
+  *lwork = 0;
+  if (ref_bad_args(L, nm, n)) return cudaErrorInvalidValue;
+  RayLayout ly;
+  ray_plan(L, n, ly);
+  *lwork = ly.bytes;
+  return cudaSuccess;
+}
+
+cudaError_t run_rayleigh(long L, int nm, int n, const double *a, const double *x, double *s, double *g, void *wk,
+                         size_t lwork, cudaStream_t stream)
+{
+  if (ref_bad_args(L, nm, n) || a == nullptr || x == nullptr || (s == nullptr && g == nullptr))
+    return cudaErrorInvalidValue;
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  RayLayout ly;
+  ray_plan(L, n, ly);
+  if (wk == nullptr || (lwork != 0 && lwork < ly.bytes)) return cudaErrorInvalidValue;
+  char *base = static_cast<char *>(wk);
+  auto P = [&](size_t off) { return static_cast<void *>(base + off); };
+  RefLayout rl;  // the slice geometry
+  rl.n = n;
+  rl.Rp = oz_rp(n);
+  rl.Kp = oz_kp(n);
+  rl.KB = oz_kb(n);
+  const size_t need = oz_gemm_smem(REF_S, REF_S, rl.KB);
+  const size_t gsm = std::min<size_t>(std::max(need, (size_t)dp.smem_sm / 2 + 1024), (size_t)dp.smem_optin);
+  if (need > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
+  if ((err = set_smem(k_oz_gemm, gsm)) != cudaSuccess) return err;
+  double *Af = static_cast<double *>(P(ly.af)), *Pm = static_cast<double *>(P(ly.p));
+  int8_t *AS = static_cast<int8_t *>(P(ly.as)), *XS = static_cast<int8_t *>(P(ly.xs)),
+         *PS = static_cast<int8_t *>(P(ly.ps));
+  int *eA = static_cast<int *>(P(ly.ea)), *eX = static_cast<int *>(P(ly.ex)), *eP = static_cast<int *>(P(ly.ep));
+  int *errf = static_cast<int *>(P(ly.err));
+  if ((err = cudaMemsetAsync(errf, 0, sizeof(int), stream)) != cudaSuccess) return err;
+  for (long c0 = 0; c0 < L; c0 += ly.Lc) {
+    const long lc = std::min(ly.Lc, L - c0);
+    k_ref_prep<<<(unsigned)lc, 256, 0, stream>>>(a + (size_t)c0 * nm * n, nm, n, Af, nullptr, nullptr, 0);
+    ref_slice(rl, lc, Af, 0, n, 1, REF_S, AS, eA, nullptr, stream);
+    // columns of X (leading dimension nm)
+    {
+      OzSlice q{};
+      q.src = x + (size_t)c0 * nm * n;
+      q.src_f32 = 0;
+      q.bs = (long long)nm * n;
+      q.rs = nm;
+      q.ks = 1;
+      q.R = n;
+      q.K = n;
+      q.Rp = rl.Rp;
+      q.Kp = rl.Kp;
+      q.KB = rl.KB;
+      q.s = REF_S;
+      q.out = XS;
+      q.e = eX;
+      const int rpb = 256 / (rl.Kp / 16);
+      k_oz_slice<><<<dim3((unsigned)lc, (unsigned)((rl.Rp + rpb - 1) / rpb)), 256, 0, stream>>>(q);
+    }
+    if (s) {
+      ref_gemm(rl, lc, AS, eA, REF_S, XS, eX, REF_S, REF_DMAX, Pm, nullptr, 0, nullptr, errf, gsm, stream);
+      ref_slice(rl, lc, Pm, 0, n, 1, REF_S, PS, eP, nullptr, stream);
+      ref_gemm(rl, lc, XS, eX, REF_S, PS, eP, REF_S, REF_DMAX, s + (size_t)c0 * n * n, nullptr, 0, nullptr, errf,
+               gsm, stream);
+    }
+    if (g)
+      ref_gemm(rl, lc, XS, eX, REF_S, XS, eX, REF_S, REF_DMAX, g + (size_t)c0 * n * n, nullptr, 0, nullptr, errf,
+               gsm, stream);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
 static_assert(EIGEN_GPU_FUNC_DIAG == SYMF_DIAG && EIGEN_GPU_FUNC_POW == SYMF_POW && EIGEN_GPU_FUNC_EXP == SYMF_EXP,
               "matrix-function codes of the header and the kernel agree");
 
@@ -1099,6 +1544,30 @@ cudaError_t eigen_GPU_batch_launch_params_FP(const int L, const int n, int *grpS
                                              int *numTH, int *sizeSH, int *sizeL2)
 {
   return eigb::launch_params<float>(L, n, grpSZ, numTB, numGR, numTH, sizeSH, sizeL2);
+}
+
+cudaError_t eigen_GPU_batch_refine_BufferSize_DP(const int L, const int nm, const int n,
+                                                const eigen_GPU_refine_opts *opts, size_t *lwork)
+{
+  return eigb::ref_buffer_size(L, nm, n, opts, lwork);
+}
+
+cudaError_t eigen_GPU_batch_refine_DP(const int L, const int nm, const int n, double *a, double *w, void *wk,
+                                      const size_t lwork, int *info, int *iters, const eigen_GPU_refine_opts *opts,
+                                      const cudaStream_t stream)
+{
+  return eigb::run_refine(L, nm, n, a, w, wk, lwork, info, iters, opts, stream);
+}
+
+cudaError_t eigen_GPU_batch_rayleigh_BufferSize_DP(const int L, const int nm, const int n, size_t *lwork)
+{
+  return eigb::ray_buffer_size(L, nm, n, lwork);
+}
+
+cudaError_t eigen_GPU_batch_rayleigh_DP(const int L, const int nm, const int n, const double *a, const double *x,
+                                        double *s, double *g, void *wk, const size_t lwork, const cudaStream_t stream)
+{
+  return eigb::run_rayleigh(L, nm, n, a, x, s, g, wk, lwork, stream);
 }
 
 cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents)

@@ -39,6 +39,12 @@ class Opts(ctypes.Structure):
                 ("zmem", ctypes.c_int), ("ql_mpw", ctypes.c_int)]
 
 
+class RefineOpts(ctypes.Structure):
+    """eigen_GPU_refine_opts of include/eigen_GPU_batch.h."""
+    _fields_ = [("max_iter", ctypes.c_int), ("tol", ctypes.c_double), ("fallback", ctypes.c_int),
+                ("chunk", ctypes.c_int)]
+
+
 def lib():
     """Load the CUDA library (raises if it has not been built)."""
     global _lib
@@ -95,6 +101,14 @@ def lib():
             f = getattr(L, "eigen_GPU_batch_launch_params_" + s_)
             f.argtypes = [I, I] + [ctypes.POINTER(I)] * 6
             f.restype = I
+        L.eigen_GPU_batch_refine_BufferSize_DP.argtypes = [I, I, I, ctypes.POINTER(RefineOpts), ctypes.POINTER(SZ)]
+        L.eigen_GPU_batch_refine_BufferSize_DP.restype = I
+        L.eigen_GPU_batch_refine_DP.argtypes = [I, I, I, P, P, P, SZ, P, P, ctypes.POINTER(RefineOpts), P]
+        L.eigen_GPU_batch_refine_DP.restype = I
+        L.eigen_GPU_batch_rayleigh_BufferSize_DP.argtypes = [I, I, I, ctypes.POINTER(SZ)]
+        L.eigen_GPU_batch_rayleigh_BufferSize_DP.restype = I
+        L.eigen_GPU_batch_rayleigh_DP.argtypes = [I, I, I, P, P, P, P, P, SZ, P]
+        L.eigen_GPU_batch_rayleigh_DP.restype = I
         L.eigen_GPU_batch_noalloc_DP.argtypes = [I, I, I, I, P, P, P, P]
         L.eigen_GPU_batch_noalloc_DP.restype = I
         L.eigen_GPU_batch_trace.argtypes = [P, I]
@@ -151,6 +165,8 @@ def exported_symbols():
         "eigen_GPU_check_ex_DP", "eigen_GPU_check_ex_FP",
         "eigen_GPU_batch_trace", "eigen_GPU_batch_noalloc_DP",
         "eigen_GPU_batch_launch_params_DP", "eigen_GPU_batch_launch_params_FP",
+        "eigen_GPU_batch_refine_DP", "eigen_GPU_batch_refine_BufferSize_DP",
+        "eigen_GPU_batch_rayleigh_DP", "eigen_GPU_batch_rayleigh_BufferSize_DP",
         "eigen_GPU_batch_symfunc_DP", "eigen_GPU_batch_symfunc_FP",
         "eigen_GPU_batch_packed_DP", "eigen_GPU_batch_packed_FP",
         "eigen_GPU_batch_uneven_DP", "eigen_GPU_batch_uneven_FP",
@@ -282,6 +298,55 @@ def solve(a, n, nm=None, method=TQL2, sort=True, max_sweep=100, wk=None, stream=
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_ex failed with cudaError {st}")
     return w, info
+
+
+def refine_workspace(L, nm, n, max_iter=0, tol=0.0, fallback=True, chunk=0, device=None):
+    o = RefineOpts(max_iter, tol, 1 if fallback else 0, chunk)
+    lw = ctypes.c_size_t(0)
+    st = lib().eigen_GPU_batch_refine_BufferSize_DP(L, nm, n, ctypes.byref(o), ctypes.byref(lw))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_refine_BufferSize_DP failed with cudaError {st}")
+    return torch.empty(max(lw.value, 16), dtype=torch.uint8, device=device or "cuda")
+
+
+def solve_refined(a, n, nm=None, max_iter=0, tol=0.0, fallback=True, chunk=0, wk=None, stream=None):
+    """eigen_GPU_batch_refine_DP: FP32 solve refined to FP64 accuracy on the
+    tensor cores, in place on the FP64 batch ``a``.  Returns (w, info,
+    iters): iters[k] is the number of refinement iterations matrix k took,
+    0 where it went to the plain FP64 fallback."""
+    L, nm = _dims(a, n, nm)
+    if a.dtype != torch.float64:
+        raise TypeError("eigen_GPU_batch_refine_DP takes float64 matrices")
+    w = torch.empty((L, n), dtype=a.dtype, device=a.device)
+    info = torch.zeros(L, dtype=torch.int32, device=a.device)
+    iters = torch.zeros(L, dtype=torch.int32, device=a.device)
+    if wk is None:
+        wk = refine_workspace(L, nm, n, max_iter, tol, fallback, chunk, a.device)
+    o = RefineOpts(max_iter, tol, 1 if fallback else 0, chunk)
+    st = lib().eigen_GPU_batch_refine_DP(L, nm, n, _ptr(a), _ptr(w), _ptr(wk), wk.numel(), _ptr(info), _ptr(iters),
+                                         ctypes.byref(o), _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_refine_DP failed with cudaError {st}")
+    return w, info, iters
+
+
+def rayleigh(a, x, n, nm=None, want_s=True, want_g=True, stream=None):
+    """eigen_GPU_batch_rayleigh_DP: (S, G) = (X^T A X, X^T X) per matrix,
+    FP64-accurate products on the int8 tensor cores (None where not
+    wanted); S and G are (L, n, n) holding column-major matrices."""
+    L, nm = _dims(a, n, nm)
+    lw = ctypes.c_size_t(0)
+    st = lib().eigen_GPU_batch_rayleigh_BufferSize_DP(L, nm, n, ctypes.byref(lw))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_rayleigh_BufferSize_DP failed with cudaError {st}")
+    wk = torch.empty(max(lw.value, 16), dtype=torch.uint8, device=a.device)
+    s = torch.empty((L, n, n), dtype=torch.float64, device=a.device) if want_s else None
+    g = torch.empty((L, n, n), dtype=torch.float64, device=a.device) if want_g else None
+    st = lib().eigen_GPU_batch_rayleigh_DP(L, nm, n, _ptr(a), _ptr(x), _ptr(s), _ptr(g), _ptr(wk), lw.value,
+                                           _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_rayleigh_DP failed with cudaError {st}")
+    return s, g
 
 
 def packed_size(n):

@@ -172,6 +172,69 @@ cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, c
                                        int *info, const cudaStream_t stream);
 
 /*
+ * Mixed-precision solve refined to FP64 accuracy (no counterpart in the
+ * reference's code; its README:165,169 lists tensor-core acceleration and
+ * "half precision + iterative refinement" as future work).  Same inputs and
+ * outputs as eigen_GPU_batch_DP (eigenvectors overwrite a, eigenvalues
+ * ascending in w; 2 <= n <= 256 here, n = 1 trivially), computed as:
+ *   1. shift by sigma = trace(A)/n and solve A - sigma I in FP32 with this
+ *      library's FP32 path;
+ *   2. refine the eigenvectors by Ogita-Aishima iterations whose products
+ *      (A X, X^T A X, X^T X, X E) run on the int8 tensor cores as exact
+ *      integer slice products (Ozaki's splitting, 8 slices for the FP64-
+ *      accurate ones) accumulated in FP64; clusters of close eigenvalues
+ *      (up to 32) are resolved by an FP64 Rayleigh-Ritz step;
+ *   3. a matrix converges when the largest correction between clusters is
+ *      at most tol; it then leaves the later iterations.
+ * Matrices that do not converge within max_iter iterations, whose FP32
+ * solve failed, or that have a cluster of more than 32 eigenvalues, are
+ * solved again by the plain FP64 path (the fallback).  Results agree with
+ * eigen_GPU_batch_DP's to FP64 accuracy (residual and orthogonality of
+ * order 1e-15 relative to ||A||); equal eigenvalues are ordered by index.
+ * info (device, L ints, optional): 0, or the plain path's status for a
+ * matrix it solved, or -1 for a matrix left unsolved with fallback = 0.
+ * iters (device, L ints, optional): refinement iterations used, 0 for a
+ * matrix that went to the fallback.
+ * The call reads the fallback count back to the host: it synchronizes
+ * `stream` once before returning (and so cannot be captured in a CUDA
+ * graph).  Workspace from eigen_GPU_batch_refine_BufferSize_DP.
+ * Returns cudaErrorInvalidValue for invalid sizes or a too small
+ * workspace, cudaErrorLaunchFailure if a tensor-core product's bounded wait
+ * gave up, otherwise the launch status.
+ */
+typedef struct eigen_GPU_refine_opts {
+  int max_iter; /* refinement iterations at most; <= 0: 3 */
+  double tol;   /* convergence threshold on max |E_ij| between clusters; <= 0: 1e-7 */
+  int fallback; /* 1: unconverged matrices are solved by the plain FP64 path (the
+                   default when opts == NULL); 0: they are left unsolved, info -1 */
+  int chunk;    /* matrices per internal chunk; <= 0: automatic (about 8 GiB) */
+} eigen_GPU_refine_opts;
+cudaError_t eigen_GPU_batch_refine_BufferSize_DP(const int L, const int nm, const int n,
+                                                const eigen_GPU_refine_opts *opts, size_t *lwork);
+cudaError_t eigen_GPU_batch_refine_DP(const int L, const int nm, const int n, double *a, double *w, void *wk,
+                                      const size_t lwork, int *info, int *iters, const eigen_GPU_refine_opts *opts,
+                                      const cudaStream_t stream);
+
+/*
+ * Rayleigh products of a batch (no counterpart in the reference): for each
+ * matrix k, with A_k the symmetric matrix whose upper triangle is at
+ * a + k*nm*n and X_k the n x n matrix at x + k*nm*n (both column-major,
+ * leading dimension nm),
+ *   s + k*n*n  <-  X_k^T A_k X_k      g + k*n*n  <-  X_k^T X_k
+ * (column-major, leading dimension n; either may be NULL).  The products
+ * are computed on the int8 tensor cores as exact integer slice products
+ * (Ozaki's splitting, eight slices) accumulated in FP64, so they carry
+ * FP64 accuracy relative to |A||X| and |X||X|, like FP64 GEMMs: the
+ * ingredients of an a-posteriori check or a refinement of eigenvectors X
+ * (S nearly diagonal, G nearly I).  2 <= n <= 256.  Asynchronous on
+ * stream; workspace from eigen_GPU_batch_rayleigh_BufferSize_DP.
+ */
+cudaError_t eigen_GPU_batch_rayleigh_BufferSize_DP(const int L, const int nm, const int n, size_t *lwork);
+cudaError_t eigen_GPU_batch_rayleigh_DP(const int L, const int nm, const int n, const double *a, const double *x,
+                                        double *s, double *g, void *wk, const size_t lwork,
+                                        const cudaStream_t stream);
+
+/*
  * Packed input (the "flexible data format" the reference's README:166 lists
  * as future work; no counterpart in its code): matrix k is the upper
  * triangle in LAPACK 'U' packed order, element (r, c), r <= c (0-based), at
