@@ -53,7 +53,7 @@ constexpr int OZ_NT = 64;          // N tile (columns of the output per CTA)
 constexpr int OZ_MT = 128;         // M tile (rows of the output per CTA)
 constexpr int OZ_THREADS = 128;
 constexpr int OZ_TMEM_COLS = 512;
-constexpr unsigned OZ_WAIT_LIMIT = 1u << 26;  // try_wait polls before giving up
+constexpr unsigned OZ_WAIT_LIMIT = 1u << 22;  // try_wait polls before giving up
 
 // Padded sizes of the slice layout for order n.
 __host__ __device__ inline int oz_rp(int n) { return ((n + OZ_MT - 1) / OZ_MT) * OZ_MT; }
@@ -242,6 +242,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t a, int32_t (&v)[16])
   for (int u = 0; u < 16; u++) v[u] = (int32_t)r[u];
 }
 
+// thirty-two consecutive 32-bit columns of this thread's TMEM lane (the wait
+// is in the same statement, so no register is read before it arrived)
+__device__ __forceinline__ void tmem_ld32(uint32_t a, int32_t (&v)[32])
+{
+  uint32_t r[32] = {};
+#if EIGB_TCGEN05
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(a));
+#endif
+#pragma unroll
+  for (int u = 0; u < 32; u++) v[u] = (int32_t)r[u];
+}
+
 // ------------------------------------------------------------------ product
 struct OzGemm {
   const int8_t *Ls, *Rs;  // slices of the left / right operand
@@ -262,11 +282,58 @@ struct OzGemm {
   int *err;               // set to 1 when a wait gave up
 };
 
-// dynamic shared memory of k_oz_gemm (operands of one K-block, 1 KB of
-// barriers and alignment slack)
-__host__ __device__ inline size_t oz_gemm_smem(int sL, int sR, int KB)
+// Diagonal groups.  An MMA with N = 256 costs about as long to issue as one
+// with N = 64 (measured on B200: ~125 cycles each), so the right operand
+// of each MMA is a window of four consecutive R slices (4 x 64 rows), and
+// the four 64-column blocks of its 256-column accumulator each collect one
+// diagonal.  In shared memory the R slices sit in descending order, R_j in
+// slot jtop - j, with zero slots where a window reaches past R_sR or below
+// R_1.  Group g (base D = 2 + 4g) accumulates diagonals D+3, D+2, D+1, D in
+// its blocks 0..3; for L slice i its window starts at the slot of
+// j = D + 3 - i.  (1-based slice indices, d = i + j.)
+struct OzGeom {
+  int groups;  // diagonal groups (256 TMEM columns each)
+  int jtop;    // largest j any window reaches (>= sR: slots above R_sR are zero)
+  int jbot;    // smallest j any window reaches (<= 1: slots below R_1 are zero)
+  __host__ __device__ int slots() const { return jtop - jbot + 1; }
+  __host__ __device__ int slot(int j) const { return jtop - j; }
+};
+
+__host__ __device__ inline bool oz_pair_used(int D, int i, int sR) { return D + 3 - i >= 1 && D - i <= sR; }
+
+__host__ __device__ inline OzGeom oz_geom(int sL, int sR, int dmax)
 {
-  return (size_t)(sL * OZ_MT + sR * OZ_NT) * KB + 2048;
+  OzGeom g{};
+  g.groups = (dmax - 2) / 4 + 1;
+  g.jtop = sR;
+  g.jbot = 1;
+  for (int gi = 0; gi < g.groups; gi++) {
+    const int D = 2 + 4 * gi;
+    for (int i = 1; i <= sL; i++) {
+      if (!oz_pair_used(D, i, sR)) continue;
+      g.jtop = max(g.jtop, D + 3 - i);
+      g.jbot = min(g.jbot, D - i);
+    }
+  }
+  return g;
+}
+
+// dynamic shared memory of k_oz_gemm: L slices of one K-block, the R slots,
+// 1 KB of barriers and column scales, 1 KB alignment slack
+__host__ __device__ inline size_t oz_gemm_smem(int sL, int sR, int KB, int dmax = 0)
+{
+  if (dmax <= 0) dmax = sL + sR - 1;
+  const OzGeom g = oz_geom(sL, sR, dmax);
+  return (size_t)(sL * OZ_MT + g.slots() * OZ_NT) * KB + 2048;
+}
+
+constexpr int OZ_SMAX = 8;  // slices per operand at most
+
+// 2^e as an exact double (normal range)
+__device__ __forceinline__ double pow2(int e)
+{
+  e = max(-1022, min(1023, e));
+  return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
 __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_gemm(const OzGemm p)
@@ -278,19 +345,35 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_gemm(const OzGemm p)
   const int nt = tile % p.ntiles;
   if (p.active && !p.active[b]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // 1 KB-aligned operand area, barriers after it
+  const OzGeom geo = oz_geom(p.sL, p.sR, p.dmax);
+  const uint32_t lbytes = OZ_MT * p.KB, rbytes = OZ_NT * p.KB;
+  // 1 KB-aligned operand area, then barriers and the column scales
   unsigned char *base = oz_smem + ((1024 - (smem_u32(oz_smem) & 1023)) & 1023);
   unsigned char *sLb = base;
-  unsigned char *sRb = sLb + (size_t)p.sL * OZ_MT * p.KB;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(sRb + (size_t)p.sR * OZ_NT * p.KB);
-  uint64_t *full = bars, *mdone = bars + 1;
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+  unsigned char *sRb = sLb + (size_t)p.sL * lbytes;  // geo.slots() slots of rbytes
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sRb + (size_t)geo.slots() * rbytes);
+  // bars[0 .. OZ_SMAX): slices L_k, R_k of the K-block landed; bars[OZ_SMAX]:
+  // the K-block's MMAs completed
+  uint64_t *mdone = bars + OZ_SMAX;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + OZ_SMAX + 1);
+  double *cscale = reinterpret_cast<double *>(bars + OZ_SMAX + 2);  // OZ_NT column scales
   __shared__ int failed;
+  const int ns = max(p.sL, p.sR);
   if (threadIdx.x == 0) {
     failed = 0;
-    mbar_init(full, 1);
-    mbar_init(mdone, 1);
+    for (int k = 0; k <= OZ_SMAX; k++) mbar_init(&bars[k], 1);
     mbar_fence_init();
+  }
+  // zero slots (never written by the copies)
+  for (int j = geo.jbot; j <= geo.jtop; j++) {
+    if (j >= 1 && j <= p.sR) continue;
+    uint4 *z = reinterpret_cast<uint4 *>(sRb + (size_t)geo.slot(j) * rbytes);
+    for (uint32_t u = threadIdx.x; u < rbytes / 16; u += OZ_THREADS) z[u] = make_uint4(0, 0, 0, 0);
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (threadIdx.x < OZ_NT) {
+    const int c = nt * OZ_NT + threadIdx.x;
+    cscale[threadIdx.x] = c < p.n ? pow2(p.eR[b * p.RpR + c]) : 0.0;
   }
   if (warp == 0) tmem_alloc(tslot, OZ_TMEM_COLS);
   tmem_fence_before();
@@ -299,72 +382,89 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_gemm(const OzGemm p)
   const uint32_t tmem = *tslot;
   const int nkb = p.Kp / p.KB;
   const size_t Lsz = (size_t)p.RpL * p.Kp, Rsz = (size_t)p.RpR * p.Kp;
-  const uint32_t lbytes = OZ_MT * p.KB, rbytes = OZ_NT * p.KB;
 
-  if (warp == 0 && lane == 0) {  // producer: the slices of each K-block
+  if (warp == 0 && lane == 0) {  // producer: slices L_k, R_k of each K-block, in order of k
     for (int kb = 0; kb < nkb; kb++) {
       if (kb > 0 && !mbar_wait(mdone, (kb - 1) & 1)) {
         atomicExch(&failed, 1);
         break;
       }
-      mbar_expect_tx(full, (uint32_t)(p.sL * lbytes + p.sR * rbytes));
       const int8_t *gl = p.Ls + (size_t)b * p.sL * Lsz + (size_t)kb * p.RpL * p.KB + (size_t)mt * OZ_MT * p.KB;
       const int8_t *gr = p.Rs + (size_t)b * p.sR * Rsz + (size_t)kb * p.RpR * p.KB + (size_t)nt * OZ_NT * p.KB;
-      for (int i = 0; i < p.sL; i++) bulk_g2s(sLb + (size_t)i * lbytes, gl + (size_t)i * Lsz, lbytes, full);
-      for (int j = 0; j < p.sR; j++) bulk_g2s(sRb + (size_t)j * rbytes, gr + (size_t)j * Rsz, rbytes, full);
+      for (int k = 0; k < ns; k++) {
+        const uint32_t bytes = (k < p.sL ? lbytes : 0u) + (k < p.sR ? rbytes : 0u);
+        mbar_expect_tx(&bars[k], bytes);
+        if (k < p.sL) bulk_g2s(sLb + (size_t)k * lbytes, gl + (size_t)k * Lsz, lbytes, &bars[k]);
+        if (k < p.sR) bulk_g2s(sRb + (size_t)geo.slot(k + 1) * rbytes, gr + (size_t)k * Rsz, rbytes, &bars[k]);
+      }
     }
   } else if (warp == 1 && lane == 0) {  // MMA issuer
-    const uint32_t idesc = oz_idesc(OZ_MT, OZ_NT);
+    const uint32_t idesc = oz_idesc(OZ_MT, 4 * OZ_NT);
     const uint32_t sbo = 8 * p.KB;
     uint32_t init = 0;
-    for (int kb = 0; kb < nkb; kb++) {
-      if (!mbar_wait(full, kb & 1)) {
-        atomicExch(&failed, 1);
-        break;
-      }
-      tmem_fence_after();
-      for (int t = 0; t < p.KB / 32; t++) {
-        for (int i = 0; i < p.sL; i++) {
-          const uint64_t da = oz_desc(smem_u32(sLb + (size_t)i * lbytes) + t * 256, 128, sbo);
-          for (int j = 0; j < p.sR && i + j + 2 <= p.dmax; j++) {
-            const uint64_t db = oz_desc(smem_u32(sRb + (size_t)j * rbytes) + t * 256, 128, sbo);
-            const int a = i + j;
-            oz_mma(tmem + (uint32_t)(a * OZ_NT), da, db, idesc, (init >> a) & 1u);
-            init |= 1u << a;
+    for (int kb = 0; kb < nkb && !failed; kb++) {
+      // (group, i) pairs issue once slices L_i and the window's real R_j have landed
+      uint32_t done = 0;  // bit g * 8 + (i - 1)
+      for (int k = 0; k < ns; k++) {
+        if (!mbar_wait(&bars[k], kb & 1)) {
+          atomicExch(&failed, 1);
+          break;
+        }
+        tmem_fence_after();
+        for (int gi = 0; gi < geo.groups; gi++) {
+          const int D = 2 + 4 * gi;
+          for (int i = 1; i <= p.sL; i++) {
+            const uint32_t bit = 1u << (gi * 8 + i - 1);
+            if ((done & bit) || !oz_pair_used(D, i, p.sR)) continue;
+            const int jneed = min(p.sR, D + 3 - i);  // largest real slice of the window
+            if (i > k + 1 || jneed > k + 1) continue;
+            done |= bit;
+            const uint32_t sa = smem_u32(sLb + (size_t)(i - 1) * lbytes);
+            const uint32_t sb = smem_u32(sRb + (size_t)geo.slot(D + 3 - i) * rbytes);
+            for (int t = 0; t < p.KB / 32; t++) {
+              oz_mma(tmem + (uint32_t)(gi * 4 * OZ_NT), oz_desc(sa + t * 256, 128, sbo),
+                     oz_desc(sb + t * 256, 128, sbo), idesc, (init >> gi) & 1u);
+              init |= 1u << gi;
+            }
           }
         }
       }
       oz_commit(mdone);
     }
+    // the last K-block's MMAs: one thread waits, the barrier below releases the rest
+    if (!failed && !mbar_wait(mdone, (nkb - 1) & 1)) atomicExch(&failed, 1);
   }
   __syncwarp();
-  // epilogue: every thread waits for the last K-block's MMAs
-  const bool ok = mbar_wait(mdone, (nkb - 1) & 1);
-  tmem_fence_after();
+  tmem_fence_before();
   __syncthreads();
-  if (!ok || failed) {
+  tmem_fence_after();
+  if (failed) {
     if (threadIdx.x == 0 && p.err) atomicExch(p.err, 1);
   } else {
     const int m = mt * OZ_MT + warp * 32 + lane;  // this thread's output row
     const bool mrow = m < p.n;
-    const int em = p.eL[b * p.RpL + m];
+    const double rsc = pow2(p.eL[b * p.RpL + m] - 12);
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-    for (int c0 = 0; c0 < OZ_NT; c0 += 16) {
-      double acc[16];
+    // every diagonal the groups hold, from the least significant (Horner),
+    // 32 columns at a time
+    const int dtop = 4 * geo.groups + 1;
+    for (int h = 0; h < OZ_NT; h += 32) {
+      double acc[32];
 #pragma unroll
-      for (int u = 0; u < 16; u++) acc[u] = 0.0;
-      for (int a = p.dmax - 2; a >= 0; a--) {
-        int32_t v[16];
-        tmem_ld16(lane_addr + (uint32_t)(a * OZ_NT + c0), v);
+      for (int u = 0; u < 32; u++) acc[u] = 0.0;
+      for (int d = dtop; d >= 2; d--) {
+        const int gi = (d - 2) / 4, blk = 3 - (d - 2) % 4;
+        int32_t v[32];
+        tmem_ld32(lane_addr + (uint32_t)(gi * 4 * OZ_NT + blk * OZ_NT + h), v);
 #pragma unroll
-        for (int u = 0; u < 16; u++) acc[u] = fma(acc[u], 0.0078125, (double)v[u]);
+        for (int u = 0; u < 32; u++) acc[u] = fma(acc[u], 0.0078125, (double)v[u]);
       }
       if (mrow) {
 #pragma unroll
-        for (int u = 0; u < 16; u++) {
-          const int c = nt * OZ_NT + c0 + u;
+        for (int u = 0; u < 32; u++) {
+          const int c = nt * OZ_NT + h + u;
           if (c < p.n) {
-            double r = scalbn(acc[u], em + p.eR[b * p.RpR + c] - 12);
+            double r = acc[u] * rsc * cscale[h + u];
             if (p.add) {
               const long long ai = b * p.ab + (long long)c * p.lda + m;
               r += p.add_f32 ? (double)static_cast<const float *>(p.add)[ai] : static_cast<const double *>(p.add)[ai];

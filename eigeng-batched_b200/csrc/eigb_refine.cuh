@@ -23,9 +23,14 @@
 //        Rayleigh quotient of the corrected basis to first order;
 //        M = W diag(mu) W^T by FP64 Jacobi (one warp); X'_c <- X'_c W,
 //        lambda_c <- mu                          (k_cluster_apply)
-//      A matrix has converged when max |E_ij| between clusters is at most
-//      tol (default 1e-7): its error after that update is of the order
-//      of tol^2 relative.  It then leaves the later iterations.
+//      A matrix has converged when n max|E_ij|^2 (E between clusters) is at
+//      most tol (default 1e-14): the update then leaves a loss of
+//      orthogonality of about ten times that (X'^T X' - I = E^T E - ... to
+//      second order, as E + E^T = R exactly; the factor ten is measured) and
+//      a residual below it.  It then leaves the later iterations.  From
+//      this library's FP32 eigenvectors (max|E| about 1e-3 on the first
+//      iteration for matrices with close eigenvalues, eps_32 ||A|| / gap)
+//      that takes two or three iterations.
 //   4. eigenvalues lambda + sigma, sorted ascending (ties in index order),
 //      eigenvectors to the caller's a; matrices that did not converge in
 //      max_iter iterations, or whose clusters exceed 32 eigenvalues, or
@@ -185,20 +190,24 @@ __device__ void warp_jacobi(double *M, double *V, const int k)
 }
 
 // One CTA (256 threads) per matrix.  Dynamic shared memory: ref_update_smem(n).
+constexpr int REF_JW = 2;  // warps that run the cluster Jacobi (their scratch bounds the CTAs per SM)
 __host__ __device__ inline size_t ref_update_smem(int n)
 {
-  return sizeof(double) * ((size_t)n + 8 * 2 * 32 * 33) + sizeof(int) * 4 * (size_t)n + 64;
+  return sizeof(double) * ((size_t)n + REF_JW * 2 * 32 * 33) + sizeof(int) * 4 * (size_t)n + 64;
 }
 
 __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
 {
   extern __shared__ __align__(16) unsigned char ru_smem[];
   const long b = blockIdx.x;
-  if (!p.act_in[b]) return;
+  if (!p.act_in[b]) {  // inactive stays inactive (the flags alternate between two arrays)
+    if (threadIdx.x == 0) p.act_out[b] = 0;
+    return;
+  }
   const int n = p.n;
   double *lam = reinterpret_cast<double *>(ru_smem);
-  double *jw = lam + n;  // 8 warps x (M, V) of 32 x 33
-  int *ord = reinterpret_cast<int *>(jw + 8 * 2 * 32 * 33);
+  double *jw = lam + n;  // REF_JW warps x (M, V) of 32 x 33
+  int *ord = reinterpret_cast<int *>(jw + REF_JW * 2 * 32 * 33);
   int *cid = ord + n;
   int *csz = cid + n;
   int *cst = csz + n;  // sorted start positions of the clusters of 2 .. REF_CL_MAX
@@ -274,10 +283,11 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
     E[(size_t)j * n + i] = e;
   }
   em = blk_max(em, red);
-  // cluster Rayleigh-Ritz: one warp per cluster of 2 .. REF_CL_MAX
+  // cluster Rayleigh-Ritz: one warp per cluster of 2 .. REF_CL_MAX, the
+  // first REF_JW warps
   const int warp = tid >> 5, l = tid & 31;
-  double *M = jw + warp * 2 * 32 * 33, *V = M + 32 * 33;
-  for (int c = warp; c < ncl; c += 8) {
+  double *M = jw + (warp % REF_JW) * 2 * 32 * 33, *V = M + 32 * 33;
+  for (int c = warp; warp < REF_JW && c < ncl; c += REF_JW) {
     const int k0 = cst[c], sz = csz[k0];
     for (int q = 0; q < sz; q++) {
       if (l < sz) {
@@ -320,7 +330,7 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
   }
   if (tid == 0) {
     const bool fin = !bad && em <= 1.7976931348623157e308;
-    const bool conv = fin && em <= p.tol;
+    const bool conv = fin && (double)n * em * em <= p.tol;
     p.emax[b] = em;
     if (conv) p.conv_it[b] = p.it;
     const bool more = fin && !conv && !p.last;

@@ -22,6 +22,8 @@
 #include "eigb_kernels.cuh"
 #include "eigb_symfunc.cuh"
 #include "eigb_refine.cuh"
+#include "eigb_learned.cuh"
+#include "../../include/eigen_GPU_learned.h"
 #include "../../include/eigen_GPU_batch.h"
 
 namespace eigb {
@@ -68,6 +70,46 @@ cudaError_t dev_props(DevProps &out)
 }
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Tuned options (eigen_GPU_batch_tune_set): per device, per (element size,
+// n), the options a solve uses where the caller leaves them automatic.
+struct TuneKey {
+  int dev, esize, n;
+  bool operator<(const TuneKey &o) const
+  {
+    return dev != o.dev ? dev < o.dev : (esize != o.esize ? esize < o.esize : n < o.n);
+  }
+};
+std::map<TuneKey, eigen_GPU_tune_entry> g_tune;
+
+// the caller's options with the tuned values filled in where they are
+// automatic (split <= 0, zmem == AUTO, ql_mpw <= 0); `out` receives them
+inline const eigen_GPU_batch_opts *tuned(const eigen_GPU_batch_opts *opts, int esize, int n,
+                                         eigen_GPU_batch_opts &out)
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return opts;
+  eigen_GPU_tune_entry e;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_tune.empty()) return opts;
+    auto it = g_tune.find(TuneKey{dev, esize, n});
+    if (it == g_tune.end()) return opts;
+    e = it->second;
+  }
+  if (opts) {
+    out = *opts;
+  } else {  // the reference defaults
+    out = eigen_GPU_batch_opts{};
+    out.method = EIGEN_GPU_BATCH_TQL2;
+    out.sort = 1;
+    out.max_sweep = 100;
+  }
+  if (out.split <= 0 && e.split > 0) out.split = e.split;
+  if (out.zmem == EIGEN_GPU_ZMEM_AUTO && e.zmem == EIGEN_GPU_ZMEM_SHARED) out.zmem = EIGEN_GPU_ZMEM_SHARED;
+  if (out.ql_mpw <= 0 && e.ql_mpw > 0) out.ql_mpw = e.ql_mpw;
+  return &out;
+}
 
 // phase timing events set by eigen_GPU_batch_trace
 cudaEvent_t *g_trace = nullptr;
@@ -229,6 +271,8 @@ cudaError_t buffer_size(long L, int nm, int n, int m, size_t *lwork, const eigen
   DevProps dp;
   cudaError_t err = dev_props(dp);
   if (err != cudaSuccess) return err;
+  eigen_GPU_batch_opts tuned_opts;
+  opts = tuned(opts, (int)sizeof(T), n, tuned_opts);
   Plan<T> pl;
   if ((err = make_plan<T>(L, nm, n, dp, pl, opts)) != cudaSuccess) return err;
   if (lwork) *lwork = pl.bytes;
@@ -309,6 +353,8 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
                 const Indirect &ix = Indirect(), const Stage &sg = Stage())
 {
   if (bad_args(L, nm, n, m) || a == nullptr || w == nullptr) return cudaErrorInvalidValue;
+  eigen_GPU_batch_opts tuned_opts;
+  opts = tuned(opts, (int)sizeof(T), n, tuned_opts);
   const long first = sg.first, count = sg.count <= 0 ? L - sg.first : sg.count;
   if (first < 0 || count < 1 || first + count > L || sg.phases < 1 || sg.phases > EIGEN_GPU_STAGE_ALL)
     return cudaErrorInvalidValue;
@@ -901,7 +947,7 @@ constexpr int REF_DMAX = 9, REF_DMAX_XE = 8;
 
 struct RefOpts {
   int max_iter = 3;
-  double tol = 1e-7;
+  double tol = 1e-14;
   int fallback = 1;
   int chunk = 0;
 };
@@ -1106,7 +1152,7 @@ cudaError_t run_refine(long L, int nm, int n, double *a, double *w, void *wk, si
   if ((err = cudaMemsetAsync(cnt, 0, 2 * sizeof(int), stream)) != cudaSuccess) return err;
   // shared memory of the products: their operands, and at least half of
   // the SM so that no two of these CTAs (512 TMEM columns each) share an SM
-  const size_t need = std::max(oz_gemm_smem(REF_S, REF_S, ly.KB), oz_gemm_smem(REF_SX, REF_SE, ly.KB));
+  const size_t need = std::max(oz_gemm_smem(REF_S, REF_S, ly.KB, REF_DMAX), oz_gemm_smem(REF_SX, REF_SE, ly.KB, REF_DMAX_XE));
   const size_t half = (size_t)dp.smem_sm / 2 + 1024;
   const size_t gsm = std::min<size_t>(std::max(need, half), (size_t)dp.smem_optin);
   if (need > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
@@ -1191,7 +1237,10 @@ cudaError_t run_refine(long L, int nm, int n, double *a, double *w, void *wk, si
     }
     long long *aoff = static_cast<long long *>(P(ly.aoff)), *woff = static_cast<long long *>(P(ly.woff));
     k_ref_offsets<<<(unsigned)std::min<long>((L + 255) / 256, 4096), 256, 0, stream>>>(L, nm, n, aoff, woff);
-    eigen_GPU_batch_opts o64{};
+    eigen_GPU_batch_opts o64{};  // the reference defaults: tql2, sorted, 100 sweeps
+    o64.method = EIGEN_GPU_BATCH_TQL2;
+    o64.sort = 1;
+    o64.max_sweep = 100;
     o64.chunk = (int)ly.Lc;
     Indirect ix;
     ix.kid = fb_list;
@@ -1273,7 +1322,7 @@ cudaError_t run_rayleigh(long L, int nm, int n, const double *a, const double *x
   rl.Rp = oz_rp(n);
   rl.Kp = oz_kp(n);
   rl.KB = oz_kb(n);
-  const size_t need = oz_gemm_smem(REF_S, REF_S, rl.KB);
+  const size_t need = oz_gemm_smem(REF_S, REF_S, rl.KB, REF_DMAX);
   const size_t gsm = std::min<size_t>(std::max(need, (size_t)dp.smem_sm / 2 + 1024), (size_t)dp.smem_optin);
   if (need > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
   if ((err = set_smem(k_oz_gemm, gsm)) != cudaSuccess) return err;
@@ -1316,6 +1365,491 @@ cudaError_t run_rayleigh(long L, int nm, int n, const double *a, const double *x
       ref_gemm(rl, lc, XS, eX, REF_S, XS, eX, REF_S, REF_DMAX, g + (size_t)c0 * n * n, nullptr, 0, nullptr, errf,
                gsm, stream);
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  }
+  return cudaSuccess;
+}
+
+// ---- the learned warm start's network (eigb_mlp.cuh) ----
+//
+// Parameters of the MLP d0 -> d1 -> d2 -> d3 (tanh, tanh, linear), d0 a
+// multiple of 8: FP32 flat [W1 b1 W2 b2 W3 b3] (W_l row-major, out x in),
+// its Adam moments m and v, then the BF16 copies W1, W2, W2^T, W3, W3^T.
+struct MlpLayout {
+  int d0, d1, d2, d3;
+  size_t w1, b1, w2, b2, w3, b3, P;  // element offsets in the flat FP32 block, and its size
+  size_t m, v, w1b, w2b, w2t, w3b, w3t, bytes;  // byte offsets
+};
+
+inline bool mlp_bad(int d0, int d1, int d2, int d3)
+{
+  return d0 < 8 || d1 < 8 || d2 < 8 || d3 < 8 || (d0 % 8) || (d1 % 8) || (d2 % 8) || (d3 % 8) || d1 > 4096 ||
+         d2 > 4096 || d3 > 65536;
+}
+
+inline MlpLayout mlp_layout(int d0, int d1, int d2, int d3)
+{
+  MlpLayout l{};
+  l.d0 = d0;
+  l.d1 = d1;
+  l.d2 = d2;
+  l.d3 = d3;
+  size_t e = 0;
+  l.w1 = e;
+  e += (size_t)d1 * d0;
+  l.b1 = e;
+  e += d1;
+  l.w2 = e;
+  e += (size_t)d2 * d1;
+  l.b2 = e;
+  e += d2;
+  l.w3 = e;
+  e += (size_t)d3 * d2;
+  l.b3 = e;
+  e += d3;
+  l.P = e;
+  size_t o = align256(sizeof(float) * e);
+  l.m = o;
+  o = align256(o + sizeof(float) * e);
+  l.v = o;
+  o = align256(o + sizeof(float) * e);
+  l.w1b = o;
+  o = align256(o + 2 * (size_t)d1 * d0);
+  l.w2b = o;
+  o = align256(o + 2 * (size_t)d2 * d1);
+  l.w2t = o;
+  o = align256(o + 2 * (size_t)d2 * d1);
+  l.w3b = o;
+  o = align256(o + 2 * (size_t)d3 * d2);
+  l.w3t = o;
+  o = align256(o + 2 * (size_t)d3 * d2);
+  l.bytes = o;
+  return l;
+}
+
+// workspace of a forward (train = 0) or training pass over `rows` rows
+struct MlpWs {
+  size_t xb, xt, h1, h1b, h1t, h2, h2b, h2t, y, yb, dyb, dy32, dyt, dh2, dz2b, dz2, dz2t, dh1, dz1b, dz1, dz1t, grad,
+      sse, err, bytes;
+};
+
+inline MlpWs mlp_ws(const MlpLayout &l, int rows, bool train)
+{
+  MlpWs w{};
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = align256(o + bytes);
+    return at;
+  };
+  const size_t R = (size_t)rows;
+  w.xb = take(2 * R * l.d0);
+  w.h1b = take(2 * R * l.d1);
+  w.h2b = take(2 * R * l.d2);
+  w.yb = take(2 * R * l.d3);
+  w.err = take(sizeof(int));
+  if (train) {
+    w.y = take(4 * R * l.d3);
+    w.xt = take(2 * R * l.d0);
+    w.h1 = take(4 * R * l.d1);
+    w.h1t = take(2 * R * l.d1);
+    w.h2 = take(4 * R * l.d2);
+    w.h2t = take(2 * R * l.d2);
+    w.dyb = take(2 * R * l.d3);
+    w.dy32 = take(4 * R * l.d3);
+    w.dyt = take(2 * R * l.d3);
+    w.dh2 = take(4 * R * l.d2);
+    w.dz2b = take(2 * R * l.d2);
+    w.dz2 = take(4 * R * l.d2);
+    w.dz2t = take(2 * R * l.d2);
+    w.dh1 = take(4 * R * l.d1);
+    w.dz1b = take(2 * R * l.d1);
+    w.dz1 = take(4 * R * l.d1);
+    w.dz1t = take(2 * R * l.d1);
+    w.grad = take(sizeof(float) * l.P);
+    w.sse = take(sizeof(double));
+  }
+  w.bytes = o;
+  return w;
+}
+
+inline cudaError_t mm_launch(const bf16 *A, int lda, const bf16 *B, int ldb, int M, int N, int K, float *C, int ldc,
+                             bf16 *Cb, int ldcb, const float *bias, int act, float alpha, int *err, cudaStream_t st)
+{
+  if (M < 1 || N < 1 || K < 8 || (K % 8) || (lda % 8) || (ldb % 8)) return cudaErrorInvalidValue;
+  MmP p{};
+  p.A = A;
+  p.lda = lda;
+  p.B = B;
+  p.ldb = ldb;
+  p.M = M;
+  p.N = N;
+  p.K = K;
+  p.C = C;
+  p.ldc = ldc;
+  p.Cb = Cb;
+  p.ldcb = ldcb;
+  p.bias = bias;
+  p.act = act;
+  p.alpha = alpha;
+  p.err = err;
+  dim3 grid((unsigned)((N + MM_T - 1) / MM_T), (unsigned)((M + MM_T - 1) / MM_T), 1);
+  k_mm_bf16<<<grid, MM_THREADS, mm_smem(), st>>>(p);
+  return cudaGetLastError();
+}
+
+inline cudaError_t mm_setup()
+{
+  return cudaFuncSetAttribute(k_mm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mm_smem());
+}
+
+inline unsigned grid1(long count) { return (unsigned)std::max<long>(1, std::min<long>((count + 255) / 256, 8192)); }
+
+inline void transpose_bf16(const bf16 *in, int rows, int cols, bf16 *out, cudaStream_t st)
+{
+  dim3 g((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+  k_t_bf16<<<g, 256, 0, st>>>(rows, cols, in, cols, out, rows);
+}
+
+// forward over rows (x: rows x d0 FP32, row-major); output Y (FP32) and its
+// BF16 copy in the workspace; y (optional) receives the FP32 output
+cudaError_t mlp_forward(const MlpLayout &l, const void *params, int rows, const float *x, float *y, char *ws,
+                        const MlpWs &w, bool keep32, cudaStream_t st)
+{
+  const float *P = static_cast<const float *>(params);
+  const char *pb = static_cast<const char *>(params);
+  cudaError_t err;
+  if ((err = mm_setup()) != cudaSuccess) return err;
+  bf16 *xb = reinterpret_cast<bf16 *>(ws + w.xb);
+  k_to_bf16<<<grid1((long)rows * l.d0), 256, 0, st>>>(rows, l.d0, x, l.d0, xb, l.d0);
+  int *ef = reinterpret_cast<int *>(ws + w.err);
+  bf16 *h1b = reinterpret_cast<bf16 *>(ws + w.h1b), *h2b = reinterpret_cast<bf16 *>(ws + w.h2b);
+  float *h1 = keep32 ? reinterpret_cast<float *>(ws + w.h1) : nullptr;
+  float *h2 = keep32 ? reinterpret_cast<float *>(ws + w.h2) : nullptr;
+  if ((err = mm_launch(xb, l.d0, reinterpret_cast<const bf16 *>(pb + l.w1b), l.d0, rows, l.d1, l.d0, h1, l.d1, h1b,
+                       l.d1, P + l.b1, 1, 1.0f, ef, st)) != cudaSuccess)
+    return err;
+  if ((err = mm_launch(h1b, l.d1, reinterpret_cast<const bf16 *>(pb + l.w2b), l.d1, rows, l.d2, l.d1, h2, l.d2, h2b,
+                       l.d2, P + l.b2, 1, 1.0f, ef, st)) != cudaSuccess)
+    return err;
+  float *yo = y ? y : (keep32 ? reinterpret_cast<float *>(ws + w.y) : nullptr);
+  return mm_launch(h2b, l.d2, reinterpret_cast<const bf16 *>(pb + l.w3b), l.d2, rows, l.d3, l.d2, yo, l.d3,
+                   reinterpret_cast<bf16 *>(ws + w.yb), l.d3, P + l.b3, 0, 1.0f, ef, st);
+}
+
+// gradient of the mean squared error over rows x d3 outputs into grad (the
+// flat FP32 layout); sse (device, optional) += sum of squared errors
+cudaError_t mlp_backward(const MlpLayout &l, const void *params, int rows, const float *t, float *grad, double *sse,
+                         char *ws, const MlpWs &w, cudaStream_t st)
+{
+  const char *pb = static_cast<const char *>(params);
+  cudaError_t err;
+  int *ef = reinterpret_cast<int *>(ws + w.err);
+  auto F = [&](size_t off) { return reinterpret_cast<float *>(ws + off); };
+  auto H = [&](size_t off) { return reinterpret_cast<bf16 *>(ws + off); };
+  const long ny = (long)rows * l.d3;
+  k_mse_grad<<<grid1(ny), 256, 0, st>>>(ny, F(w.y), t, H(w.dyb), F(w.dy32), sse ? sse : reinterpret_cast<double *>(ws + w.sse));
+  // layer 3: dW3 = dY^T H2, db3 = colsum dY, dH2 = dY W3
+  transpose_bf16(H(w.dyb), rows, l.d3, H(w.dyt), st);
+  transpose_bf16(H(w.h2b), rows, l.d2, H(w.h2t), st);
+  if ((err = mm_launch(H(w.dyt), rows, H(w.h2t), rows, l.d3, l.d2, rows, grad + l.w3, l.d2, nullptr, 0, nullptr, 0,
+                       1.0f, ef, st)) != cudaSuccess)
+    return err;
+  k_colsum<<<(l.d3 + 255) / 256, 256, 0, st>>>(rows, l.d3, F(w.dy32), grad + l.b3);
+  if ((err = mm_launch(H(w.dyb), l.d3, reinterpret_cast<const bf16 *>(pb + l.w3t), l.d3, rows, l.d2, l.d3, F(w.dh2),
+                       l.d2, nullptr, 0, nullptr, 0, 1.0f, ef, st)) != cudaSuccess)
+    return err;
+  // layer 2
+  k_tanh_bwd<<<grid1((long)rows * l.d2), 256, 0, st>>>((long)rows * l.d2, F(w.dh2), F(w.h2), H(w.dz2b), F(w.dz2));
+  transpose_bf16(H(w.dz2b), rows, l.d2, H(w.dz2t), st);
+  transpose_bf16(H(w.h1b), rows, l.d1, H(w.h1t), st);
+  if ((err = mm_launch(H(w.dz2t), rows, H(w.h1t), rows, l.d2, l.d1, rows, grad + l.w2, l.d1, nullptr, 0, nullptr, 0,
+                       1.0f, ef, st)) != cudaSuccess)
+    return err;
+  k_colsum<<<(l.d2 + 255) / 256, 256, 0, st>>>(rows, l.d2, F(w.dz2), grad + l.b2);
+  if ((err = mm_launch(H(w.dz2b), l.d2, reinterpret_cast<const bf16 *>(pb + l.w2t), l.d2, rows, l.d1, l.d2, F(w.dh1),
+                       l.d1, nullptr, 0, nullptr, 0, 1.0f, ef, st)) != cudaSuccess)
+    return err;
+  // layer 1
+  k_tanh_bwd<<<grid1((long)rows * l.d1), 256, 0, st>>>((long)rows * l.d1, F(w.dh1), F(w.h1), H(w.dz1b), F(w.dz1));
+  transpose_bf16(H(w.dz1b), rows, l.d1, H(w.dz1t), st);
+  transpose_bf16(H(w.xb), rows, l.d0, H(w.xt), st);
+  if ((err = mm_launch(H(w.dz1t), rows, H(w.xt), rows, l.d1, l.d0, rows, grad + l.w1, l.d0, nullptr, 0, nullptr, 0,
+                       1.0f, ef, st)) != cudaSuccess)
+    return err;
+  k_colsum<<<(l.d1 + 255) / 256, 256, 0, st>>>(rows, l.d1, F(w.dz1), grad + l.b1);
+  return cudaGetLastError();
+}
+
+// BF16 copies (and transposes) of the FP32 weights
+inline void mlp_sync_bf16(const MlpLayout &l, void *params, cudaStream_t st)
+{
+  float *P = static_cast<float *>(params);
+  char *pb = static_cast<char *>(params);
+  k_to_bf16<<<grid1((long)l.d1 * l.d0), 256, 0, st>>>(l.d1, l.d0, P + l.w1, l.d0, reinterpret_cast<bf16 *>(pb + l.w1b),
+                                                     l.d0);
+  k_to_bf16<<<grid1((long)l.d2 * l.d1), 256, 0, st>>>(l.d2, l.d1, P + l.w2, l.d1, reinterpret_cast<bf16 *>(pb + l.w2b),
+                                                     l.d1);
+  transpose_bf16(reinterpret_cast<bf16 *>(pb + l.w2b), l.d2, l.d1, reinterpret_cast<bf16 *>(pb + l.w2t), st);
+  k_to_bf16<<<grid1((long)l.d3 * l.d2), 256, 0, st>>>(l.d3, l.d2, P + l.w3, l.d2, reinterpret_cast<bf16 *>(pb + l.w3b),
+                                                     l.d2);
+  transpose_bf16(reinterpret_cast<bf16 *>(pb + l.w3b), l.d3, l.d2, reinterpret_cast<bf16 *>(pb + l.w3t), st);
+}
+
+cudaError_t mlp_init(const MlpLayout &l, void *params, unsigned long long seed, cudaStream_t st)
+{
+  float *P = static_cast<float *>(params);
+  char *pb = static_cast<char *>(params);
+  cudaError_t err;
+  if ((err = cudaMemsetAsync(params, 0, l.bytes, st)) != cudaSuccess) return err;
+  // uniform +-sqrt(6 / (fan_in + fan_out)) weights, zero biases
+  k_init_uniform<<<grid1((long)l.d1 * l.d0), 256, 0, st>>>((long)l.d1 * l.d0, P + l.w1,
+                                                           sqrtf(6.0f / (l.d0 + l.d1)), seed);
+  k_init_uniform<<<grid1((long)l.d2 * l.d1), 256, 0, st>>>((long)l.d2 * l.d1, P + l.w2,
+                                                           sqrtf(6.0f / (l.d1 + l.d2)), seed + 1);
+  k_init_uniform<<<grid1((long)l.d3 * l.d2), 256, 0, st>>>((long)l.d3 * l.d2, P + l.w3,
+                                                           sqrtf(6.0f / (l.d2 + l.d3)), seed + 2);
+  (void)pb;
+  mlp_sync_bf16(l, params, st);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_adam(const MlpLayout &l, void *params, const float *grad, float lr, int step, cudaStream_t st)
+{
+  float *P = static_cast<float *>(params);
+  char *pb = static_cast<char *>(params);
+  float *m = reinterpret_cast<float *>(pb + l.m), *v = reinterpret_cast<float *>(pb + l.v);
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float c1 = 1.0f / (1.0f - powf(b1, (float)step)), c2 = 1.0f / (1.0f - powf(b2, (float)step));
+  k_adam<<<grid1((long)l.P), 256, 0, st>>>(1, (int)l.P, P, grad, m, v, nullptr, nullptr, lr, b1, b2, eps, c1, c2);
+  mlp_sync_bf16(l, params, st);
+  return cudaGetLastError();
+}
+
+// ---- learned warm start solve (eigb_learned.cuh) ----
+struct LwLayout {
+  long Lc = 0;
+  size_t af, x0, pm, sm, gm, ym, xm, axm, mu, sw, as, x0s, ps, x0r, ys, xs, ea, ex0, ep, ex0r, ey, ex, feat, ginv,
+      v0r, mws, cnt, fb, aoff, woff, bytes, chunk_bytes;
+  MlpWs mw;
+};
+constexpr int LW_S = 4, LW_DMAX = 5;  // FP32-level products: 4 slices, diagonals up to 5
+
+inline size_t lw_chunk_layout(long Lc, int nm, int n, const MlpLayout &ml, const DevProps &dp, LwLayout &ly)
+{
+  const size_t nn = (size_t)n * n, sl = oz_slice_bytes(n), rp = (size_t)oz_rp(n);
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = o;
+    o = align256(o + bytes);
+    return at;
+  };
+  ly.Lc = Lc;
+  ly.af = take(8 * nn * Lc);
+  ly.x0 = take(4 * nn * Lc);
+  ly.pm = take(8 * nn * Lc);
+  ly.sm = take(8 * nn * Lc);
+  ly.gm = take(8 * nn * Lc);
+  ly.ym = take(8 * nn * Lc);
+  ly.xm = take(8 * nn * Lc);
+  ly.axm = ly.pm;  // P is dead once S is formed
+  ly.mu = take(8 * (size_t)n * Lc);
+  ly.sw = take(4 * (size_t)Lc);
+  ly.as = take(sl * LW_S * Lc);
+  ly.x0s = take(sl * LW_S * Lc);
+  ly.ps = take(sl * LW_S * Lc);
+  ly.x0r = ly.ps;  // P's slices are dead once S is formed
+  ly.ys = take(sl * LW_S * Lc);
+  ly.xs = ly.x0s;  // X0's column slices are dead once G is formed
+  ly.ea = take(4 * rp * Lc);
+  ly.ex0 = take(4 * rp * Lc);
+  ly.ep = take(4 * rp * Lc);
+  ly.ex0r = ly.ep;
+  ly.ey = take(4 * rp * Lc);
+  ly.ex = ly.ex0;
+  ly.feat = take(4 * (size_t)LW_D0 * Lc);
+  ly.ginv = take(8 * 16);
+  ly.v0r = take(2 * nn);
+  ly.mw = mlp_ws(ml, (int)Lc, false);
+  ly.mws = take(ly.mw.bytes);
+  Plan<float> pf;
+  eigen_GPU_batch_opts o32{};
+  o32.method = EIGEN_GPU_BATCH_TQL2;
+  o32.sort = 1;
+  o32.max_sweep = 100;
+  o32.chunk = (int)Lc;
+  if (make_plan<float>(Lc, nm, n, dp, pf, &o32) != cudaSuccess) return 0;
+  return std::max(o, pf.bytes);
+}
+
+inline cudaError_t lw_plan(long L, int nm, int n, const MlpLayout &ml, const DevProps &dp, int chunk, LwLayout &ly)
+{
+  long Lc = chunk > 0 ? std::min<long>(L, chunk) : L;
+  size_t cb = 0;
+  for (;;) {
+    cb = lw_chunk_layout(Lc, nm, n, ml, dp, ly);
+    if (cb == 0) return cudaErrorInvalidValue;
+    if (chunk > 0 || cb <= kWsBudget || Lc <= 256) break;
+    Lc = std::max<long>(256, (long)((double)Lc * (double)kWsBudget / (double)cb * 0.98));
+    const long nch = (L + Lc - 1) / Lc;
+    Lc = (L + nch - 1) / nch;
+  }
+  ly.chunk_bytes = align256(cb);
+  size_t o = ly.chunk_bytes;
+  ly.fb = o;
+  o = align256(o + sizeof(int) * L);
+  ly.aoff = o;
+  o = align256(o + sizeof(long long) * L);
+  ly.woff = o;
+  o = align256(o + sizeof(long long) * L);
+  ly.cnt = o;
+  o = align256(o + 2 * sizeof(int));
+  ly.bytes = o;
+  return cudaSuccess;
+}
+
+struct LwOpts {
+  int warm = EIGEN_GPU_WARM_NETWORK;
+  int max_sweeps = 10;
+  double tol = 1e-6;
+  double jacobi_tol = 1e-10;
+  int fallback = 1;
+  int chunk = 0;
+};
+
+inline LwOpts lw_opts(const eigen_GPU_learned_opts *o)
+{
+  LwOpts r;
+  if (o) {
+    r.warm = o->warm;
+    if (o->max_sweeps > 0) r.max_sweeps = o->max_sweeps;
+    if (o->tol > 0) r.tol = o->tol;
+    if (o->jacobi_tol > 0) r.jacobi_tol = o->jacobi_tol;
+    r.fallback = o->fallback ? 1 : 0;
+    r.chunk = o->chunk;
+  }
+  return r;
+}
+
+inline bool lw_bad(long L, int nm, int n, int d1, int d2)
+{
+  return L < 1 || n < 8 || n > LW_NMAX || (n % 8) || nm < n || mlp_bad(LW_D0, d1, d2, n * n);
+}
+
+cudaError_t lw_buffer_size(long L, int nm, int n, int d1, int d2, const eigen_GPU_learned_opts *opts, size_t *lwork)
+{
+  if (!lwork) return cudaErrorInvalidValue;
+  *lwork = 0;
+  if (lw_bad(L, nm, n, d1, d2)) return cudaErrorInvalidValue;
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  LwLayout ly;
+  if ((err = lw_plan(L, nm, n, mlp_layout(LW_D0, d1, d2, n * n), dp, lw_opts(opts).chunk, ly)) != cudaSuccess)
+    return err;
+  *lwork = ly.bytes;
+  return cudaSuccess;
+}
+
+cudaError_t run_learned(long L, int nm, int n, float *a, float *w, const float *fam, const void *params, int d1, int d2,
+                        void *wk, size_t lwork, int *info, int *sweeps, double *resid,
+                        const eigen_GPU_learned_opts *opts, cudaStream_t stream)
+{
+  if (lw_bad(L, nm, n, d1, d2) || !a || !w || !fam) return cudaErrorInvalidValue;
+  const LwOpts lo = lw_opts(opts);
+  if (lo.warm < EIGEN_GPU_WARM_NETWORK || lo.warm > EIGEN_GPU_WARM_IDENTITY) return cudaErrorInvalidValue;
+  if (lo.warm == EIGEN_GPU_WARM_NETWORK && !params) return cudaErrorInvalidValue;
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  const MlpLayout ml = mlp_layout(LW_D0, d1, d2, n * n);
+  LwLayout ly;
+  if ((err = lw_plan(L, nm, n, ml, dp, lo.chunk, ly)) != cudaSuccess) return err;
+  if (!wk || (lwork != 0 && lwork < ly.bytes)) return cudaErrorInvalidValue;
+  char *base = static_cast<char *>(wk);
+  auto P = [&](size_t off) { return static_cast<void *>(base + off); };
+  auto D = [&](size_t off) { return static_cast<double *>(P(off)); };
+  auto I8 = [&](size_t off) { return static_cast<int8_t *>(P(off)); };
+  auto IN = [&](size_t off) { return static_cast<int *>(P(off)); };
+  int *fb_list = IN(ly.fb), *cnt = IN(ly.cnt), *errf = cnt + 1;
+  if ((err = cudaMemsetAsync(cnt, 0, 2 * sizeof(int), stream)) != cudaSuccess) return err;
+  RefLayout rl;
+  rl.n = n;
+  rl.Rp = oz_rp(n);
+  rl.Kp = oz_kp(n);
+  rl.KB = oz_kb(n);
+  const size_t need = oz_gemm_smem(LW_S, LW_S, rl.KB, LW_DMAX);
+  const size_t gsm = std::min<size_t>(std::max(need, (size_t)dp.smem_sm / 2 + 1024), (size_t)dp.smem_optin);
+  if ((err = set_smem(k_oz_gemm, gsm)) != cudaSuccess) return err;
+  const size_t psm = lw_polish_smem(n);
+  if ((err = set_smem(k_lw_polish, psm)) != cudaSuccess) return err;
+  const size_t nn = (size_t)n * n;
+  const float *v0 = fam + 5 * nn;
+  double *ginv = D(ly.ginv);
+  k_lw_gram<<<1, 256, 0, stream>>>(n, fam, ginv);
+  bf16 *v0r = static_cast<bf16 *>(P(ly.v0r));
+  k_lw_v0rows<<<grid1((long)nn), 256, 0, stream>>>(n, v0, v0r);
+  float *X0 = static_cast<float *>(P(ly.x0));
+  char *mws = static_cast<char *>(P(ly.mws));
+  for (long c0 = 0; c0 < L; c0 += ly.Lc) {
+    const long lc = std::min(ly.Lc, L - c0);
+    k_lw_prep<<<(unsigned)lc, 256, 0, stream>>>(a + (size_t)c0 * nm * n, nm, n, D(ly.af));
+    if (lo.warm == EIGEN_GPU_WARM_NETWORK) {
+      float *feat = static_cast<float *>(P(ly.feat));
+      k_lw_features<<<(unsigned)lc, 256, 0, stream>>>(n, D(ly.af), fam, ginv, feat);
+      if ((err = mlp_forward(ml, params, (int)lc, feat, nullptr, mws, ly.mw, false, stream)) != cudaSuccess) return err;
+      // X0 = V0 C: rows (matrix, column j) of the output, K index k
+      if ((err = mm_launch(reinterpret_cast<const bf16 *>(mws + ly.mw.yb), n, v0r, n, (int)(lc * n), n, n, X0, n,
+                           nullptr, 0, nullptr, 0, 1.0f, errf, stream)) != cudaSuccess)
+        return err;
+    } else {
+      k_lw_fill<<<grid1(lc * (long)nn), 256, 0, stream>>>(lc, n, lo.warm, v0, X0);
+    }
+    // S = X0^T A X0, G = X0^T X0
+    ref_slice(rl, lc, D(ly.af), 0, n, 1, LW_S, I8(ly.as), IN(ly.ea), nullptr, stream);
+    ref_slice(rl, lc, X0, 1, n, 1, LW_S, I8(ly.x0s), IN(ly.ex0), nullptr, stream);
+    ref_gemm(rl, lc, I8(ly.as), IN(ly.ea), LW_S, I8(ly.x0s), IN(ly.ex0), LW_S, LW_DMAX, D(ly.pm), nullptr, 0, nullptr,
+             errf, gsm, stream);
+    ref_slice(rl, lc, D(ly.pm), 0, n, 1, LW_S, I8(ly.ps), IN(ly.ep), nullptr, stream);
+    ref_gemm(rl, lc, I8(ly.x0s), IN(ly.ex0), LW_S, I8(ly.ps), IN(ly.ep), LW_S, LW_DMAX, D(ly.sm), nullptr, 0, nullptr,
+             errf, gsm, stream);
+    ref_gemm(rl, lc, I8(ly.x0s), IN(ly.ex0), LW_S, I8(ly.x0s), IN(ly.ex0), LW_S, LW_DMAX, D(ly.gm), nullptr, 0,
+             nullptr, errf, gsm, stream);
+    k_lw_polish<<<(unsigned)lc, 256, psm, stream>>>(n, D(ly.sm), D(ly.gm), D(ly.ym), D(ly.mu), IN(ly.sw),
+                                                    lo.max_sweeps, lo.jacobi_tol);
+    // X = X0 Y, then A X for the gate
+    ref_slice(rl, lc, X0, 1, 1, n, LW_S, I8(ly.x0r), IN(ly.ex0r), nullptr, stream);
+    ref_slice(rl, lc, D(ly.ym), 0, n, 1, LW_S, I8(ly.ys), IN(ly.ey), nullptr, stream);
+    ref_gemm(rl, lc, I8(ly.x0r), IN(ly.ex0r), LW_S, I8(ly.ys), IN(ly.ey), LW_S, LW_DMAX, D(ly.xm), nullptr, 0, nullptr,
+             errf, gsm, stream);
+    ref_slice(rl, lc, D(ly.xm), 0, n, 1, LW_S, I8(ly.xs), IN(ly.ex), nullptr, stream);
+    ref_gemm(rl, lc, I8(ly.as), IN(ly.ea), LW_S, I8(ly.xs), IN(ly.ex), LW_S, LW_DMAX, D(ly.axm), nullptr, 0, nullptr,
+             errf, gsm, stream);
+    k_lw_gate<<<(unsigned)lc, 256, 0, stream>>>(n, nm, D(ly.axm), D(ly.xm), D(ly.mu), IN(ly.sw), lo.tol, a, w, info,
+                                                sweeps, resid, fb_list, cnt, c0);
+    if ((err = cudaGetLastError()) != cudaSuccess) return err;
+  }
+  int hc[2] = {0, 0};
+  if ((err = cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, stream)) != cudaSuccess) return err;
+  if ((err = cudaStreamSynchronize(stream)) != cudaSuccess) return err;
+  if (hc[1] != 0) return cudaErrorLaunchFailure;
+  if (hc[0] > 0) {
+    if (!lo.fallback) {
+      k_ref_mark<<<(unsigned)((hc[0] + 255) / 256), 256, 0, stream>>>(hc[0], fb_list, info);
+      return cudaGetLastError();
+    }
+    long long *aoff = static_cast<long long *>(P(ly.aoff)), *woff = static_cast<long long *>(P(ly.woff));
+    k_ref_offsets<<<grid1(L), 256, 0, stream>>>(L, nm, n, aoff, woff);
+    eigen_GPU_batch_opts o32{};
+    o32.method = EIGEN_GPU_BATCH_TQL2;
+    o32.sort = 1;
+    o32.max_sweep = 100;
+    o32.chunk = (int)ly.Lc;
+    Indirect ix;
+    ix.kid = fb_list;
+    ix.aoff = aoff;
+    ix.woff = woff;
+    if ((err = run<float>(hc[0], nm, n, n, a, w, wk, ly.chunk_bytes, info, &o32, stream, nullptr, ix)) != cudaSuccess)
+      return err;
   }
   return cudaSuccess;
 }
@@ -1568,6 +2102,136 @@ cudaError_t eigen_GPU_batch_rayleigh_DP(const int L, const int nm, const int n, 
                                         double *s, double *g, void *wk, const size_t lwork, const cudaStream_t stream)
 {
   return eigb::run_rayleigh(L, nm, n, a, x, s, g, wk, lwork, stream);
+}
+
+cudaError_t eigen_GPU_mlp_size(const int d0, const int d1, const int d2, const int d3, size_t *bytes)
+{
+  if (!bytes) return cudaErrorInvalidValue;
+  *bytes = 0;
+  if (eigb::mlp_bad(d0, d1, d2, d3)) return cudaErrorInvalidValue;
+  *bytes = eigb::mlp_layout(d0, d1, d2, d3).bytes;
+  return cudaSuccess;
+}
+
+cudaError_t eigen_GPU_mlp_ws_size(const int d0, const int d1, const int d2, const int d3, const int rows, size_t *bytes)
+{
+  if (!bytes) return cudaErrorInvalidValue;
+  *bytes = 0;
+  if (eigb::mlp_bad(d0, d1, d2, d3) || rows < 8 || (rows % 8)) return cudaErrorInvalidValue;
+  *bytes = eigb::mlp_ws(eigb::mlp_layout(d0, d1, d2, d3), rows, true).bytes;
+  return cudaSuccess;
+}
+
+cudaError_t eigen_GPU_mlp_init(const int d0, const int d1, const int d2, const int d3, void *params,
+                               const unsigned long long seed, const cudaStream_t stream)
+{
+  if (eigb::mlp_bad(d0, d1, d2, d3) || !params) return cudaErrorInvalidValue;
+  return eigb::mlp_init(eigb::mlp_layout(d0, d1, d2, d3), params, seed, stream);
+}
+
+cudaError_t eigen_GPU_mlp_forward(const int d0, const int d1, const int d2, const int d3, const void *params,
+                                  const int rows, const float *x, float *y, void *ws, const size_t lws,
+                                  const cudaStream_t stream)
+{
+  if (eigb::mlp_bad(d0, d1, d2, d3) || rows < 8 || (rows % 8) || !params || !x || !y || !ws)
+    return cudaErrorInvalidValue;
+  const eigb::MlpLayout l = eigb::mlp_layout(d0, d1, d2, d3);
+  const eigb::MlpWs w = eigb::mlp_ws(l, rows, true);
+  if (lws != 0 && lws < w.bytes) return cudaErrorInvalidValue;
+  return eigb::mlp_forward(l, params, rows, x, y, static_cast<char *>(ws), w, false, stream);
+}
+
+cudaError_t eigen_GPU_mlp_gradient(const int d0, const int d1, const int d2, const int d3, const void *params,
+                                   const int rows, const float *x, const float *t, float *grad, double *sse,
+                                   void *ws, const size_t lws, const cudaStream_t stream)
+{
+  if (eigb::mlp_bad(d0, d1, d2, d3) || rows < 8 || (rows % 8) || !params || !x || !t || !grad || !ws)
+    return cudaErrorInvalidValue;
+  const eigb::MlpLayout l = eigb::mlp_layout(d0, d1, d2, d3);
+  const eigb::MlpWs w = eigb::mlp_ws(l, rows, true);
+  if (lws != 0 && lws < w.bytes) return cudaErrorInvalidValue;
+  char *wsp = static_cast<char *>(ws);
+  cudaError_t err = cudaMemsetAsync(wsp + w.err, 0, sizeof(int), stream);
+  if (err != cudaSuccess) return err;
+  if ((err = eigb::mlp_forward(l, params, rows, x, nullptr, wsp, w, true, stream)) != cudaSuccess) return err;
+  return eigb::mlp_backward(l, params, rows, t, grad, sse, wsp, w, stream);
+}
+
+cudaError_t eigen_GPU_mlp_train_step(const int d0, const int d1, const int d2, const int d3, void *params,
+                                     const int rows, const float *x, const float *t, const float lr, const int step,
+                                     double *sse, void *ws, const size_t lws, const cudaStream_t stream)
+{
+  if (eigb::mlp_bad(d0, d1, d2, d3) || rows < 8 || (rows % 8) || !params || !x || !t || !ws || step < 1)
+    return cudaErrorInvalidValue;
+  const eigb::MlpLayout l = eigb::mlp_layout(d0, d1, d2, d3);
+  const eigb::MlpWs w = eigb::mlp_ws(l, rows, true);
+  if (lws != 0 && lws < w.bytes) return cudaErrorInvalidValue;
+  char *wsp = static_cast<char *>(ws);
+  float *grad = reinterpret_cast<float *>(wsp + w.grad);
+  cudaError_t err;
+  if ((err = eigb::mlp_forward(l, params, rows, x, nullptr, wsp, w, true, stream)) != cudaSuccess) return err;
+  if ((err = eigb::mlp_backward(l, params, rows, t, grad, sse, wsp, w, stream)) != cudaSuccess) return err;
+  return eigb::mlp_adam(l, params, grad, lr, step, stream);
+}
+
+cudaError_t eigen_GPU_learned_targets_FP(const int L, const int n, const float *v, const int ldv, const float *v0,
+                                         float *c, const cudaStream_t stream)
+{
+  if (L < 1 || n < 1 || n > eigb::LW_NMAX || ldv < n || !v || !v0 || !c) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(float) * 2 * (size_t)n * n;
+  cudaError_t err = eigb::set_smem(eigb::k_lw_targets, smem);
+  if (err != cudaSuccess) return err;
+  eigb::k_lw_targets<<<(unsigned)L, 256, smem, stream>>>(n, v, ldv, v0, c);
+  return cudaGetLastError();
+}
+
+cudaError_t eigen_GPU_batch_learned_BufferSize_FP(const int L, const int nm, const int n, const int d1, const int d2,
+                                                  const eigen_GPU_learned_opts *opts, size_t *lwork)
+{
+  return eigb::lw_buffer_size(L, nm, n, d1, d2, opts, lwork);
+}
+
+cudaError_t eigen_GPU_batch_learned_FP(const int L, const int nm, const int n, float *a, float *w, const float *family,
+                                       const void *params, const int d1, const int d2, void *wk, const size_t lwork,
+                                       int *info, int *sweeps, double *resid, const eigen_GPU_learned_opts *opts,
+                                       const cudaStream_t stream)
+{
+  return eigb::run_learned(L, nm, n, a, w, family, params, d1, d2, wk, lwork, info, sweeps, resid, opts, stream);
+}
+
+cudaError_t eigen_GPU_batch_tune_set(const eigen_GPU_tune_entry *entries, const int count)
+{
+  if (count < 0 || (count > 0 && entries == nullptr)) return cudaErrorInvalidValue;
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  for (int i = 0; i < count; i++) {
+    const eigen_GPU_tune_entry &e = entries[i];
+    if ((e.esize != 4 && e.esize != 8) || e.n < 1 || e.n > 1024 || e.split < 0 || e.split > 32 ||
+        (e.zmem != EIGEN_GPU_ZMEM_AUTO && e.zmem != EIGEN_GPU_ZMEM_SHARED) || e.ql_mpw < 0 || e.ql_mpw > 32 ||
+        (e.ql_mpw & (e.ql_mpw - 1)) != 0)
+      return cudaErrorInvalidValue;
+  }
+  std::lock_guard<std::mutex> lk(eigb::g_mu);
+  for (auto it = eigb::g_tune.begin(); it != eigb::g_tune.end();) {
+    if (it->first.dev == dev) it = eigb::g_tune.erase(it);
+    else ++it;
+  }
+  for (int i = 0; i < count; i++) eigb::g_tune[eigb::TuneKey{dev, entries[i].esize, entries[i].n}] = entries[i];
+  return cudaSuccess;
+}
+
+cudaError_t eigen_GPU_batch_tune_get(const int esize, const int n, eigen_GPU_tune_entry *out)
+{
+  if (!out) return cudaErrorInvalidValue;
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  std::lock_guard<std::mutex> lk(eigb::g_mu);
+  auto it = eigb::g_tune.find(eigb::TuneKey{dev, esize, n});
+  if (it == eigb::g_tune.end()) return cudaErrorInvalidValue;
+  *out = it->second;
+  return cudaSuccess;
 }
 
 cudaError_t eigen_GPU_batch_trace(cudaEvent_t *events, const int nevents)

@@ -45,6 +45,21 @@ class RefineOpts(ctypes.Structure):
                 ("chunk", ctypes.c_int)]
 
 
+class LearnedOpts(ctypes.Structure):
+    """eigen_GPU_learned_opts of include/eigen_GPU_learned.h."""
+    _fields_ = [("warm", ctypes.c_int), ("max_sweeps", ctypes.c_int), ("tol", ctypes.c_double),
+                ("jacobi_tol", ctypes.c_double), ("fallback", ctypes.c_int), ("chunk", ctypes.c_int)]
+
+
+WARM_NETWORK, WARM_BASIS, WARM_IDENTITY = 0, 1, 2
+
+
+class TuneEntry(ctypes.Structure):
+    """eigen_GPU_tune_entry of include/eigen_GPU_batch.h."""
+    _fields_ = [("esize", ctypes.c_int), ("n", ctypes.c_int), ("split", ctypes.c_int), ("zmem", ctypes.c_int),
+                ("ql_mpw", ctypes.c_int)]
+
+
 def lib():
     """Load the CUDA library (raises if it has not been built)."""
     global _lib
@@ -109,6 +124,25 @@ def lib():
         L.eigen_GPU_batch_rayleigh_BufferSize_DP.restype = I
         L.eigen_GPU_batch_rayleigh_DP.argtypes = [I, I, I, P, P, P, P, P, SZ, P]
         L.eigen_GPU_batch_rayleigh_DP.restype = I
+        SZP = ctypes.POINTER(SZ)
+        L.eigen_GPU_mlp_size.argtypes = [I, I, I, I, SZP]
+        L.eigen_GPU_mlp_ws_size.argtypes = [I, I, I, I, I, SZP]
+        L.eigen_GPU_mlp_init.argtypes = [I, I, I, I, P, ctypes.c_ulonglong, P]
+        L.eigen_GPU_mlp_forward.argtypes = [I, I, I, I, P, I, P, P, P, SZ, P]
+        L.eigen_GPU_mlp_gradient.argtypes = [I, I, I, I, P, I, P, P, P, P, P, SZ, P]
+        L.eigen_GPU_mlp_train_step.argtypes = [I, I, I, I, P, I, P, P, ctypes.c_float, I, P, P, SZ, P]
+        L.eigen_GPU_learned_targets_FP.argtypes = [I, I, P, I, P, P, P]
+        L.eigen_GPU_batch_learned_BufferSize_FP.argtypes = [I, I, I, I, I, ctypes.POINTER(LearnedOpts), SZP]
+        L.eigen_GPU_batch_learned_FP.argtypes = [I, I, I, P, P, P, P, I, I, P, SZ, P, P, P,
+                                                 ctypes.POINTER(LearnedOpts), P]
+        for f in ("eigen_GPU_mlp_size", "eigen_GPU_mlp_ws_size", "eigen_GPU_mlp_init", "eigen_GPU_mlp_forward",
+                  "eigen_GPU_mlp_gradient", "eigen_GPU_mlp_train_step", "eigen_GPU_learned_targets_FP",
+                  "eigen_GPU_batch_learned_BufferSize_FP", "eigen_GPU_batch_learned_FP"):
+            getattr(L, f).restype = I
+        L.eigen_GPU_batch_tune_set.argtypes = [P, I]
+        L.eigen_GPU_batch_tune_set.restype = I
+        L.eigen_GPU_batch_tune_get.argtypes = [I, I, ctypes.POINTER(TuneEntry)]
+        L.eigen_GPU_batch_tune_get.restype = I
         L.eigen_GPU_batch_noalloc_DP.argtypes = [I, I, I, I, P, P, P, P]
         L.eigen_GPU_batch_noalloc_DP.restype = I
         L.eigen_GPU_batch_trace.argtypes = [P, I]
@@ -167,6 +201,10 @@ def exported_symbols():
         "eigen_GPU_batch_launch_params_DP", "eigen_GPU_batch_launch_params_FP",
         "eigen_GPU_batch_refine_DP", "eigen_GPU_batch_refine_BufferSize_DP",
         "eigen_GPU_batch_rayleigh_DP", "eigen_GPU_batch_rayleigh_BufferSize_DP",
+        "eigen_GPU_batch_tune_set", "eigen_GPU_batch_tune_get",
+        "eigen_GPU_mlp_size", "eigen_GPU_mlp_ws_size", "eigen_GPU_mlp_init", "eigen_GPU_mlp_forward",
+        "eigen_GPU_mlp_gradient", "eigen_GPU_mlp_train_step", "eigen_GPU_learned_targets_FP",
+        "eigen_GPU_batch_learned_BufferSize_FP", "eigen_GPU_batch_learned_FP",
         "eigen_GPU_batch_symfunc_DP", "eigen_GPU_batch_symfunc_FP",
         "eigen_GPU_batch_packed_DP", "eigen_GPU_batch_packed_FP",
         "eigen_GPU_batch_uneven_DP", "eigen_GPU_batch_uneven_FP",
@@ -347,6 +385,25 @@ def rayleigh(a, x, n, nm=None, want_s=True, want_g=True, stream=None):
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_rayleigh_DP failed with cudaError {st}")
     return s, g
+
+
+def tune_set(entries):
+    """eigen_GPU_batch_tune_set on the current device; entries: dicts with
+    esize, n, split, zmem, ql_mpw (an empty list clears the table)."""
+    arr = (TuneEntry * max(1, len(entries)))(*[TuneEntry(e["esize"], e["n"], e["split"], e["zmem"], e["ql_mpw"])
+                                               for e in entries])
+    st = lib().eigen_GPU_batch_tune_set(ctypes.cast(arr, ctypes.c_void_p), len(entries))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_tune_set failed with cudaError {st}")
+
+
+def tune_get(esize, n):
+    """The tuned entry for (esize, n) as a dict, or None."""
+    e = TuneEntry()
+    st = lib().eigen_GPU_batch_tune_get(esize, n, ctypes.byref(e))
+    if st != 0:
+        return None
+    return {"esize": e.esize, "n": e.n, "split": e.split, "zmem": e.zmem, "ql_mpw": e.ql_mpw}
 
 
 def packed_size(n):

@@ -184,8 +184,10 @@ cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, c
  *      integer slice products (Ozaki's splitting, 8 slices for the FP64-
  *      accurate ones) accumulated in FP64; clusters of close eigenvalues
  *      (up to 32) are resolved by an FP64 Rayleigh-Ritz step;
- *   3. a matrix converges when the largest correction between clusters is
- *      at most tol; it then leaves the later iterations.
+ *   3. a matrix converges when n max|E_ij|^2, E the correction between
+ *      clusters of its last update, is at most tol: the orthogonality defect
+ *      and residual that update leaves are of that order; it then leaves the
+ *      later iterations.
  * Matrices that do not converge within max_iter iterations, whose FP32
  * solve failed, or that have a cluster of more than 32 eigenvalues, are
  * solved again by the plain FP64 path (the fallback).  Results agree with
@@ -204,7 +206,7 @@ cudaError_t eigen_GPU_batch_noalloc_DP(const int L, const int nm, const int n, c
  */
 typedef struct eigen_GPU_refine_opts {
   int max_iter; /* refinement iterations at most; <= 0: 3 */
-  double tol;   /* convergence threshold on max |E_ij| between clusters; <= 0: 1e-7 */
+  double tol;   /* convergence threshold on n max|E_ij|^2; <= 0: 1e-14 */
   int fallback; /* 1: unconverged matrices are solved by the plain FP64 path (the
                    default when opts == NULL); 0: they are left unsolved, info -1 */
   int chunk;    /* matrices per internal chunk; <= 0: automatic (about 8 GiB) */
@@ -335,6 +337,29 @@ cudaError_t eigen_GPU_batch_launch_params_DP(const int L, const int n, int *grpS
                                              int *numTH, int *sizeSH, int *sizeL2);
 cudaError_t eigen_GPU_batch_launch_params_FP(const int L, const int n, int *grpSZ, int *numTB, int *numGR,
                                              int *numTH, int *sizeSH, int *sizeL2);
+
+/*
+ * Tuned options (no counterpart in the reference, whose launch parameters
+ * are fixed rules, eigen_GPU_batch.hpp:23-102): a table, per device and per
+ * (element size, order n), of the options a solve then uses wherever the
+ * caller leaves them automatic -- the apply phase's CTAs per matrix
+ * (split), where its rows live (zmem) and the QL phase's matrices per warp
+ * (ql_mpw).  None of these changes results, bit for bit; they change speed.
+ * eigeng_b200/autotune.py measures the candidates on the device and writes
+ * such a table.  eigen_GPU_batch_tune_set replaces the current device's
+ * table by `count` entries (0 clears it); it is global to the process.
+ * eigen_GPU_batch_tune_get returns the entry for (esize, n), or
+ * cudaErrorInvalidValue when there is none.
+ */
+typedef struct eigen_GPU_tune_entry {
+  int esize;  /* 4 (FP32) or 8 (FP64) */
+  int n;      /* matrix order, 1..1024 */
+  int split;  /* 0: automatic, else as eigen_GPU_batch_opts.split (1..32) */
+  int zmem;   /* EIGEN_GPU_ZMEM_AUTO or EIGEN_GPU_ZMEM_SHARED */
+  int ql_mpw; /* 0: automatic, else a power of two 1..32 */
+} eigen_GPU_tune_entry;
+cudaError_t eigen_GPU_batch_tune_set(const eigen_GPU_tune_entry *entries, const int count);
+cudaError_t eigen_GPU_batch_tune_get(const int esize, const int n, eigen_GPU_tune_entry *out);
 
 /*
  * Phase timing (counterpart of the reference's compile-time TIMER,
