@@ -48,6 +48,10 @@ def parse():
                     help="skip the n=32 (L=16384) and n=256 (L=2048) FP64 figures added to the line")
     ap.add_argument("--uneven", type=int, default=0,
                     help="mixed-size workload: this many matrices, n uniform in [8, 512], A = Q diag(l) Q^T")
+    ap.add_argument("--no-chosen", action="store_true",
+                    help="skip the refined (tensor-core) form against the plain form at n=32/128/256")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm start on the C5 family")
+    ap.add_argument("--learned-epochs", type=int, default=10)
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
     return ap.parse_args()
 
@@ -451,6 +455,151 @@ def run_uneven_bench(args):
             f.write(json.dumps(line) + "\n")
 
 
+def make_family_batch(torch, family, L, n, seed, device):
+    """FP64 batches of the metric's families on the device: 'symu' (B + B^T)/2
+    with B iid U[-1, 1], 'letkf' (n-1) I + Y^T Y, and 'clustered': Q diag(l)
+    Q^T with Q from the QR factorization of an iid N(0,1) matrix and l in
+    clusters of eight values 1e-8 apart, 0.1 between clusters."""
+    if family != "clustered":
+        return make_batch(torch, family, L, n, torch.float64, seed, device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    out = torch.empty((L, n, n), dtype=torch.float64, device=device)
+    idx = torch.arange(n, device=device, dtype=torch.float64)
+    lam = torch.floor(idx / 8) * 0.1 + torch.remainder(idx, 8) * 1e-8 + 1.0
+    for s in range(0, L, 256):
+        e = min(L, s + 256)
+        q, r = torch.linalg.qr(torch.randn((e - s, n, n), generator=g, dtype=torch.float64, device=device))
+        q = q * torch.sign(torch.diagonal(r, dim1=1, dim2=2))[:, None, :]
+        a = (q * lam[None, None, :]) @ q.transpose(1, 2)
+        out[s:e] = 0.5 * (a + a.transpose(1, 2))
+    return out
+
+
+def timed_solves(torch, base, steps, warmup, fn, stream):
+    """Device time (ms per solve) of fn over fresh copies of base."""
+    inp = FreshInputs(torch, base, steps + warmup)
+    last = None
+    for _ in range(warmup):
+        last = inp.next()
+        fn(last)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        fn(inp.next())
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / steps, last
+
+
+def chosen_vs_plain(torch, E, args, stream):
+    """The metric's comparison at n = 32, 128, 256 (FP64): the plain form
+    (tridiagonal + QL) against the refined form (FP32 solve, tensor-core
+    Ogita-Aishima refinement to FP64), same inputs, same timing rules; each
+    with the reference's gate (err1 residual, err2 orthogonality) on its
+    last warm-up result.  'chosen' is the faster at equal gate outcome."""
+    out = {}
+    steps = max(3, min(args.steps, 10))
+    for fam, n, L in (("symu", 32, 16384), ("letkf", 128, 4096), ("clustered", 256, 2048)):
+        base = make_family_batch(torch, fam, L, n, 4242, torch.device("cuda", torch.cuda.current_device()))
+        w = torch.empty((L, n), dtype=torch.float64, device=base.device)
+        info = torch.zeros(L, dtype=torch.int32, device=base.device)
+        wk = E.workspace(L, n, n, torch.float64, base.device)
+        ms_p, lp = timed_solves(torch, base, steps, 3, lambda a: E.eigen_GPU_batch_ex(a, w, wk, n, info=info,
+                                                                                      stream=stream), stream)
+        e1, e2, fl = E.check(base, w, lp, n)
+        plain = {"matrices_per_s": L / ms_p * 1e3, "ms": ms_p, "gate_flags": int((fl != 0).sum()),
+                 "max_err1": float(e1.max()), "max_err2": float(e2.max())}
+        del wk
+        rwk = E.refine_workspace(L, n, n, device=base.device)
+        holder = {}
+
+        def refined(a):
+            holder["w"], holder["info"], holder["it"] = E.solve_refined(a, n, wk=rwk, stream=stream)
+        ms_r, lr = timed_solves(torch, base, steps, 3, refined, stream)
+        e1, e2, fl = E.check(base, holder["w"], lr, n)
+        it = holder["it"].cpu().numpy()
+        ref = {"matrices_per_s": L / ms_r * 1e3, "ms": ms_r, "gate_flags": int((fl != 0).sum()),
+               "max_err1": float(e1.max()), "max_err2": float(e2.max()),
+               "iterations": np.bincount(it, minlength=4).tolist(), "fallback": int((it == 0).sum())}
+        del rwk
+        chosen = "refined" if (ref["matrices_per_s"] > plain["matrices_per_s"] and
+                               ref["gate_flags"] <= plain["gate_flags"]) else "plain"
+        out[f"{fam}_n{n}_f64_L{L}"] = {"plain": plain, "refined": ref, "chosen": chosen,
+                                       "chosen_matrices_per_s": max(plain["matrices_per_s"], ref["matrices_per_s"])
+                                       if chosen == "refined" else plain["matrices_per_s"]}
+        del base
+    return out
+
+
+def make_theta_family(torch, L, n, seed, device, family_seed=2024):
+    """The C5 family A(theta) = A0 + sum_j theta_j E_j (j = 1..4): A0 =
+    (G + G^T)/sqrt(2n) with G iid N(0,1), E_j = H_j + H_j^T scaled to unit
+    Frobenius norm, H_j iid N(0,1) (numpy generator with family_seed), theta
+    iid U[-0.1, 0.1] (seed).  Returns (A0, E, A as FP32 L x n x n)."""
+    rng = np.random.default_rng(family_seed)
+    gm = rng.standard_normal((n, n))
+    a0 = (gm + gm.T) / np.sqrt(2.0 * n)
+    e = np.empty((4, n, n))
+    for j in range(4):
+        h = rng.standard_normal((n, n))
+        h = h + h.T
+        e[j] = h / np.linalg.norm(h)
+    th = np.random.default_rng(seed).uniform(-0.1, 0.1, size=(L, 4))
+    a = a0[None] + np.einsum("lj,jik->lik", th, e)
+    return (torch.from_numpy(a0).to(device), torch.from_numpy(e).to(device),
+            torch.from_numpy(np.ascontiguousarray(a.astype(np.float32))).to(device))
+
+
+def learned_block(torch, E, args, stream):
+    """C5: 65536 FP32 matrices n = 64 of the theta family.  The network is
+    trained (200k solver-generated eigenpairs, the library's own kernels;
+    time reported, outside the timed solves), then the learned solve is
+    timed against the plain FP32 path and against the same polish started
+    from A0's eigenbasis or from the identity (the method without the
+    network)."""
+    import eigeng_b200.learned as lw
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n, L = 64, 65536
+    a0, e, base = make_theta_family(torch, L, n, 123, dev)
+    t0 = time.perf_counter()
+    v0 = lw.basis_eigenvectors(a0)
+    fam = lw.family_buffer(a0, e, v0)
+    x, t = lw.make_dataset(a0, e, v0, 200000, seed=11)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    net = lw.MLP(512, 512, n * n, seed=5)
+    t0 = time.perf_counter()
+    hist = lw.train(net, x, t, epochs=args.learned_epochs, batch=1024, lr=1e-3, lr_final=2e-5)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    del x, t
+    steps = max(3, min(args.steps, 10))
+    wk = E.workspace(L, n, n, torch.float32, dev)
+    w = torch.empty((L, n), dtype=torch.float32, device=dev)
+    ms_p, _ = timed_solves(torch, base, steps, 3, lambda a: E.eigen_GPU_batch_ex(a, w, wk, n, stream=stream), stream)
+    del wk
+    out = {"workload": f"theta family L={L} n={n} f32", "train": {"pairs": 200000, "epochs": args.learned_epochs,
+           "data_s": t_data, "train_s": t_train, "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1],
+           "widths": list(net.dims)},
+           "plain_fp32": {"matrices_per_s": L / ms_p * 1e3, "ms": ms_p}}
+    lwk = lw.learned_workspace(L, n, n, net.dims, device=dev)
+    for name, warm in (("network", lw.WARM_NETWORK), ("a0_basis", 1), ("identity", 2)):
+        holder = {}
+
+        def solve(a):
+            holder["r"] = lw.solve_learned(a, n, fam, net if warm == 0 else None, warm=warm, wk=lwk, stream=stream)
+        ms, _ = timed_solves(torch, base, steps, 3, solve, stream)
+        wv, info, sw, resid = holder["r"]
+        swn = sw.cpu().numpy()
+        ok = swn >= 0
+        out[name] = {"matrices_per_s": L / ms * 1e3, "ms": ms, "gate_pass": float(ok.mean()),
+                     "mean_sweeps": float(swn[ok].mean()) if ok.any() else None,
+                     "max_gate_residual": float(resid.max()), "info_nonzero": int((info != 0).sum())}
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -627,6 +776,11 @@ def main():
             sizes[f"n{n2}_f64_L{L2}"] = world * L2 * args.steps / (ms2 / 1000.0)
             del cps, wk2
         line["sizes"] = {"unit": "matrices/s", "data": "synthetic (B + B^T)/2, B iid U[-1,1]", **sizes}
+
+    if not args.no_chosen and world == 1:
+        line["chosen_vs_plain"] = chosen_vs_plain(torch, E, args, stream)
+    if not args.no_learned and world == 1:
+        line["learned"] = learned_block(torch, E, args, stream)
 
     if rank == 0 and world == 1 and not args.no_cpu:  # the CPU baseline is an N=1 figure
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

@@ -112,7 +112,7 @@ __device__ __forceinline__ void mm_load(const MmP &p, const bf16 *A, const bf16 
 
 __global__ void __launch_bounds__(MM_THREADS) k_mm_bf16(const MmP p)
 {
-  extern __shared__ __align__(1024) unsigned char mm_smem_raw[];
+  extern __shared__ __align__(16) unsigned char mm_smem_raw[];  // 1 KB alignment is done by hand below
   unsigned char *base = mm_smem_raw + ((1024 - (smem_u32(mm_smem_raw) & 1023)) & 1023);
   unsigned char *sbuf = base;  // MM_STAGES x (A tile, B tile), 16 KB each
   uint64_t *bars = reinterpret_cast<uint64_t *>(base + (size_t)MM_STAGES * 2 * MM_T * MM_KB * 2);

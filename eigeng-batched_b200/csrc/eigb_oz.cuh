@@ -318,6 +318,20 @@ __host__ __device__ inline OzGeom oz_geom(int sL, int sR, int dmax)
   return g;
 }
 
+// TMEM columns of a CTA: 256 per diagonal group (a power of two)
+__host__ __device__ inline int oz_tmem_cols(int groups) { return groups <= 1 ? 256 : 512; }
+
+// dynamic shared memory a launch of k_oz_gemm requests: its operands, and
+// enough of the SM's shared memory that the CTAs sharing an SM never ask
+// for more than its 512 TMEM columns together (an allocation would wait)
+__host__ inline size_t oz_launch_smem(size_t need, int groups, int smem_sm, int smem_rsv)
+{
+  const int per_sm = 512 / oz_tmem_cols(groups);  // CTAs whose columns fit together
+  const size_t floor_bytes = (size_t)smem_sm / (size_t)(per_sm + 1) + 1024;
+  (void)smem_rsv;
+  return need > floor_bytes ? need : floor_bytes;
+}
+
 // dynamic shared memory of k_oz_gemm: L slices of one K-block, the R slots,
 // 1 KB of barriers and column scales, 1 KB alignment slack
 __host__ __device__ inline size_t oz_gemm_smem(int sL, int sR, int KB, int dmax = 0)
@@ -338,7 +352,7 @@ __device__ __forceinline__ double pow2(int e)
 
 __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_gemm(const OzGemm p)
 {
-  extern __shared__ __align__(1024) unsigned char oz_smem[];
+  extern __shared__ __align__(16) unsigned char oz_smem[];  // 1 KB alignment is done by hand below
   const int tile = blockIdx.x;
   const long b = tile / (p.mtiles * p.ntiles);
   const int mt = (tile / p.ntiles) % p.mtiles;
@@ -375,7 +389,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_gemm(const OzGemm p)
     const int c = nt * OZ_NT + threadIdx.x;
     cscale[threadIdx.x] = c < p.n ? pow2(p.eR[b * p.RpR + c]) : 0.0;
   }
-  if (warp == 0) tmem_alloc(tslot, OZ_TMEM_COLS);
+  const int tcols = oz_tmem_cols(geo.groups);
+  if (warp == 0) tmem_alloc(tslot, tcols);
   tmem_fence_before();
   __syncthreads();
   tmem_fence_after();
@@ -477,7 +492,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) k_oz_gemm(const OzGemm p)
   }
   tmem_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, OZ_TMEM_COLS);
+  if (warp == 0) tmem_dealloc(tmem, tcols);
 }
 
 }  // namespace eigb

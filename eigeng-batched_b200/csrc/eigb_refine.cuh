@@ -13,7 +13,7 @@
 //        P = Af X, S = X^T P, G = X^T X   FP64-accurate int8 tensor-core
 //                                        products (eigb_oz.cuh, 8 slices)
 //        R = I - G;  lambda_i = s_ii / g_ii;  both S and R symmetrized
-//        delta = 2 (||S - diag S||_F + max|lambda| ||R||_F)
+//        delta = max(2 (||S - diag S||_F + max|lambda| ||R||_F), 1e-7 max|lambda|)
 //        clusters: runs of eigenvalues (in sorted order) with gaps <= delta
 //        E_ij = (s_ij + lambda_j r_ij) / (lambda_j - lambda_i) between
 //               clusters, r_ij / 2 inside a cluster      (k_oa_update)
@@ -46,6 +46,7 @@
 namespace eigb {
 
 constexpr int REF_CL_MAX = 32;  // largest cluster resolved in place
+constexpr double REF_DELTA_FLOOR = 1e-7;
 
 // ----------------------------------------------------------------- shift
 // One CTA (32 x 8 threads) per matrix: sigma, Af = A - sigma I and its FP32
@@ -232,7 +233,10 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
   off = blk_sum(off, red);
   rn = blk_sum(rn, red);
   am = blk_max(am, red);
-  const double delta = 2.0 * (sqrt(off) + am * sqrt(rn));
+  // eigenvalues closer than 1e-7 max|lambda| always go through the cluster
+  // Rayleigh-Ritz step (exact in S and R) rather than the division by
+  // their gap, whatever the iteration's corrections
+  const double delta = fmax(2.0 * (sqrt(off) + am * sqrt(rn)), REF_DELTA_FLOOR * am);
   if (!(delta <= 1.7976931348623157e308) || !(am <= 1.7976931348623157e308)) {  // NaN or Inf
     if (tid == 0) bad = 1;
   }

@@ -1153,8 +1153,7 @@ cudaError_t run_refine(long L, int nm, int n, double *a, double *w, void *wk, si
   // shared memory of the products: their operands, and at least half of
   // the SM so that no two of these CTAs (512 TMEM columns each) share an SM
   const size_t need = std::max(oz_gemm_smem(REF_S, REF_S, ly.KB, REF_DMAX), oz_gemm_smem(REF_SX, REF_SE, ly.KB, REF_DMAX_XE));
-  const size_t half = (size_t)dp.smem_sm / 2 + 1024;
-  const size_t gsm = std::min<size_t>(std::max(need, half), (size_t)dp.smem_optin);
+  const size_t gsm = std::min<size_t>(oz_launch_smem(need, 2, dp.smem_sm, dp.smem_rsv), (size_t)dp.smem_optin);
   if (need > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
   if ((err = set_smem(k_oz_gemm, gsm)) != cudaSuccess) return err;
   const size_t usm = ref_update_smem(n);
@@ -1323,7 +1322,7 @@ cudaError_t run_rayleigh(long L, int nm, int n, const double *a, const double *x
   rl.Kp = oz_kp(n);
   rl.KB = oz_kb(n);
   const size_t need = oz_gemm_smem(REF_S, REF_S, rl.KB, REF_DMAX);
-  const size_t gsm = std::min<size_t>(std::max(need, (size_t)dp.smem_sm / 2 + 1024), (size_t)dp.smem_optin);
+  const size_t gsm = std::min<size_t>(oz_launch_smem(need, 2, dp.smem_sm, dp.smem_rsv), (size_t)dp.smem_optin);
   if (need > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
   if ((err = set_smem(k_oz_gemm, gsm)) != cudaSuccess) return err;
   double *Af = static_cast<double *>(P(ly.af)), *Pm = static_cast<double *>(P(ly.p));
@@ -1711,7 +1710,7 @@ struct LwOpts {
   int warm = EIGEN_GPU_WARM_NETWORK;
   int max_sweeps = 10;
   double tol = 1e-6;
-  double jacobi_tol = 1e-10;
+  double jacobi_tol = 1e-7;
   int fallback = 1;
   int chunk = 0;
 };
@@ -1778,7 +1777,8 @@ cudaError_t run_learned(long L, int nm, int n, float *a, float *w, const float *
   rl.Kp = oz_kp(n);
   rl.KB = oz_kb(n);
   const size_t need = oz_gemm_smem(LW_S, LW_S, rl.KB, LW_DMAX);
-  const size_t gsm = std::min<size_t>(std::max(need, (size_t)dp.smem_sm / 2 + 1024), (size_t)dp.smem_optin);
+  const size_t gsm = std::min<size_t>(oz_launch_smem(need, oz_geom(LW_S, LW_S, LW_DMAX).groups, dp.smem_sm,
+                                                     dp.smem_rsv), (size_t)dp.smem_optin);
   if ((err = set_smem(k_oz_gemm, gsm)) != cudaSuccess) return err;
   const size_t psm = lw_polish_smem(n);
   if ((err = set_smem(k_lw_polish, psm)) != cudaSuccess) return err;

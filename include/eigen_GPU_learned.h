@@ -79,7 +79,7 @@ typedef struct eigen_GPU_learned_opts {
   int warm;          /* EIGEN_GPU_WARM_*; 0 by default */
   int max_sweeps;    /* Jacobi sweeps at most; <= 0: 10 */
   double tol;        /* gate: max_j ||A x_j - w_j x_j|| / max|w| at most this; <= 0: 1e-6 */
-  double jacobi_tol; /* Jacobi stops when off(B) <= jacobi_tol ||B||_F; <= 0: 1e-10 */
+  double jacobi_tol; /* Jacobi stops when off(B) <= jacobi_tol ||B||_F; <= 0: 1e-7 */
   int fallback;      /* 1 (default when opts == NULL): matrices that fail the gate are
                         solved by the plain path; 0: left unsolved, info -1 */
   int chunk;         /* matrices per internal chunk; <= 0: automatic (about 8 GiB) */

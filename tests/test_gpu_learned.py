@@ -118,9 +118,11 @@ def test_learned_solve_and_ablation(oracle_mod, family, trained):
         info, sweeps = info.cpu().numpy(), sweeps.cpu().numpy()
         r, o, dw = _check(oracle_mod, A, a.cpu().numpy(), w.cpu().numpy(), n)
         assert (info == 0).all()
-        assert r.max() <= 2e-6, (warm, r.max())       # the gate's 1e-6, plus the FP32 rounding of the output
-        assert o.max() <= 1e-5 and dw.max() <= 1e-5, (warm, o.max(), dw.max())
         passed = sweeps >= 0
+        # gate-passing matrices: the gate's 1e-6 plus the FP32 rounding of the
+        # output; the others come from the plain FP32 path, at its accuracy
+        assert r[passed].max() <= 2e-6, (warm, r[passed].max())
+        assert r.max() <= 2e-5 and o.max() <= 2e-5 and dw.max() <= 1e-5, (warm, r.max(), o.max(), dw.max())
         res[warm] = (passed.mean(), sweeps[passed].mean() if passed.any() else np.inf)
         print("warm", warm, "gate pass rate", res[warm][0], "mean sweeps", res[warm][1])
     assert res[0][0] >= 0.95
