@@ -23,11 +23,11 @@
 //        Rayleigh quotient of the corrected basis to first order;
 //        M = W diag(mu) W^T by FP64 Jacobi (one warp); X'_c <- X'_c W,
 //        lambda_c <- mu                          (k_cluster_apply)
-//      A matrix has converged when n max|E_ij|^2 (E between clusters) is at
-//      most tol (default 1e-14): the update then leaves a loss of
-//      orthogonality of about ten times that (X'^T X' - I = E^T E - ... to
-//      second order, as E + E^T = R exactly; the factor ten is measured) and
-//      a residual below it.  It then leaves the later iterations.  From
+//      A matrix has converged when n max|E_ij|^2 (all entries of E, the
+//      orthonormalising r_ij/2 included) is at most tol (default 1e-14):
+//      the update then leaves a loss of orthogonality of about ten times
+//      that (X'^T X' - I = E^T E - ... to second order, as E + E^T = R
+//      exactly; the factor ten is measured) and a residual below it.  It then leaves the later iterations.  From
 //      this library's FP32 eigenvectors (max|E| about 1e-3 on the first
 //      iteration for matrices with close eigenvalues, eps_32 ||A|| / gap)
 //      that takes two or three iterations.
@@ -120,7 +120,7 @@ struct RefP {
   int *act_out;         // active in the next iteration
   int *conv_it;         // iteration at which the matrix converged (0: not yet)
   int *fail;            // 1: to be solved by the fallback
-  double *emax;         // max |E| between clusters, per matrix (diagnostic)
+  double *emax;         // max |E_ij|, per matrix (diagnostic)
   double tol;
   int it;               // this iteration (1-based)
   int last;             // 1 on the last iteration
@@ -219,7 +219,11 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
   double *E = p.E + (size_t)b * n * n;
   const int tid = threadIdx.x;
   if (tid == 0) bad = 0;
-  for (int i = tid; i < n; i += 256) lam[i] = S[(size_t)i * n + i] / G[(size_t)i * n + i];
+  for (int i = tid; i < n; i += 256) {
+    const double v = S[(size_t)i * n + i] / G[(size_t)i * n + i];
+    if (!(fabs(v) <= 1.7976931348623157e308)) bad = 1;  // NaN or Inf: the matrix goes to the fallback
+    lam[i] = v;
+  }
   __syncthreads();
   double off = 0.0, rn = 0.0, am = 0.0;
   for (int i = tid; i < n; i += 256) am = fmax(am, fabs(lam[i]));
@@ -236,9 +240,19 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
   // eigenvalues closer than 1e-7 max|lambda| always go through the cluster
   // Rayleigh-Ritz step (exact in S and R) rather than the division by
   // their gap, whatever the iteration's corrections
-  const double delta = fmax(2.0 * (sqrt(off) + am * sqrt(rn)), REF_DELTA_FLOOR * am);
+  double delta = 2.0 * (sqrt(off) + am * sqrt(rn));
   if (!(delta <= 1.7976931348623157e308) || !(am <= 1.7976931348623157e308)) {  // NaN or Inf
     if (tid == 0) bad = 1;
+  }
+  delta = delta > REF_DELTA_FLOOR * am ? delta : REF_DELTA_FLOOR * am;
+  __syncthreads();
+  if (bad) {  // not finite: no ordering, clusters or update; the fallback solves it
+    if (tid == 0) {
+      p.emax[b] = 0.0;
+      p.act_out[b] = 0;
+      p.fail[b] = 1;
+    }
+    return;
   }
   // ascending order of the estimates (ties by index)
   for (int i = tid; i < n; i += 256) {
@@ -271,19 +285,16 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
     ncl = nc;
   }
   __syncthreads();
-  // E, and the largest entry between clusters
+  // E, and its largest entry: the update leaves errors of the order of its
+  // square, from the division by gaps and from the orthonormalisation
+  // (r/2) alike
   double em = 0.0;
   for (long idx = tid; idx < (long)n * n; idx += 256) {
     const int i = (int)(idx % n), j = (int)(idx / n);
     const double s = 0.5 * (S[(size_t)j * n + i] + S[(size_t)i * n + j]);
     const double r = (i == j ? 1.0 : 0.0) - 0.5 * (G[(size_t)j * n + i] + G[(size_t)i * n + j]);
-    double e;
-    if (cid[i] == cid[j]) {
-      e = 0.5 * r;
-    } else {
-      e = (s + lam[j] * r) / (lam[j] - lam[i]);
-      em = fmax(em, fabs(e));
-    }
+    const double e = (cid[i] == cid[j]) ? 0.5 * r : (s + lam[j] * r) / (lam[j] - lam[i]);
+    em = fmax(em, fabs(e));
     E[(size_t)j * n + i] = e;
   }
   em = blk_max(em, red);
@@ -348,21 +359,37 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
 // row of X' per thread.
 __global__ void __launch_bounds__(256) k_cluster_apply(const int n, double *__restrict__ X, const int *__restrict__ act,
                                                        const int *__restrict__ fail, const int *__restrict__ order,
-                                                       const int *__restrict__ cl, const double *__restrict__ W)
+                                                       const int *__restrict__ cl, const double *__restrict__ W,
+                                                       int *__restrict__ err)
 {
   __shared__ double ws[REF_CL_MAX * REF_CL_MAX];
   __shared__ int mem[REF_CL_MAX];
   const long b = blockIdx.x;
   if (!act[b] || fail[b]) return;
   double *Xb = X + (size_t)b * n * n;
+  __shared__ int badidx;
   for (int k0 = 0; k0 < n; k0++) {
     const int sz = cl[(size_t)b * n + k0];
     if (sz < 2) continue;
     __syncthreads();
+    if (threadIdx.x == 0) badidx = (sz > REF_CL_MAX || k0 + sz > n) ? 1 : 0;
+    __syncthreads();
+    if (badidx) {  // an inconsistent cluster table: record it, leave X as it is
+      if (threadIdx.x == 0 && err) atomicExch(err, 1);
+      return;
+    }
     for (int u = threadIdx.x; u < sz * REF_CL_MAX; u += blockDim.x)
       ws[u] = W[((size_t)b * n + k0) * REF_CL_MAX + u];
-    if (threadIdx.x < sz) mem[threadIdx.x] = order[(size_t)b * n + k0 + threadIdx.x];
+    if (threadIdx.x < sz) {
+      const int m = order[(size_t)b * n + k0 + threadIdx.x];
+      mem[threadIdx.x] = m;
+      if (m < 0 || m >= n) atomicExch(&badidx, 1);
+    }
     __syncthreads();
+    if (badidx) {
+      if (threadIdx.x == 0 && err) atomicExch(err, 1);
+      return;
+    }
     for (int r = threadIdx.x; r < n; r += blockDim.x) {
       double x[REF_CL_MAX];
 #pragma unroll

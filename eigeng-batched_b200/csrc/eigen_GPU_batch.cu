@@ -15,6 +15,7 @@
 #include <stdio.h>
 
 #include <algorithm>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -23,6 +24,7 @@
 #include "eigb_symfunc.cuh"
 #include "eigb_refine.cuh"
 #include "eigb_learned.cuh"
+#include "eigb_queue.cuh"
 #include "../../include/eigen_GPU_learned.h"
 #include "../../include/eigen_GPU_batch.h"
 
@@ -359,7 +361,6 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   if (first < 0 || count < 1 || first + count > L || sg.phases < 1 || sg.phases > EIGEN_GPU_STAGE_ALL)
     return cudaErrorInvalidValue;
   const bool ranged = first != 0 || count != L || sg.phases != EIGEN_GPU_STAGE_ALL;
-  if (ranged && ix.kid) return cudaErrorInvalidValue;
   int method = EIGEN_GPU_BATCH_TQL2, sort = 1, max_sweep = 100;
   if (opts) {
     method = opts->method;
@@ -683,22 +684,37 @@ cudaError_t run_interleaved(long L, int n, const T *ai, T *zi, T *wi, void *wk, 
 //
 // Matrix k has order n_k (1 <= n_k <= 1024), column-major with leading
 // dimension n_k at a + sum_{j<k} n_j^2; its eigenvalues at w + sum_{j<k} n_j.
-// The host groups the matrices by order; each group runs the three phases
-// like a uniform batch (reaching its members through an index list) on one
-// of a few streams, groups placed longest-first (cost count * n^3), so that
-// the latency-bound steps of one group overlap the work of others.
+// The host groups the matrices by order, largest first, and cuts the groups
+// into waves whose workspaces fit the budget together.  In each wave the
+// reduction of every group runs like a uniform batch (reaching its members
+// through an index list) on one of a pool of streams, groups placed
+// longest-first on the least loaded stream; then one persistent launch
+// (k2_ql_queue) runs the QL recurrence of every matrix of the wave from a
+// device work queue, longest first; then each group's apply phase runs on
+// its stream again.  Orders 1 and the Jacobi method are one pass each and
+// run beside the first wave's reductions.
 constexpr int kUnevenStreams = 32;
 
-struct UnevenGroup {
+struct UnevenItem {            // matrices start .. start+count-1 of the grouped index list, one order
   int n = 0, start = 0, count = 0, stream = 0;
+  bool single = false;         // n == 1 or the Jacobi method: one pass, no workspace
+  size_t ws_off = 0, ws_bytes = 0;  // workspace of the item within its wave's region
   eigen_GPU_batch_opts opts{};
+};
+struct UnevenWave {
+  int first = 0, count = 0;    // items
+  int job0 = 0, njobs = 0;     // jobs of the QL queue
+  int nmax = 0;                // largest order with a QL phase
 };
 struct UnevenPlan {
   std::vector<int> kid;  // matrix indices, grouped
   std::vector<long long> aoff, woff;
-  std::vector<UnevenGroup> groups;
-  int nstreams = 0;
-  size_t off_kid = 0, off_aoff = 0, off_woff = 0, off_slices = 0, slice = 0, bytes = 0;
+  std::vector<UnevenItem> items;
+  std::vector<UnevenWave> waves;
+  std::vector<QJob> jobs;
+  int nstreams = 0, mpw = 4, method = QL_TQL2, max_sweep = 100;
+  size_t off_kid = 0, off_aoff = 0, off_woff = 0, off_groups = 0, off_jobs = 0, off_next = 0, off_region = 0;
+  size_t region = 0, bytes = 0;
 };
 
 template <class T>
@@ -706,7 +722,10 @@ cudaError_t make_uneven_plan(long L, const int *n_host, const eigen_GPU_batch_op
 {
   if (L < 1 || n_host == nullptr) return cudaErrorInvalidValue;
   const int method = opts ? opts->method : EIGEN_GPU_BATCH_TQL2;
-  std::map<int, std::vector<int>> by_n;
+  if (method < EIGEN_GPU_BATCH_TQL2 || method > EIGEN_GPU_BATCH_JACOBI) return cudaErrorInvalidValue;
+  if (opts && opts->ql_mpw > 0 && (opts->ql_mpw > 32 || (opts->ql_mpw & (opts->ql_mpw - 1)) != 0))
+    return cudaErrorInvalidValue;
+  std::map<int, std::vector<int>, std::greater<int>> by_n;  // largest order first
   up.aoff.resize(L);
   up.woff.resize(L);
   long long ao = 0, wo = 0;
@@ -723,44 +742,108 @@ cudaError_t make_uneven_plan(long L, const int *n_host, const eigen_GPU_batch_op
   DevProps dp;
   cudaError_t err = dev_props(dp);
   if (err != cudaSuccess) return err;
+  up.method = method == EIGEN_GPU_BATCH_IMTQL2 ? QL_IMTQL2 : QL_TQL2;
+  if (opts && opts->max_sweep > 0) up.max_sweep = opts->max_sweep;
+  if (opts && opts->ql_mpw > 0) up.mpw = opts->ql_mpw;
+  // items: whole groups, or parts of a group whose workspace alone is over
+  // the budget; single-pass groups go to the first wave
+  std::vector<UnevenItem> multi, single;
   for (auto &g : by_n) {
-    UnevenGroup ug;
-    ug.n = g.first;
-    ug.start = (int)up.kid.size();
-    ug.count = (int)g.second.size();
+    UnevenItem it;
+    it.n = g.first;
+    it.start = (int)up.kid.size();
+    it.count = (int)g.second.size();
     up.kid.insert(up.kid.end(), g.second.begin(), g.second.end());
-    up.groups.push_back(ug);
-  }
-  // longest first onto the least loaded stream
-  std::sort(up.groups.begin(), up.groups.end(), [](const UnevenGroup &x, const UnevenGroup &y) {
-    return (double)x.count * x.n * x.n * x.n > (double)y.count * y.n * y.n * y.n;
-  });
-  up.nstreams = (int)std::min<size_t>(kUnevenStreams, up.groups.size());
-  std::vector<double> load(up.nstreams, 0.0);
-  std::vector<size_t> need(up.nstreams, 0);
-  const size_t cap = kWsBudget / kUnevenStreams;  // workspace per stream
-  for (auto &g : up.groups) {
-    const int s = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-    g.stream = s;
-    load[s] += (double)g.count * g.n * g.n * g.n;
-    g.opts = opts ? *opts : eigen_GPU_batch_opts{};
-    if (!opts) g.opts.sort = 1;
-    // groups solve concurrently: the QL phase at four matrices per warp
-    // leaves the other groups' kernels their issue slots (measured on B200,
-    // 10000 matrices of n ~ U[8,512] FP64: 1.40 s against 1.46 s)
-    if (g.opts.ql_mpw <= 0 && up.nstreams > 1) g.opts.ql_mpw = 4;
-    if (g.n == 1 || method == EIGEN_GPU_BATCH_JACOBI) continue;  // no workspace
-    Plan<T> one;
-    eigen_GPU_batch_opts o1 = g.opts;
+    it.opts = opts ? *opts : eigen_GPU_batch_opts{};
+    if (!opts) {
+      it.opts.method = EIGEN_GPU_BATCH_TQL2;
+      it.opts.sort = 1;
+      it.opts.max_sweep = 100;
+    }
+    if (it.n == 1 || method == EIGEN_GPU_BATCH_JACOBI) {
+      it.single = true;
+      single.push_back(it);
+      continue;
+    }
+    // the plan run() makes for one matrix of this order, tuned as it tunes
+    eigen_GPU_batch_opts t1;
+    eigen_GPU_batch_opts o1 = *tuned(&it.opts, (int)sizeof(T), it.n, t1);
     o1.chunk = 1;
-    if ((err = make_plan<T>(1, g.n, g.n, dp, one, &o1)) != cudaSuccess) return err;
-    const long fit = std::max<long>(1, (long)(cap / one.bytes));
-    g.opts.chunk = (int)std::min<long>(g.count, std::min<long>(fit, 1L << 30));
-    Plan<T> pl;
-    if ((err = make_plan<T>(g.count, g.n, g.n, dp, pl, &g.opts)) != cudaSuccess) return err;
-    need[s] = std::max(need[s], pl.bytes);
+    Plan<T> one;
+    if ((err = make_plan<T>(1, it.n, it.n, dp, one, &o1)) != cudaSuccess) return err;
+    long fit = std::max<long>(1, (long)(kWsBudget / one.bytes));
+    if (opts && opts->chunk > 0) fit = std::min<long>(fit, opts->chunk);
+    for (int s0 = 0; s0 < it.count; s0 += (int)std::min<long>(fit, it.count)) {
+      UnevenItem part = it;
+      part.start = it.start + s0;
+      part.count = (int)std::min<long>(fit, it.count - s0);
+      multi.push_back(part);
+    }
   }
-  up.slice = align256(*std::max_element(need.begin(), need.end()));
+  // waves: consecutive items (decreasing order) while their workspaces fit
+  // the budget together, and at most opts->chunk matrices when it is set
+  up.nstreams = 1;
+  size_t used = 0;
+  long in_wave = 0;
+  const long wave_cap = (opts && opts->chunk > 0) ? opts->chunk : (1L << 40);
+  UnevenWave wv;
+  auto close_wave = [&]() {
+    if (wv.count > 0) up.waves.push_back(wv);
+    wv = UnevenWave();
+    wv.first = (int)up.items.size();
+    used = 0;
+    in_wave = 0;
+  };
+  close_wave();
+  for (UnevenItem it : multi) {
+    eigen_GPU_batch_opts t1;
+    eigen_GPU_batch_opts oc = *tuned(&it.opts, (int)sizeof(T), it.n, t1);
+    oc.chunk = it.count;
+    Plan<T> pl;
+    if ((err = make_plan<T>(it.count, it.n, it.n, dp, pl, &oc)) != cudaSuccess) return err;
+    const size_t b = align256(pl.bytes);
+    if (wv.count > 0 && (used + b > kWsBudget || in_wave + it.count > wave_cap)) close_wave();
+    it.opts.chunk = it.count;
+    it.ws_off = used;
+    it.ws_bytes = pl.bytes;
+    used += b;
+    in_wave += it.count;
+    up.region = std::max(up.region, used);
+    up.items.push_back(it);
+    wv.count++;
+  }
+  close_wave();
+  for (UnevenItem it : single) up.items.push_back(it);  // after the waves' items
+  // streams: within a wave (and for the single-pass items, with the first
+  // wave), longest first onto the least loaded stream
+  const int nwaves = (int)up.waves.size();
+  for (int wi = 0; wi < std::max(1, nwaves); wi++) {
+    std::vector<int> idx;
+    if (wi < nwaves)
+      for (int i = 0; i < up.waves[wi].count; i++) idx.push_back(up.waves[wi].first + i);
+    if (wi == 0)
+      for (int i = (int)up.items.size() - (int)single.size(); i < (int)up.items.size(); i++) idx.push_back(i);
+    auto cost = [&](int i) { return (double)up.items[i].count * up.items[i].n * up.items[i].n * up.items[i].n; };
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    const int ns = (int)std::min<size_t>(kUnevenStreams, idx.size());
+    up.nstreams = std::max(up.nstreams, ns);
+    std::vector<double> load(std::max(ns, 1), 0.0);
+    for (int i : idx) {
+      const int s = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      up.items[i].stream = s;
+      load[s] += cost(i);
+    }
+  }
+  // the QL queue of each wave: its items' matrices in item order (items are
+  // in decreasing order of n already)
+  for (UnevenWave &w : up.waves) {
+    w.job0 = (int)up.jobs.size();
+    for (int i = w.first; i < w.first + w.count; i++) {
+      w.nmax = std::max(w.nmax, up.items[i].n);
+      for (int k = 0; k < up.items[i].count; k++) up.jobs.push_back(QJob{i, k});
+    }
+    w.njobs = (int)up.jobs.size() - w.job0;
+  }
   size_t off = 0;
   up.off_kid = off;
   off = align256(off + sizeof(int) * (size_t)L);
@@ -768,8 +851,14 @@ cudaError_t make_uneven_plan(long L, const int *n_host, const eigen_GPU_batch_op
   off = align256(off + sizeof(long long) * (size_t)L);
   up.off_woff = off;
   off = align256(off + sizeof(long long) * (size_t)L);
-  up.off_slices = off;
-  up.bytes = off + up.slice * up.nstreams;
+  up.off_groups = off;
+  off = align256(off + sizeof(QGroup<T>) * up.items.size());
+  up.off_jobs = off;
+  off = align256(off + sizeof(QJob) * std::max<size_t>(1, up.jobs.size()));
+  up.off_next = off;
+  off = align256(off + sizeof(int) * std::max<size_t>(1, up.waves.size()));
+  up.off_region = off;
+  up.bytes = off + up.region;
   return cudaSuccess;
 }
 
@@ -801,6 +890,37 @@ cudaError_t uneven_buffer_size(long L, const int *n_host, const eigen_GPU_batch_
   return err;
 }
 
+// Launch of the QL queue of one wave on st: matrices per warp up.mpw,
+// warps per block within 96 KB of slots, one resident wave of blocks.
+template <class T>
+cudaError_t launch_ql_queue(const UnevenPlan &up, const UnevenWave &wv, const QGroup<T> *groups,
+                            const QJob *jobs, int *next, cudaStream_t st)
+{
+  if (wv.njobs < 1) return cudaSuccess;
+  DevProps dp;
+  cudaError_t err = dev_props(dp);
+  if (err != cudaSuccess) return err;
+  const size_t per = queue_slot_bytes<T>(wv.nmax);
+  const size_t budget = std::min<size_t>((size_t)dp.smem_optin, 96 * 1024);
+  int mpw = up.mpw;
+  int warps = (int)std::min<size_t>(std::max(1, std::min(K2_MAX_WARPS, 32 / mpw)), budget / (per * mpw));
+  if (warps < 1) {  // one slot per warp
+    mpw = 1;
+    warps = (int)std::min<size_t>(K2_MAX_WARPS, std::max<size_t>(1, budget / per));
+    if (per > (size_t)dp.smem_optin) return cudaErrorInvalidValue;
+  }
+  const size_t smem = per * (size_t)mpw * warps;
+  if ((err = set_smem(k2_ql_queue<T>, smem)) != cudaSuccess) return err;
+  int nb = 0;
+  if ((err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k2_ql_queue<T>, 32 * warps, smem)) != cudaSuccess)
+    return err;
+  const long need = (wv.njobs + (long)mpw * warps - 1) / ((long)mpw * warps);
+  const long blocks = std::max<long>(1, std::min<long>(need, (long)std::max(nb, 1) * dp.sms));
+  k2_ql_queue<T><<<(unsigned)blocks, 32 * warps, smem, st>>>(groups, jobs + wv.job0, wv.njobs, next, mpw, wv.nmax,
+                                                               up.method, up.max_sweep);
+  return cudaGetLastError();
+}
+
 template <class T>
 cudaError_t run_uneven(long L, const int *n_host, T *a, T *w, void *wk, size_t lwork, int *info,
                        const eigen_GPU_batch_opts *opts, cudaStream_t stream)
@@ -814,6 +934,32 @@ cudaError_t run_uneven(long L, const int *n_host, T *a, T *w, void *wk, size_t l
   int *d_kid = reinterpret_cast<int *>(base + up.off_kid);
   long long *d_aoff = reinterpret_cast<long long *>(base + up.off_aoff);
   long long *d_woff = reinterpret_cast<long long *>(base + up.off_woff);
+  QGroup<T> *d_groups = reinterpret_cast<QGroup<T> *>(base + up.off_groups);
+  QJob *d_jobs = reinterpret_cast<QJob *>(base + up.off_jobs);
+  int *d_next = reinterpret_cast<int *>(base + up.off_next);
+  char *region = base + up.off_region;
+  // each item's workspace slots, as run() lays them out for its plan
+  std::vector<QGroup<T>> qg(up.items.size());
+  {
+    DevProps dp;
+    if ((err = dev_props(dp)) != cudaSuccess) return err;
+    for (size_t i = 0; i < up.items.size(); i++) {
+      const UnevenItem &it = up.items[i];
+      if (it.single) continue;
+      eigen_GPU_batch_opts t1;
+      const eigen_GPU_batch_opts *o = tuned(&it.opts, (int)sizeof(T), it.n, t1);
+      Plan<T> pl;
+      if ((err = make_plan<T>(it.count, it.n, it.n, dp, pl, o)) != cudaSuccess) return err;
+      if (pl.Lc < it.count || pl.bytes != it.ws_bytes) return cudaErrorInvalidValue;  // not reached
+      char *ws = region + it.ws_off;
+      qg[i].d = reinterpret_cast<T *>(ws + pl.off_d);
+      qg[i].e = reinterpret_cast<T *>(ws + pl.off_e);
+      qg[i].meta = reinterpret_cast<Meta *>(ws + pl.off_meta);
+      qg[i].rec = reinterpret_cast<Rec<T> *>(ws + pl.off_rec);
+      qg[i].n = it.n;
+      qg[i].rcap = pl.rcap;
+    }
+  }
   // from pageable host memory: the copies are staged before these calls return
   if ((err = cudaMemcpyAsync(d_kid, up.kid.data(), sizeof(int) * (size_t)L, cudaMemcpyHostToDevice, stream)) ||
       (err = cudaMemcpyAsync(d_aoff, up.aoff.data(), sizeof(long long) * (size_t)L, cudaMemcpyHostToDevice,
@@ -821,31 +967,64 @@ cudaError_t run_uneven(long L, const int *n_host, T *a, T *w, void *wk, size_t l
       (err = cudaMemcpyAsync(d_woff, up.woff.data(), sizeof(long long) * (size_t)L, cudaMemcpyHostToDevice,
                              stream)))
     return err;
+  if (!up.items.empty() &&
+      (err = cudaMemcpyAsync(d_groups, qg.data(), sizeof(QGroup<T>) * qg.size(), cudaMemcpyHostToDevice, stream)))
+    return err;
+  if (!up.jobs.empty() &&
+      (err = cudaMemcpyAsync(d_jobs, up.jobs.data(), sizeof(QJob) * up.jobs.size(), cudaMemcpyHostToDevice, stream)))
+    return err;
+  if ((err = cudaMemsetAsync(d_next, 0, sizeof(int) * std::max<size_t>(1, up.waves.size()), stream))) return err;
   cudaStream_t st[kUnevenStreams];
   if ((err = uneven_streams(up.nstreams, st)) != cudaSuccess) return err;
-  cudaEvent_t ev;
-  if ((err = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return err;
-  cudaEventRecord(ev, stream);  // the index lists and everything before on the caller's stream
-  for (int i = 0; i < up.nstreams; i++) cudaStreamWaitEvent(st[i], ev, 0);
-  cudaEventDestroy(ev);
-  for (const UnevenGroup &g : up.groups) {
+  // one event per pool stream (joins) and one on the caller's stream (forks);
+  // an event may be recorded again once the waits on it are enqueued
+  cudaEvent_t ev[kUnevenStreams + 1];
+  int nev = 0;
+  for (; nev <= up.nstreams; nev++)
+    if ((err = cudaEventCreateWithFlags(&ev[nev], cudaEventDisableTiming)) != cudaSuccess) break;
+  auto fork = [&]() {
+    cudaEventRecord(ev[up.nstreams], stream);
+    for (int i = 0; i < up.nstreams; i++) cudaStreamWaitEvent(st[i], ev[up.nstreams], 0);
+  };
+  auto join = [&]() {
+    for (int i = 0; i < up.nstreams; i++) {
+      cudaEventRecord(ev[i], st[i]);
+      cudaStreamWaitEvent(stream, ev[i], 0);
+    }
+  };
+  auto stage = [&](const UnevenItem &it, int phases) {
     Indirect ix;
-    ix.kid = d_kid + g.start;
+    ix.kid = d_kid + it.start;
     ix.aoff = d_aoff;
     ix.woff = d_woff;
-    void *slice = base + up.off_slices + up.slice * g.stream;
-    err = run<T>(g.count, g.n, g.n, g.n, a, w, slice, up.slice, info, &g.opts, st[g.stream], nullptr, ix);
-    if (err != cudaSuccess) break;
+    Stage sg;
+    sg.phases = phases;
+    return run<T>(it.count, it.n, it.n, it.n, a, w, it.single ? nullptr : region + it.ws_off, it.ws_bytes, info,
+                  &it.opts, st[it.stream], nullptr, ix, sg);
+  };
+  if (err == cudaSuccess) {
+    fork();
+    const int nwaves = (int)up.waves.size();
+    for (const UnevenItem &it : up.items)  // single-pass groups beside the first wave
+      if (it.single && err == cudaSuccess) err = stage(it, EIGEN_GPU_STAGE_ALL);
+    for (int wi = 0; wi < nwaves && err == cudaSuccess; wi++) {
+      const UnevenWave &wv = up.waves[wi];
+      if (wi > 0) {  // the previous wave's apply phase is done with the region
+        join();
+        fork();
+      }
+      for (int i = wv.first; i < wv.first + wv.count && err == cudaSuccess; i++)
+        err = stage(up.items[i], EIGEN_GPU_STAGE_REDUCE);
+      if (err != cudaSuccess) break;
+      join();
+      if ((err = launch_ql_queue<T>(up, wv, d_groups, d_jobs, d_next + wi, stream)) != cudaSuccess) break;
+      fork();
+      for (int i = wv.first; i < wv.first + wv.count && err == cudaSuccess; i++)
+        err = stage(up.items[i], EIGEN_GPU_STAGE_APPLY);
+    }
+    join();  // the caller's stream waits for every pool stream
   }
-  // the caller's stream waits for every group stream
-  for (int i = 0; i < up.nstreams; i++) {
-    cudaEvent_t done;
-    cudaError_t e2 = cudaEventCreateWithFlags(&done, cudaEventDisableTiming);
-    if (e2 != cudaSuccess) return e2;
-    cudaEventRecord(done, st[i]);
-    cudaStreamWaitEvent(stream, done, 0);
-    cudaEventDestroy(done);
-  }
+  for (int i = 0; i < nev; i++) cudaEventDestroy(ev[i]);
   return err;
 }
 
@@ -1215,7 +1394,7 @@ cudaError_t run_refine(long L, int nm, int n, double *a, double *w, void *wk, si
       ref_slice(ly, lc, Xs, xf32, 1, n, REF_SX, XR, eXR, ain, stream);           // rows of X
       ref_slice(ly, lc, PE, 0, n, 1, REF_SE, ES, eE, ain, stream);               // columns of E
       ref_gemm(ly, lc, XR, eXR, REF_SX, ES, eE, REF_SE, REF_DMAX_XE, Xd, Xs, xf32, ain, errf, gsm, stream);
-      k_cluster_apply<<<(unsigned)lc, 256, 0, stream>>>(n, Xd, ain, fail, rp.order, rp.cl, rp.W);
+      k_cluster_apply<<<(unsigned)lc, 256, 0, stream>>>(n, Xd, ain, fail, rp.order, rp.cl, rp.W, errf);
       if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
     k_ref_final<<<(unsigned)lc, 256, fsm, stream>>>(n, nm, a, w, info, XB[0], XB[1],

@@ -463,17 +463,19 @@ def solve_interleaved(ai, n, method=TQL2, sort=True, max_sweep=100, stream=None)
     return zi, wi, info
 
 
-def solve_uneven(a, ns, method=TQL2, sort=True, max_sweep=100, stream=None, zmem=ZMEM_AUTO, ql_mpw=0):
+def solve_uneven(a, ns, method=TQL2, sort=True, max_sweep=100, stream=None, zmem=ZMEM_AUTO, ql_mpw=0, wave=0,
+                 rec_cap=0):
     """eigen_GPU_batch_uneven: a is a flat CUDA tensor holding matrix k
     (order ns[k], column-major, leading dimension ns[k]) at offset
     sum_{j<k} ns[j]^2; solved in place.  Returns (w, info), w flat with the
-    eigenvalues of matrix k at sum_{j<k} ns[j]."""
+    eigenvalues of matrix k at sum_{j<k} ns[j].  wave > 0 caps the matrices
+    solved together (opts.chunk), and so the workspace."""
     nsa = (ctypes.c_int * len(ns))(*[int(x) for x in ns])
     L = len(ns)
     tot = sum(int(x) * int(x) for x in ns)
     if not a.is_cuda or not a.is_contiguous() or a.numel() != tot:
         raise EigenGError("a must be a contiguous CUDA tensor of sum(n^2) elements")
-    o = Opts(method, 1 if sort else 0, max_sweep, 0, 0, 0, zmem, ql_mpw)
+    o = Opts(method, 1 if sort else 0, max_sweep, int(rec_cap), int(wave), 0, zmem, ql_mpw)
     sfx = _sfx(a.dtype)
     lw = ctypes.c_size_t(0)
     st = getattr(lib(), "eigen_GPU_batch_uneven_BufferSize_" + sfx)(L, nsa, ctypes.byref(o), ctypes.byref(lw))

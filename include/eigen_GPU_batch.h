@@ -281,12 +281,18 @@ cudaError_t eigen_GPU_batch_interleaved_FP(const int L, const int n, const float
  * order n[k] (1..1024, n is a HOST array of L ints) and is stored
  * column-major with leading dimension n[k] at a + sum_{j<k} n[j]^2; its
  * eigenvalues go to w + sum_{j<k} n[j] and its status to info[k] (device,
- * optional).  The matrices are grouped by order and the groups run
- * concurrently on internal streams; the call is asynchronous with respect to
- * the host except for three small index copies from host memory, and the
- * caller's stream waits for all of it.  Results equal eigen_GPU_batch_ex_*
- * on each matrix.  Options as eigen_GPU_batch_ex_* (chunk is chosen per
- * group); lwork from eigen_GPU_batch_uneven_BufferSize_*.
+ * optional).  The matrices are grouped by order, largest first, and cut
+ * into waves whose workspaces fit an 8 GB budget together (opts->chunk > 0
+ * also caps the matrices of a wave, and so the workspace).  In each wave
+ * the groups' reductions run concurrently on internal streams, then one
+ * persistent launch runs the QL phase of every matrix of the wave from a
+ * device work queue (longest first, opts->ql_mpw matrices per warp, 4 by
+ * default), then the groups' apply phases run concurrently again.  The call
+ * is asynchronous with respect to the host except for small index copies
+ * from host memory, and the caller's stream waits for all of it.  Results
+ * equal eigen_GPU_batch_ex_* on each matrix, bit for bit.  Other options as
+ * eigen_GPU_batch_ex_*; lwork from eigen_GPU_batch_uneven_BufferSize_*
+ * with the same options.
  * Limits: the index lists are copied from pageable host memory, so a call
  * cannot be captured in a CUDA graph; the group streams are a pool per
  * device shared by every caller of the library, so concurrent uneven calls

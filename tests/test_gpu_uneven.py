@@ -14,12 +14,12 @@ def E():
     return eigeng_b200
 
 
-def _check(O, ns, dtype, method=0, seed=0):
+def _check(O, ns, dtype, method=0, seed=0, **kw):
     rng = np.random.default_rng(seed)
     mats = [O.sym_uniform(1, int(n), seed=int(rng.integers(1 << 30)))[0].astype(dtype) for n in ns]
     flat = np.concatenate([m.reshape(-1) for m in mats])
     a = torch.from_numpy(flat.copy()).cuda()
-    w, info = E().solve_uneven(a, ns, method=method)
+    w, info = E().solve_uneven(a, ns, method=method, **kw)
     torch.cuda.synchronize()
     ao = np.cumsum([0] + [int(n) * int(n) for n in ns])
     wo = np.cumsum([0] + [int(n) for n in ns])
@@ -27,7 +27,7 @@ def _check(O, ns, dtype, method=0, seed=0):
     for n in sorted(set(int(x) for x in ns)):
         idx = [k for k, x in enumerate(ns) if int(x) == n]
         ref = torch.from_numpy(np.stack([mats[k] for k in idx])).cuda()
-        wr, ir = E().solve(ref, n, method=method)
+        wr, ir = E().solve(ref, n, method=method, rec_cap=kw.get("rec_cap", 0))
         torch.cuda.synchronize()
         refn, wrn = ref.cpu().numpy(), wr.cpu().numpy()
         for j, k in enumerate(idx):
@@ -42,6 +42,26 @@ def test_uneven_matches_uniform(oracle_mod, dtype):
     ns = list(rng.integers(1, 300, size=70)) + [1, 2, 32, 33, 128, 129, 256, 256, 5, 5, 5]
     rng.shuffle(ns)
     _check(oracle_mod, ns, dtype, seed=2)
+
+
+@pytest.mark.parametrize("wave,mpw", [(7, 0), (40, 1), (1, 32)])
+def test_uneven_waves_and_queue_widths(oracle_mod, wave, mpw):
+    """Waves of at most `wave` matrices (groups cut across waves, the
+    workspace reused), and the QL queue at 1 and 32 matrices per warp:
+    the same bits as the uniform solve."""
+    rng = np.random.default_rng(4)
+    ns = [int(x) for x in rng.integers(2, 200, size=30)] + [1, 1, 64, 64, 64, 64, 64, 64, 64, 64, 64]
+    rng.shuffle(ns)
+    _check(oracle_mod, ns, np.float64, seed=5, wave=wave, ql_mpw=mpw)
+
+
+def test_uneven_imtql2_and_overflowing_records(oracle_mod):
+    """imtql2 through the queue; and every matrix's records overflowing a
+    small capacity (rec_cap), which the apply phase then regenerates."""
+    rng = np.random.default_rng(8)
+    ns = [int(x) for x in rng.integers(2, 150, size=20)]
+    _check(oracle_mod, ns, np.float64, method=1, seed=9)
+    _check(oracle_mod, ns, np.float64, method=0, seed=10, rec_cap=8)
 
 
 def test_uneven_jacobi_and_errors(oracle_mod):
