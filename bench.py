@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--L", type=int, default=4096)
     ap.add_argument("--dtype", default="f64", choices=["f64", "f32"])
-    ap.add_argument("--family", default="letkf", choices=["letkf", "symu"])
+    ap.add_argument("--family", default="letkf", choices=["letkf", "symu", "clustered"])
     ap.add_argument("--method", default="tql2", choices=["tql2", "imtql2", "jacobi"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -52,6 +52,9 @@ def parse():
                     help="skip the refined (tensor-core) form against the plain form at n=32/128/256")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm start on the C5 family")
     ap.add_argument("--learned-epochs", type=int, default=10)
+    ap.add_argument("--form", default="plain", choices=["plain", "refined", "learned"],
+                    help="the solver form timed: the plain solve (default), the refined FP32->FP64 form on "
+                         "--family/--n/--L, or the learned warm start on the theta family (--L matrices, n = 64)")
     ap.add_argument("--out", default=None, help="also append the JSON line to this file")
     return ap.parse_args()
 
@@ -146,6 +149,8 @@ class ClockSampler:
 def make_batch(torch, family, L, n, dtype, seed, device):
     """Seeded synthetic batch generated on the device (column-major matrices,
     symmetric).  LETKF-style: (n-1) I + Y^T Y, Y n x n iid N(0,1)/sqrt(n)."""
+    if family == "clustered":
+        return make_family_batch(torch, family, L, n, seed, device).to(dtype)
     g = torch.Generator(device=device)
     g.manual_seed(seed)
     out = torch.empty((L, n, n), dtype=dtype, device=device)
@@ -165,6 +170,7 @@ def make_batch(torch, family, L, n, dtype, seed, device):
 FAMILY_TEXT = {
     "letkf": "LETKF-like (n-1) I + Y^T Y, Y iid N(0,1)/sqrt(n)",
     "symu": "(B + B^T)/2, B iid U[-1,1]",
+    "clustered": "Q diag(l) Q^T, l in clusters of eight values 1e-8 apart, 0.1 between clusters",
 }
 
 
@@ -612,16 +618,16 @@ def make_theta_family(torch, L, n, seed, device, family_seed=2024):
             torch.from_numpy(np.ascontiguousarray(a.astype(np.float32))).to(device))
 
 
-def learned_block(torch, E, args, stream):
-    """C5: 65536 FP32 matrices n = 64 of the theta family.  The network is
-    trained (200k solver-generated eigenpairs, the library's own kernels;
-    time reported, outside the timed solves), then the learned solve is
-    timed against the plain FP32 path and against the same polish started
-    from A0's eigenbasis or from the identity (the method without the
-    network)."""
+def learned_block(torch, E, args, stream, L=65536):
+    """C5: L (default 65536) FP32 matrices n = 64 of the theta family.  The
+    network is trained (200k solver-generated eigenpairs, the library's own
+    kernels; time reported, outside the timed solves), then the learned
+    solve is timed against the plain FP32 path and against the same polish
+    started from A0's eigenbasis or from the identity (the method without
+    the network)."""
     import eigeng_b200.learned as lw
     dev = torch.device("cuda", torch.cuda.current_device())
-    n, L = 64, 65536
+    n = 64
     a0, e, base = make_theta_family(torch, L, n, 123, dev)
     t0 = time.perf_counter()
     v0 = lw.basis_eigenvectors(a0)
@@ -660,6 +666,53 @@ def learned_block(torch, E, args, stream):
     return out
 
 
+def run_form(args):
+    """One JSON line for the refined or the learned form alone (one GPU),
+    same timing rules as the plain solve: fresh copy per step, warm-up, CUDA
+    events on the launching stream."""
+    import torch
+    import eigeng_b200 as E
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    clk = ClockSampler(0).start()
+    try:
+        if args.form == "learned":
+            w0 = time.perf_counter()
+            out = learned_block(torch, E, args, stream, L=args.L)
+            w1 = time.perf_counter()
+            line = {"metric": f"eigendecomps/s learned form (n=64, f32, theta family, L={args.L})",
+                    "value": out["network"]["matrices_per_s"], "unit": "matrices/s", "n_gpus": 1,
+                    "higher_is_better": True, "dtype": "f32", "data": "synthetic theta family", "learned": out}
+        else:
+            n, L = args.n, args.L
+            dev = torch.device("cuda", 0)
+            base = make_family_batch(torch, args.family, L, n, 4242, dev)
+            rwk = E.refine_workspace(L, n, n, device=dev)
+            holder = {}
+
+            def refined(a):
+                holder["w"], holder["info"], holder["it"] = E.solve_refined(a, n, wk=rwk, stream=stream)
+            w0 = time.perf_counter()
+            ms, last = timed_solves(torch, base, max(1, args.steps), max(3, args.warmup), refined, stream)
+            w1 = time.perf_counter()
+            e1, e2, fl = E.check(base, holder["w"], last, n)
+            it = holder["it"].cpu().numpy()
+            line = {"metric": f"eigendecomps/s refined form (n={n}, f64, {args.family}, L={L})",
+                    "value": L / ms * 1e3, "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
+                    "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "dtype": "f64",
+                    "data": "synthetic, seeded on device", "gate_flags": int((fl != 0).sum()),
+                    "max_err1": float(e1.max()), "max_err2": float(e2.max()),
+                    "iterations": np.bincount(it, minlength=4).tolist(), "fallback": int((it == 0).sum())}
+    finally:
+        clk.stop()
+    line["clocks"] = clk.summary(w0, w1)
+    s = json.dumps(line)
+    print(s, flush=True)
+    if args.out:
+        with open(args.out, "a") as f:
+            f.write(s + "\n")
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -668,6 +721,8 @@ def main():
         return run_uneven_bench(args)
     if args.impl == "cusolver":
         return run_cusolver(args)
+    if args.form != "plain":
+        return run_form(args)
     import torch
     import torch.distributed as dist
     import eigeng_b200 as E

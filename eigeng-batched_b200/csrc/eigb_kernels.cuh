@@ -2,6 +2,8 @@
 //
 //   k_n1           n == 1 (eigen_GPU_batch.cu:36-54): w = a(1,1), a(1,1) = 1
 //   k1_warp        phase 1 for n <= 32: one warp per matrix, 4 per CTA
+//   k1_cl          phase 1 for 32 < n <= 512 on a thread-block cluster, the
+//                  matrix in the cluster's distributed shared memory
 //   k1_reg<NB>     phase 1 for 32 < n <= 128: one CTA per matrix, the matrix
 //                  in registers (eigb_tridiag_reg.cuh)
 //   k1_cta<SPLIT>  phase 1 for larger n: one CTA per matrix; the leading
@@ -28,6 +30,7 @@
 #include "eigb_symfunc.cuh"
 #include "eigb_tmem.cuh"
 #include "eigb_tridiag.cuh"
+#include "eigb_tridiag_cl.cuh"
 #include "eigb_tridiag_reg.cuh"
 
 namespace eigb {
@@ -220,6 +223,20 @@ __global__ void __launch_bounds__(32 * NB * NB, k1r_min_blocks<T>(NB)) k1_reg(co
   CtaTeam tm;
   tridiag_qt_reg<T, NB>(tm, mat_ptr(p, k), p.nm, p.n, p.d + k * p.n, p.e + k * p.n,
                         reinterpret_cast<T *>(smem_raw), p.ap ? p.ap + (size_t)k * packed_size(p.n) : nullptr);
+}
+
+// Phase 1 on a cluster of cl_cn(n) CTAs per matrix, the matrix in their
+// distributed shared memory (eigb_tridiag_cl.cuh); 32 < n <= 512.
+// SPLIT warps per CTA, one column range each; two CTAs per SM by registers.
+constexpr int K1CL_SPLIT = 16;
+template <class T, int SPLIT = K1CL_SPLIT>
+__global__ void __launch_bounds__(32 * SPLIT, 1024 / (32 * SPLIT)) k1_cl(const KP<T> p)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const long k = blockIdx.x / cl_cn(p.n);
+  tridiag_qt_cluster<T, SPLIT>(mat_ptr(p, k), p.nm, p.n, p.d + k * p.n, p.e + k * p.n,
+                               p.ap ? p.ap + (size_t)k * packed_size(p.n) : nullptr,
+                               reinterpret_cast<T *>(smem_raw));
 }
 
 // ---------------------------------------------------------------- phase 2

@@ -113,6 +113,16 @@ inline const eigen_GPU_batch_opts *tuned(const eigen_GPU_batch_opts *opts, int e
   return &out;
 }
 
+// the phase-1 kernel the table asks for (EIGEN_GPU_REDUCE_*)
+inline int tuned_reduce(int esize, int n)
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return EIGEN_GPU_REDUCE_AUTO;
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_tune.find(TuneKey{dev, esize, n});
+  return it == g_tune.end() ? EIGEN_GPU_REDUCE_AUTO : it->second.reduce;
+}
+
 // phase timing events set by eigen_GPU_batch_trace
 cudaEvent_t *g_trace = nullptr;
 int g_ntrace = 0;
@@ -315,6 +325,51 @@ template <class T> void launch_k1r(const KP<T> &p, unsigned blocks, size_t smem,
   else k1_reg<T, 4><<<blocks, 32 * 16, smem, st>>>(p);
 }
 
+// phase 1 on a cluster: usable when the device can hold one of its
+// clusters (shared memory, cluster size; sizes above 8 need the
+// non-portable opt-in)
+template <class T> cudaLaunchConfig_t k1cl_config(int n, long cnt, cudaStream_t st, cudaLaunchAttribute *at)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(cnt * cl_cn(n)));
+  cfg.blockDim = dim3(32 * K1CL_SPLIT);
+  cfg.dynamicSmemBytes = cl_smem_bytes<T, K1CL_SPLIT>(n);
+  cfg.stream = st;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cl_cn(n);
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+template <class T> bool k1cl_usable(int n, const DevProps &dp)
+{
+  if (n <= 32 || n > 32 * CL_MAX_CN) return false;
+  const size_t smem = cl_smem_bytes<T, K1CL_SPLIT>(n);
+  if (smem > (size_t)dp.smem_optin) return false;
+  if (set_smem(k1_cl<T>, smem) != cudaSuccess) return false;
+  if (cl_cn(n) > 8 &&
+      cudaFuncSetAttribute(k1_cl<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = k1cl_config<T>(n, 1, nullptr, at);
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, k1_cl<T>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return clusters >= 1;
+}
+template <class T> cudaError_t launch_k1cl(const KP<T> &p, long cnt, cudaStream_t st)
+{
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = k1cl_config<T>(p.n, cnt, st, at);
+  return cudaLaunchKernelEx(&cfg, k1_cl<T>, p);
+}
+
 template <class T> cudaError_t set_k1_smem(int n, size_t bytes)
 {
   const int sp = k1_split(n);
@@ -432,7 +487,9 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   p.zsplit = pl.zsplit;
   p.k1b = pl.k1b;
   const int k1c_nt = k1c_threads(n);
-  const bool k1_in_regs = reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin;
+  const int red_form = tuned_reduce((int)sizeof(T), n);
+  const bool k1_cluster = red_form == EIGEN_GPU_REDUCE_CLUSTER && k1cl_usable<T>(n, dp);
+  const bool k1_in_regs = !k1_cluster && reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin;
   const size_t k1c_smem = k1_in_regs ? k1r_smem_bytes<T>(n) : sizeof(T) * k1c_smem_elems(n, k1c_nt, pl.k1b);
   size_t k3c_smem = k3c_smem_bytes<T>(n, ztm ? 0 : pl.zrows);
   int k3_wpp = 0, k3_parts = 0, k3_acols = 0;  // tensor-memory form: warps per part, parts per CTA, columns
@@ -510,7 +567,9 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     if ((err = set_smem(k1_warp<T>, k1w_smem)) != cudaSuccess) return err;
     if ((err = set_smem(k3_warp<T>, k3w_smem)) != cudaSuccess) return err;
   } else {
-    if (k1_in_regs) {
+    if (k1_cluster) {
+      // attributes set by k1cl_usable
+    } else if (k1_in_regs) {
       if ((err = set_k1r_smem<T>(n, k1c_smem)) != cudaSuccess) return err;
     } else if ((err = set_k1_smem<T>(n, k1c_smem)) != cudaSuccess) {
       return err;
@@ -526,9 +585,13 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   if ((err = set_smem(k2_ql<T>, k2_smem)) != cudaSuccess) return err;
 
   // the three phase launches of cnt matrices described by q, on st
+  cudaError_t lerr = cudaSuccess;  // a launch error returned rather than left for cudaGetLastError
   auto phase1 = [&](const KP<T> &q, long cnt, cudaStream_t st) {
     if (n <= 32) {
       k1_warp<T><<<(unsigned)((cnt + K1W_NW - 1) / K1W_NW), 32 * K1W_NW, k1w_smem, st>>>(q);
+    } else if (k1_cluster) {
+      const cudaError_t e = launch_k1cl<T>(q, cnt, st);
+      if (e != cudaSuccess && lerr == cudaSuccess) lerr = e;
     } else if (k1_in_regs) {
       launch_k1r<T>(q, (unsigned)cnt, k1c_smem, st);
     } else {
@@ -584,6 +647,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
     trace(chunk, 2, stream);
     if (sg.phases & EIGEN_GPU_STAGE_APPLY) phase3(p, lc, stream);
     trace(chunk, 3, stream);
+    if (lerr != cudaSuccess) return lerr;
     if ((err = cudaGetLastError()) != cudaSuccess) return err;
   }
   return cudaSuccess;
@@ -612,7 +676,14 @@ cudaError_t launch_params(long L, int n, int *grp, int *tb, int *gr, int *th, in
   Plan<T> pl;
   if ((err = make_plan<T>(L, n, n, dp, pl, nullptr)) != cudaSuccess) return err;
   const long lc = std::min(L, pl.Lc);
-  if (n <= 32) {  // k1_warp: one warp per matrix
+  const int red_form = tuned_reduce((int)sizeof(T), n);
+  if (n > 32 && red_form == EIGEN_GPU_REDUCE_CLUSTER && k1cl_usable<T>(n, dp)) {  // k1_cl: ceil(n/32) blocks per matrix
+    *th = 32 * K1CL_SPLIT;
+    *grp = cl_cn(n) * *th;
+    *gr = 1;
+    *tb = (int)(lc * cl_cn(n));
+    *sh = (int)cl_smem_bytes<T, K1CL_SPLIT>(n);
+  } else if (n <= 32) {  // k1_warp: one warp per matrix
     *grp = 32;
     *gr = K1W_NW;
     *th = 32 * K1W_NW;
@@ -2388,7 +2459,7 @@ cudaError_t eigen_GPU_batch_tune_set(const eigen_GPU_tune_entry *entries, const 
     const eigen_GPU_tune_entry &e = entries[i];
     if ((e.esize != 4 && e.esize != 8) || e.n < 1 || e.n > 1024 || e.split < 0 || e.split > 32 ||
         (e.zmem != EIGEN_GPU_ZMEM_AUTO && e.zmem != EIGEN_GPU_ZMEM_SHARED) || e.ql_mpw < 0 || e.ql_mpw > 32 ||
-        (e.ql_mpw & (e.ql_mpw - 1)) != 0)
+        (e.ql_mpw & (e.ql_mpw - 1)) != 0 || e.reduce < EIGEN_GPU_REDUCE_AUTO || e.reduce > EIGEN_GPU_REDUCE_CLUSTER)
       return cudaErrorInvalidValue;
   }
   std::lock_guard<std::mutex> lk(eigb::g_mu);

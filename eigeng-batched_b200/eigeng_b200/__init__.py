@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libeigenGbatch.so")
 
 TQL2, IMTQL2, JACOBI = 0, 1, 2
 ZMEM_AUTO, ZMEM_SHARED = 0, 1  # where the apply phase keeps Z (eigen_GPU_batch_opts.zmem)
+REDUCE_AUTO, REDUCE_CTA, REDUCE_CLUSTER = 0, 1, 2  # phase-1 kernel (eigen_GPU_tune_entry.reduce)
 # phases of eigen_GPU_batch_stage_* (EIGEN_GPU_STAGE_*)
 STAGE_REDUCE, STAGE_QL, STAGE_APPLY, STAGE_ALL = 1, 2, 4, 7
 
@@ -57,7 +58,7 @@ WARM_NETWORK, WARM_BASIS, WARM_IDENTITY = 0, 1, 2
 class TuneEntry(ctypes.Structure):
     """eigen_GPU_tune_entry of include/eigen_GPU_batch.h."""
     _fields_ = [("esize", ctypes.c_int), ("n", ctypes.c_int), ("split", ctypes.c_int), ("zmem", ctypes.c_int),
-                ("ql_mpw", ctypes.c_int)]
+                ("ql_mpw", ctypes.c_int), ("reduce", ctypes.c_int)]
 
 
 def lib():
@@ -389,9 +390,10 @@ def rayleigh(a, x, n, nm=None, want_s=True, want_g=True, stream=None):
 
 def tune_set(entries):
     """eigen_GPU_batch_tune_set on the current device; entries: dicts with
-    esize, n, split, zmem, ql_mpw (an empty list clears the table)."""
-    arr = (TuneEntry * max(1, len(entries)))(*[TuneEntry(e["esize"], e["n"], e["split"], e["zmem"], e["ql_mpw"])
-                                               for e in entries])
+    esize, n, split, zmem, ql_mpw and optionally reduce (REDUCE_*; an empty
+    list clears the table)."""
+    arr = (TuneEntry * max(1, len(entries)))(*[TuneEntry(e["esize"], e["n"], e["split"], e["zmem"], e["ql_mpw"],
+                                                         e.get("reduce", REDUCE_AUTO)) for e in entries])
     st = lib().eigen_GPU_batch_tune_set(ctypes.cast(arr, ctypes.c_void_p), len(entries))
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_tune_set failed with cudaError {st}")
@@ -403,7 +405,7 @@ def tune_get(esize, n):
     st = lib().eigen_GPU_batch_tune_get(esize, n, ctypes.byref(e))
     if st != 0:
         return None
-    return {"esize": e.esize, "n": e.n, "split": e.split, "zmem": e.zmem, "ql_mpw": e.ql_mpw}
+    return {"esize": e.esize, "n": e.n, "split": e.split, "zmem": e.zmem, "ql_mpw": e.ql_mpw, "reduce": e.reduce}
 
 
 def packed_size(n):

@@ -3,10 +3,13 @@ reference, whose launch parameters are fixed rules in
 eigen_GPU_batch.hpp:23-102).
 
 For each (precision, order n) it times, on this device, a solve of a
-representative batch under every candidate setting of the options that
-change speed but not results -- the apply phase's CTAs per matrix (split),
-where that phase keeps its rows (zmem: tensor or shared memory) and the QL
-phase's matrices per warp (ql_mpw) -- and keeps the fastest.  The table is
+representative batch: first under each phase-1 kernel that applies
+(reduce: the one-CTA forms or the cluster form, 32 < n <= 512; they differ
+in rounding only), then, with the faster one, under every candidate
+setting of the options that change speed but not results -- the apply
+phase's CTAs per matrix (split), where that phase keeps its rows (zmem:
+tensor or shared memory) and the QL phase's matrices per warp (ql_mpw) --
+and keeps the fastest.  The table is
 written as JSON and installed with eigen_GPU_batch_tune_set, after which
 every solve of that (precision, n) whose options are automatic uses it
 (including the groups of mixed-size batches).
@@ -21,7 +24,8 @@ import json
 
 import torch
 
-from . import ZMEM_AUTO, ZMEM_SHARED, eigen_GPU_batch_ex, tune_set, workspace
+from . import (REDUCE_AUTO, REDUCE_CLUSTER, REDUCE_CTA, ZMEM_AUTO, ZMEM_SHARED, eigen_GPU_batch_ex, tune_set,
+               workspace)
 
 QL_MPW = (0, 1, 2, 4, 8, 16, 32)
 SPLITS = (0, 2, 4)
@@ -35,6 +39,11 @@ def candidates(n):
         return [dict(split=0, zmem=ZMEM_AUTO, ql_mpw=q) for q in QL_MPW]
     return [dict(split=s, zmem=z, ql_mpw=q) for s, z, q in itertools.product(SPLITS, ZMEM, QL_MPW)
             if s == 0 or s <= (n + 31) // 32]
+
+
+def reduce_forms(n):
+    """The phase-1 kernels tried for order n."""
+    return [REDUCE_CTA, REDUCE_CLUSTER] if 32 < n <= 512 else [REDUCE_AUTO]
 
 
 def default_batch(n):
@@ -80,10 +89,20 @@ def tune(sizes, dtype=torch.float64, batch=None, reps=3, log=None):
     for n in sizes:
         L = batch or default_batch(n)
         base = symmetric_batch(L, n, dtype, seed=n)
+        plain = dict(split=0, zmem=ZMEM_AUTO, ql_mpw=0)
+        tune_set([])
+        auto_ms = time_setting(base, n, plain, reps, dtype)
+        forms = []
+        for red in reduce_forms(n):
+            tune_set([dict(esize=esize, n=n, reduce=red, **plain)])
+            forms.append((time_setting(base, n, plain, reps, dtype), red))
+        red = min(forms)[1]
+        tune_set([dict(esize=esize, n=n, reduce=red, **plain)])
         results = [(time_setting(base, n, c, reps, dtype), i, c) for i, c in enumerate(candidates(n))]
-        auto = [r for r in results if r[2]["split"] == 0 and r[2]["zmem"] == ZMEM_AUTO and r[2]["ql_mpw"] == 0][0]
+        tune_set([])
         best = min(results)
-        e = dict(esize=esize, n=n, **best[2], ms=best[0], auto_ms=auto[0], batch=L)
+        e = dict(esize=esize, n=n, **best[2], reduce=red, ms=best[0], auto_ms=auto_ms, batch=L)
+        auto = (auto_ms,)
         table.append(e)
         if log:
             log(f"n={n}: auto {auto[0]:.3f} ms, best {best[0]:.3f} ms with {best[2]}")

@@ -334,10 +334,12 @@ cudaError_t eigen_GPU_batch_symfunc_FP(const int L, const int nm, const int n, c
  * device, for the first chunk of the batch; counterpart of the reference's
  * header-only eigen_GPU_batch_get_Launch_params (eigen_GPU_batch.hpp:23-102),
  * which include/eigen_GPU_batch.hpp forwards here.  grpSZ: threads that own
- * one matrix; numGR: matrices per thread block; numTH: threads per block;
- * numTB: thread blocks of the launch; sizeSH: dynamic shared memory bytes
- * per block; sizeL2: the device's L2 bytes.  cudaErrorInvalidValue for
- * L < 1, n < 1 or n > 1024.
+ * one matrix; numGR: matrices per thread block (1 also for the cluster
+ * form, where a matrix spans a cluster of ceil(n/32) blocks and grpSZ
+ * counts the cluster's threads); numTH: threads per block; numTB: thread
+ * blocks of the launch; sizeSH: dynamic shared memory bytes per block;
+ * sizeL2: the device's L2 bytes.  cudaErrorInvalidValue for L < 1, n < 1
+ * or n > 1024.
  */
 cudaError_t eigen_GPU_batch_launch_params_DP(const int L, const int n, int *grpSZ, int *numTB, int *numGR,
                                              int *numTH, int *sizeSH, int *sizeL2);
@@ -349,8 +351,9 @@ cudaError_t eigen_GPU_batch_launch_params_FP(const int L, const int n, int *grpS
  * are fixed rules, eigen_GPU_batch.hpp:23-102): a table, per device and per
  * (element size, order n), of the options a solve then uses wherever the
  * caller leaves them automatic -- the apply phase's CTAs per matrix
- * (split), where its rows live (zmem) and the QL phase's matrices per warp
- * (ql_mpw).  None of these changes results, bit for bit; they change speed.
+ * (split), where its rows live (zmem), the QL phase's matrices per warp
+ * (ql_mpw) and the phase-1 kernel (reduce).  split, zmem and ql_mpw change
+ * speed, not results (bit for bit); reduce changes rounding (see below).
  * eigeng_b200/autotune.py measures the candidates on the device and writes
  * such a table.  eigen_GPU_batch_tune_set replaces the current device's
  * table by `count` entries (0 clears it); it is global to the process.
@@ -363,7 +366,17 @@ typedef struct eigen_GPU_tune_entry {
   int split;  /* 0: automatic, else as eigen_GPU_batch_opts.split (1..32) */
   int zmem;   /* EIGEN_GPU_ZMEM_AUTO or EIGEN_GPU_ZMEM_SHARED */
   int ql_mpw; /* 0: automatic, else a power of two 1..32 */
+  int reduce; /* phase-1 kernel: EIGEN_GPU_REDUCE_AUTO, _CTA or _CLUSTER */
 } eigen_GPU_tune_entry;
+/* phase-1 kernels: automatic (the one-CTA forms, measured faster on B200),
+ * one CTA per matrix (registers for n <= 128, shared memory and a band in
+ * global memory above), or a thread-block cluster holding the matrix in
+ * distributed shared memory (32 < n <= 512, where the device can run it).
+ * Unlike the other entries, the choice changes rounding (another summation
+ * order), within the solver's accuracy. */
+#define EIGEN_GPU_REDUCE_AUTO 0
+#define EIGEN_GPU_REDUCE_CTA 1
+#define EIGEN_GPU_REDUCE_CLUSTER 2
 cudaError_t eigen_GPU_batch_tune_set(const eigen_GPU_tune_entry *entries, const int count);
 cudaError_t eigen_GPU_batch_tune_get(const int esize, const int n, eigen_GPU_tune_entry *out);
 

@@ -90,7 +90,9 @@ def test_launch_params_report_the_launched_geometry(tmp_path):
     for n <= 32, a CTA of 32*NB*NB threads (NB = ceil(n/32)) in the
     register form for 32 < n <= 128, and the CTA form's
     min(1024, ceil(n/32)*32*split) threads above (split 4 up to n = 256, 2
-    up to 512, then 1), one block per matrix."""
+    up to 512, then 1), one block per matrix; with the cluster form asked
+    for (tuned option reduce), ceil(n/32) blocks of 256 threads per
+    matrix."""
     import subprocess
     out = subprocess.check_output([_cpp_launch_params_program(str(tmp_path))], text=True)
     rows = {int(x.split()[0]): [int(v) for v in x.split()[1:]] for x in out.strip().splitlines()}
@@ -113,3 +115,9 @@ def test_launch_params_report_the_launched_geometry(tmp_path):
             assert 0 < b <= 4096
     import eigeng_b200 as E
     assert E.launch_params(4096, 128)["numTH"] == rows[128][3]
+    E.tune_set([dict(esize=8, n=256, split=0, zmem=0, ql_mpw=0, reduce=E.REDUCE_CLUSTER)])
+    try:
+        lp = E.launch_params(4096, 256)
+    finally:
+        E.tune_set([])
+    assert (lp["grpSZ"], lp["numGR"], lp["numTH"]) == (8 * 256, 1, 256) and lp["numTB"] % 8 == 0
