@@ -91,7 +91,7 @@ def test_launch_params_report_the_launched_geometry(tmp_path):
     register form for 32 < n <= 128, and the CTA form's
     min(1024, ceil(n/32)*32*split) threads above (split 4 up to n = 256, 2
     up to 512, then 1), one block per matrix; with the cluster form asked
-    for (tuned option reduce), ceil(n/32) blocks of 256 threads per
+    for (tuned option reduce), ceil(n/32) blocks of 512 threads per
     matrix."""
     import subprocess
     out = subprocess.check_output([_cpp_launch_params_program(str(tmp_path))], text=True)
@@ -120,4 +120,4 @@ def test_launch_params_report_the_launched_geometry(tmp_path):
         lp = E.launch_params(4096, 256)
     finally:
         E.tune_set([])
-    assert (lp["grpSZ"], lp["numGR"], lp["numTH"]) == (8 * 256, 1, 256) and lp["numTB"] % 8 == 0
+    assert (lp["grpSZ"], lp["numGR"], lp["numTH"]) == (8 * 512, 1, 512) and lp["numTB"] % 8 == 0
