@@ -378,8 +378,11 @@ __global__ void __launch_bounds__(256) k_cluster_apply(const int n, double *__re
       if (threadIdx.x == 0 && err) atomicExch(err, 1);
       return;
     }
+    // the entries past the cluster's size in each column of W are never
+    // written: zeros here, so that the products below (over all
+    // REF_CL_MAX slots) never meet whatever the workspace held
     for (int u = threadIdx.x; u < sz * REF_CL_MAX; u += blockDim.x)
-      ws[u] = W[((size_t)b * n + k0) * REF_CL_MAX + u];
+      ws[u] = (u % REF_CL_MAX) < sz ? W[((size_t)b * n + k0) * REF_CL_MAX + u] : 0.0;
     if (threadIdx.x < sz) {
       const int m = order[(size_t)b * n + k0 + threadIdx.x];
       mem[threadIdx.x] = m;
