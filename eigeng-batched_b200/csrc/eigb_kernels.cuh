@@ -91,8 +91,16 @@ constexpr int K3W_CH = 128;     // records staged per warp
 // per warp: S (K1W_LD x 32), beta[32], pv[32], red[72], ubuf[4*32], gram[3*32]
 template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD * 32 + 32 + 32 + 72 + 128 + 96; }
 
-// threads per row in k1_cta (column ranges split across warps)
-__host__ __device__ constexpr int k1_split(int n) { return n <= 256 ? 4 : (n <= 512 ? 2 : 1); }
+// threads per row in k1_cta (column ranges split across warps).  FP64
+// 128 < n <= 240 takes two, which with a smaller leading block in shared
+// memory (k1c_block) leaves room for two or three CTAs per SM: measured on
+// B200, phase 1 in ms at four per row / two per row: n=136 20.6 / 15.9,
+// n=160 27.8 / 23.5, n=192 47.8 / 41.7, n=224 34.5 / 32.4 (L=2048), n=240
+// 44.2 / 42.6; at n=256 52.4 against 51.0, so four stay there.
+template <class T> __host__ __device__ constexpr int k1_split(int n)
+{
+  return (sizeof(T) == 8 && n <= 240) ? 2 : (n <= 256 ? 4 : (n <= 512 ? 2 : 1));
+}
 
 // ---------------------------------------------------------------- n == 1
 template <class T>

@@ -140,18 +140,21 @@ inline void trace(long chunk, int slot, cudaStream_t stream)
   if (ev && 4 * chunk + 3 < nev) cudaEventRecord(ev[i], stream);
 }
 
-inline int k1c_threads(int n) { return std::min(1024, ((n + 31) / 32) * 32 * k1_split(n)); }
+template <class T> int k1c_threads(int n) { return std::min(1024, ((n + 31) / 32) * 32 * k1_split<T>(n)); }
 // leading block of phase 1 (CTA form) held in shared memory: the whole
 // matrix when it fits; otherwise the largest that fits next to the scratch
 // arrays, for FP64 at most 128 x 128, which leaves L1 room for the outer
 // band (measured on B200 at n = 200 and 256: 15-20 % faster than the
-// largest block; FP32 is fastest with the largest)
+// largest block; FP32 is fastest with the largest).  FP64 128 < n <= 240
+// keeps a 64 x 64 (n <= 176) or 96 x 96 block: more CTAs per SM pay more
+// than a larger block (see k1_split)
 template <class T> int k1c_block(int n, size_t optin)
 {
-  const size_t base = sizeof(T) * k1c_smem_elems(n, k1c_threads(n), 0);
+  const size_t base = sizeof(T) * k1c_smem_elems(n, k1c_threads<T>(n), 0);
   if (base >= optin) return 0;
   int B = n;
   if (sizeof(T) == 8 && base + sizeof(T) * (size_t)n * (size_t)(n | 1) > optin) B = std::min(n, 128);
+  if (sizeof(T) == 8 && n > 128 && n <= 240) B = n <= 176 ? 64 : 96;
   while (B > 0 && base + sizeof(T) * (size_t)B * (size_t)(B | 1) > optin) B--;
   return B;
 }
@@ -372,7 +375,7 @@ template <class T> cudaError_t launch_k1cl(const KP<T> &p, long cnt, cudaStream_
 
 template <class T> cudaError_t set_k1_smem(int n, size_t bytes)
 {
-  const int sp = k1_split(n);
+  const int sp = k1_split<T>(n);
   if (sp == 4) return set_smem(k1_cta<T, 4>, bytes);
   if (sp == 2) return set_smem(k1_cta<T, 2>, bytes);
   return set_smem(k1_cta<T, 1>, bytes);
@@ -380,7 +383,7 @@ template <class T> cudaError_t set_k1_smem(int n, size_t bytes)
 
 template <class T> void launch_k1(const KP<T> &p, unsigned blocks, int nt, size_t smem, cudaStream_t st)
 {
-  const int sp = k1_split(p.n);
+  const int sp = k1_split<T>(p.n);
   if (sp == 4) k1_cta<T, 4><<<blocks, nt, smem, st>>>(p);
   else if (sp == 2) k1_cta<T, 2><<<blocks, nt, smem, st>>>(p);
   else k1_cta<T, 1><<<blocks, nt, smem, st>>>(p);
@@ -486,7 +489,7 @@ cudaError_t run(long L, int nm, int n, int m, T *a, T *w, void *wk, size_t lwork
   p.zrows = pl.zrows;
   p.zsplit = pl.zsplit;
   p.k1b = pl.k1b;
-  const int k1c_nt = k1c_threads(n);
+  const int k1c_nt = k1c_threads<T>(n);
   const int red_form = tuned_reduce((int)sizeof(T), n);
   const bool k1_cluster = red_form == EIGEN_GPU_REDUCE_CLUSTER && k1cl_usable<T>(n, dp);
   const bool k1_in_regs = !k1_cluster && reg_nb(n) > 0 && k1r_smem_bytes<T>(n) <= (size_t)dp.smem_optin;
@@ -696,10 +699,10 @@ cudaError_t launch_params(long L, int n, int *grp, int *tb, int *gr, int *th, in
     *tb = (int)lc;
     *sh = (int)k1r_smem_bytes<T>(n);
   } else {  // k1_cta
-    *grp = *th = k1c_threads(n);
+    *grp = *th = k1c_threads<T>(n);
     *gr = 1;
     *tb = (int)lc;
-    *sh = (int)(sizeof(T) * k1c_smem_elems(n, k1c_threads(n), pl.k1b));
+    *sh = (int)(sizeof(T) * k1c_smem_elems(n, k1c_threads<T>(n), pl.k1b));
   }
   return cudaSuccess;
 }

@@ -89,8 +89,8 @@ def test_launch_params_report_the_launched_geometry(tmp_path):
     it: one thread per matrix for n = 1, a warp per matrix (four per block)
     for n <= 32, a CTA of 32*NB*NB threads (NB = ceil(n/32)) in the
     register form for 32 < n <= 128, and the CTA form's
-    min(1024, ceil(n/32)*32*split) threads above (split 4 up to n = 256, 2
-    up to 512, then 1), one block per matrix; with the cluster form asked
+    min(1024, ceil(n/32)*32*split) threads above (FP64 split 2 up to n =
+    240, 4 up to 256, 2 up to 512, then 1), one block per matrix; with the cluster form asked
     for (tuned option reduce), ceil(n/32) blocks of 512 threads per
     matrix."""
     import subprocess
@@ -109,7 +109,7 @@ def test_launch_params_report_the_launched_geometry(tmp_path):
             assert (g, r, t) == (32 * nb * nb, 1, 32 * nb * nb), n
             assert 0 < b <= 4096
         else:
-            split = 4 if n <= 256 else (2 if n <= 512 else 1)
+            split = 2 if n <= 240 else (4 if n <= 256 else (2 if n <= 512 else 1))
             th = min(1024, math.ceil(n / 32) * 32 * split)
             assert (g, r, t) == (th, 1, th), n
             assert 0 < b <= 4096
