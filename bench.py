@@ -559,6 +559,52 @@ def timed_solves(torch, base, steps, warmup, fn, stream):
     return t0.elapsed_time(t1) / steps, last
 
 
+def gate_in_packed_solve(torch, E, base, n, stream, steps):
+    """The packed solve alone against the packed solve with the accuracy
+    gate in the same call (eigen_GPU_batch_packed_check), same packed
+    inputs, same timing rules; plus the gate's verdict."""
+    L = base.shape[0]
+    ap = E.pack_upper(base, n)
+    dt = base.dtype
+    wk = E.workspace(L, n, n, dt, base.device)
+    z = torch.empty_like(base)
+    w = torch.empty((L, n), dtype=dt, device=base.device)
+    info = torch.zeros(L, dtype=torch.int32, device=base.device)
+    import ctypes
+    e1 = torch.empty(L, dtype=torch.float64, device=base.device)
+    e2 = torch.empty(L, dtype=torch.float64, device=base.device)
+    fl = torch.empty(L, dtype=torch.int32, device=base.device)
+    o = E.Opts(0, 1, 100, 0, 0, 0)
+    sfx = "DP" if dt == torch.float64 else "FP"
+    plain = getattr(E.lib(), "eigen_GPU_batch_packed_" + sfx)
+    checked = getattr(E.lib(), "eigen_GPU_batch_packed_check_" + sfx)
+    st = E._stream(stream)
+
+    def run(with_gate):
+        if with_gate:
+            return checked(L, n, E._ptr(ap), E._ptr(z), n, E._ptr(w), E._ptr(wk), wk.numel(), E._ptr(info),
+                           ctypes.byref(o), E._ptr(e1), E._ptr(e2), E._ptr(fl), st)
+        return plain(L, n, E._ptr(ap), E._ptr(z), n, E._ptr(w), E._ptr(wk), wk.numel(), E._ptr(info),
+                     ctypes.byref(o), st)
+    out = {}
+    for name, g in (("packed_solve", False), ("packed_solve_with_gate", True)):
+        for _ in range(3):
+            assert run(g) == 0
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(steps):
+            run(g)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        out[name] = {"ms": t0.elapsed_time(t1) / steps}
+    out["overhead"] = out["packed_solve_with_gate"]["ms"] / out["packed_solve"]["ms"] - 1.0
+    out["gate_flags"] = int((fl != 0).sum())
+    out["max_err1"] = float(e1.max())
+    out["max_err2"] = float(e2.max())
+    return out
+
+
 def chosen_vs_plain(torch, E, args, stream):
     """The metric's comparison at n = 32, 128, 256 (FP64): the plain form
     (tridiagonal + QL) against the refined form (FP32 solve, tensor-core
@@ -892,6 +938,8 @@ def main():
             del cps, wk2
         line["sizes"] = {"unit": "matrices/s", "data": "synthetic (B + B^T)/2, B iid U[-1,1]", **sizes}
 
+    if not args.no_extra and world == 1:
+        line["gate_in_packed_solve"] = gate_in_packed_solve(torch, E, base, n, stream, max(3, min(args.steps, 10)))
     if not args.no_chosen and world == 1:
         line["chosen_vs_plain"] = chosen_vs_plain(torch, E, args, stream)
     if not args.no_learned and world == 1:

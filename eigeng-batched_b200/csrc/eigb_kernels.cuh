@@ -1394,6 +1394,135 @@ __global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, c
   }
 }
 
+// The same two norms with TILE x TILE output tiles (TILE = 32, 64 or 128):
+// a 16 x 16 thread grid, an R x R FP64 register tile per thread (R =
+// TILE/16; rows and columns 16 apart), 16-deep panels of A (or of Z for
+// Z^T Z) and of Z staged in shared memory; R^2 FMAs per 2R shared-memory
+// loads (64 per 16 at TILE = 128).  PACKED reads A from the packed upper
+// triangle (ap + id n(n+1)/2, element (r, c), r <= c, at r + c(c+1)/2)
+// instead of the full layout; Z has leading dimension ldz.
+constexpr int CK8_KC = 16;
+
+template <class T, bool PACKED, int TILE>
+__global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, const int ldz, const int n, const int m,
+                                                   const T *a0, const T *w, const T *z, double *err1, double *err2,
+                                                   int *flags, float *ref_flags)
+{
+  constexpr int R = TILE / 16, LDP = TILE + 1;
+  __shared__ double P[CK8_KC][LDP];  // P(k, tile row)
+  __shared__ double Q[CK8_KC][LDP];  // Q(k, tile column)
+  __shared__ double red[64];
+  const long id = blockIdx.x;
+  if (id >= L) return;
+  const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * lda * n;
+  const T *zz = z + (size_t)id * ldz * n;
+  const T *d = w + (size_t)id * n;
+  const int t = threadIdx.x, tr = t % 16, tc = t / 16;
+  const int ntn = (n + TILE - 1) / TILE, ntm = (m + TILE - 1) / TILE;
+  double s1 = 0.0, s2 = 0.0;
+  const int nres = ntn * ntm, nort = ntm * (ntm + 1) / 2;
+  for (int tile = 0; tile < nres + nort; tile++) {
+    const bool res = tile < nres;
+    int ti, tj;
+    if (res) {
+      ti = tile % ntn;
+      tj = tile / ntn;
+    } else {
+      symf_tile(tile - nres, ntm, ti, tj);
+    }
+    const int i0 = ti * TILE, j0 = tj * TILE;
+    const int ilim = res ? n : m;
+    double acc[R][R];
+#pragma unroll
+    for (int x = 0; x < R; x++)
+#pragma unroll
+      for (int y = 0; y < R; y++) acc[x][y] = 0.0;
+    for (int kc = 0; kc < n; kc += CK8_KC) {
+      __syncthreads();  // the previous panels are consumed
+#pragma unroll
+      for (int q = 0; q < (CK8_KC * TILE) / 256; q++) {
+        const int e = t + 256 * q;
+        const int cc = e % CK8_KC, rr = e / CK8_KC;  // 16 consecutive k of one row / column
+        const int kk = kc + cc;
+        const int i = i0 + rr, j = j0 + rr;
+        double pv = 0.0, qv = 0.0;
+        if (kk < n) {
+          if (i < ilim) {
+            if (!res) {
+              pv = (double)zz[kk + (size_t)i * ldz];  // Z(k, i)
+            } else {
+              const int lo = i < kk ? i : kk, hi = i < kk ? kk : i;  // A(i, k) from the upper triangle
+              pv = (double)(PACKED ? a[lo + (size_t)hi * (hi + 1) / 2] : a[lo + (size_t)hi * lda]);
+            }
+          }
+          if (j < m) qv = (double)zz[kk + (size_t)j * ldz];  // Z(k, j)
+        }
+        P[cc][rr] = pv;
+        Q[cc][rr] = qv;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < CK8_KC; c++) {
+        double pa[R], qb[R];
+#pragma unroll
+        for (int u = 0; u < R; u++) {
+          pa[u] = P[c][tr + 16 * u];
+          qb[u] = Q[c][tc + 16 * u];
+        }
+#pragma unroll
+        for (int x = 0; x < R; x++)
+#pragma unroll
+          for (int y = 0; y < R; y++) acc[x][y] = fma(pa[x], qb[y], acc[x][y]);
+      }
+    }
+#pragma unroll
+    for (int x = 0; x < R; x++)
+#pragma unroll
+      for (int y = 0; y < R; y++) {
+        const int i = i0 + tr + 16 * x, j = j0 + tc + 16 * y;
+        if (res) {
+          if (i < n && j < m) {
+            const double rr = acc[x][y] - (double)d[j] * (double)zz[i + (size_t)j * ldz];
+            s1 = fma(rr, rr, s1);
+          }
+        } else if (i < m && j < m && i <= j) {
+          const double rr = acc[x][y] - (i == j ? 1.0 : 0.0);
+          s2 += (i == j ? 1.0 : 2.0) * rr * rr;
+        }
+      }
+  }
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
+  if ((t & 31) == 0) {
+    red[t >> 5] = s1;
+    red[32 + (t >> 5)] = s2;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double e1 = 0.0, e2 = 0.0;
+    for (int q = 0; q < 8; q++) {
+      e1 += red[q];
+      e2 += red[32 + q];
+    }
+    e1 = sqrt(e1);
+    e2 = sqrt(e2);
+    const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
+    const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
+    const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
+    const bool f1 = e1 > dmax * TOL, f2 = e2 > n * TOL;
+    if (err1) err1[id] = e1;
+    if (err2) err2[id] = e2;
+    if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
+    if (ref_flags) {
+      float *ans = ref_flags + (size_t)id * lda * n * (sizeof(T) / sizeof(float));
+      ans[0] = (float)(f1 ? e1 / dmax : 0.0);
+      ans[1] = (float)(f2 ? e2 : 0.0);
+      ans[2] = (float)TOL;
+      ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
+    }
+  }
+}
+
 template <class T>
 __global__ void k_check_print(const long L, const int nm, const int n, const T *a_)
 {

@@ -2130,6 +2130,11 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
                       int *flags, float *ref_flags, cudaStream_t stream)
 {
   if (bad_args(L, nm, n, m) || !a0 || !w || !z) return cudaErrorInvalidValue;
+  if (n > 64) {  // 128 x 128 tiles, 8 x 8 per thread
+    if (L > 0x7fffffffL) return cudaErrorInvalidValue;
+    k_check8<T, false, 128><<<(unsigned)L, 256, 0, stream>>>(L, nm, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+    return cudaGetLastError();
+  }
   if (n > 32) {
     if (L > 0x7fffffffL) return cudaErrorInvalidValue;
     k_check_cta<T><<<(unsigned)L, 256, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
@@ -2137,6 +2142,22 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
   }
   const long blocks = std::min<long>((L + 3) / 4, 65535);
   k_check<T><<<(unsigned)blocks, 128, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+  return cudaGetLastError();
+}
+
+// The gate on a packed input (left intact by the packed solve): the tile
+// that covers n, 32 .. 128.
+template <class T>
+cudaError_t check_packed_run(long L, int n, const T *ap, const T *w, const T *z, int ldz, double *err1, double *err2,
+                             int *flags, cudaStream_t stream)
+{
+  if (L < 1 || L > 0x7fffffffL || n < 1 || n > 1024 || ldz < n || !ap || !w || !z) return cudaErrorInvalidValue;
+  if (n <= 32)
+    k_check8<T, true, 32><<<(unsigned)L, 256, 0, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+  else if (n <= 64)
+    k_check8<T, true, 64><<<(unsigned)L, 256, 0, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+  else
+    k_check8<T, true, 128><<<(unsigned)L, 256, 0, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
   return cudaGetLastError();
 }
 
@@ -2245,6 +2266,28 @@ cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap,
 {
   if (ap == nullptr) return cudaErrorInvalidValue;
   return eigb::run<float>(L, ldz, n, n, z, w, wk, lwork, info, opts, stream, ap);
+}
+
+cudaError_t eigen_GPU_batch_packed_check_DP(const int L, const int n, const double *ap, double *z, const int ldz,
+                                            double *w, void *wk, const size_t lwork, int *info,
+                                            const eigen_GPU_batch_opts *opts, double *err1, double *err2, int *flags,
+                                            const cudaStream_t stream)
+{
+  if (ap == nullptr) return cudaErrorInvalidValue;
+  const cudaError_t err = eigb::run<double>(L, ldz, n, n, z, w, wk, lwork, info, opts, stream, ap);
+  if (err != cudaSuccess) return err;
+  return eigb::check_packed_run<double>(L, n, ap, w, z, ldz, err1, err2, flags, stream);
+}
+
+cudaError_t eigen_GPU_batch_packed_check_FP(const int L, const int n, const float *ap, float *z, const int ldz,
+                                            float *w, void *wk, const size_t lwork, int *info,
+                                            const eigen_GPU_batch_opts *opts, double *err1, double *err2, int *flags,
+                                            const cudaStream_t stream)
+{
+  if (ap == nullptr) return cudaErrorInvalidValue;
+  const cudaError_t err = eigb::run<float>(L, ldz, n, n, z, w, wk, lwork, info, opts, stream, ap);
+  if (err != cudaSuccess) return err;
+  return eigb::check_packed_run<float>(L, n, ap, w, z, ldz, err1, err2, flags, stream);
 }
 
 cudaError_t eigen_GPU_batch_interleaved_BufferSize_DP(const int L, const int n, const eigen_GPU_batch_opts *opts,

@@ -110,6 +110,10 @@ def lib():
             f.argtypes = [I, I, P, P, I, P, P, SZ, P, ctypes.POINTER(Opts), P]
             f.restype = I
         for s_ in ("DP", "FP"):
+            f = getattr(L, "eigen_GPU_batch_packed_check_" + s_)
+            f.argtypes = [I, I, P, P, I, P, P, SZ, P, ctypes.POINTER(Opts), P, P, P, P]
+            f.restype = I
+        for s_ in ("DP", "FP"):
             f = getattr(L, "eigen_GPU_batch_symfunc_" + s_)
             f.argtypes = [I, I, I, P, P, P, I, ctypes.c_double, P]
             f.restype = I
@@ -208,6 +212,7 @@ def exported_symbols():
         "eigen_GPU_batch_learned_BufferSize_FP", "eigen_GPU_batch_learned_FP",
         "eigen_GPU_batch_symfunc_DP", "eigen_GPU_batch_symfunc_FP",
         "eigen_GPU_batch_packed_DP", "eigen_GPU_batch_packed_FP",
+        "eigen_GPU_batch_packed_check_DP", "eigen_GPU_batch_packed_check_FP",
         "eigen_GPU_batch_uneven_DP", "eigen_GPU_batch_uneven_FP",
         "eigen_GPU_batch_uneven_BufferSize_DP", "eigen_GPU_batch_uneven_BufferSize_FP",
         "eigen_GPU_batch_interleaved_DP", "eigen_GPU_batch_interleaved_FP",
@@ -439,6 +444,31 @@ def solve_packed(ap, n, ldz=None, method=TQL2, sort=True, max_sweep=100, stream=
     if st != 0:
         raise EigenGError(f"eigen_GPU_batch_packed failed with cudaError {st}")
     return z, w, info
+
+
+def solve_packed_checked(ap, n, ldz=None, method=TQL2, sort=True, max_sweep=100, stream=None, wk=None):
+    """eigen_GPU_batch_packed_check: the packed solve and the accuracy gate
+    in one call; returns (z, w, info, err1, err2, flags)."""
+    if not ap.is_cuda or not ap.is_contiguous() or ap.numel() % packed_size(n):
+        raise EigenGError("ap must be a contiguous CUDA tensor of L*n(n+1)/2 elements")
+    L = ap.numel() // packed_size(n)
+    ldz = n if ldz is None else ldz
+    z = torch.empty((L, n, ldz), dtype=ap.dtype, device=ap.device)
+    w = torch.empty((L, n), dtype=ap.dtype, device=ap.device)
+    info = torch.zeros(L, dtype=torch.int32, device=ap.device)
+    e1 = torch.empty(L, dtype=torch.float64, device=ap.device)
+    e2 = torch.empty(L, dtype=torch.float64, device=ap.device)
+    fl = torch.empty(L, dtype=torch.int32, device=ap.device)
+    if wk is None and method != JACOBI:
+        wk = workspace(L, ldz, n, ap.dtype, ap.device)
+    o = Opts(method, 1 if sort else 0, max_sweep, 0, 0, 0)
+    lw = 0 if wk is None else wk.numel()
+    st = getattr(lib(), "eigen_GPU_batch_packed_check_" + _sfx(ap.dtype))(
+        L, n, _ptr(ap), _ptr(z), ldz, _ptr(w), _ptr(wk), lw, _ptr(info), ctypes.byref(o), _ptr(e1), _ptr(e2),
+        _ptr(fl), _stream(stream))
+    if st != 0:
+        raise EigenGError(f"eigen_GPU_batch_packed_check failed with cudaError {st}")
+    return z, w, info, e1, e2, fl
 
 
 def solve_interleaved(ai, n, method=TQL2, sort=True, max_sweep=100, stream=None):

@@ -255,6 +255,28 @@ cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap,
                                       const cudaStream_t stream);
 
 /*
+ * Packed solve with the accuracy gate in the same call (the reference's
+ * eigen_GPU_check, eigen_GPU_check.cu:4-102, run on device as part of the
+ * solve rather than as a second pass over a copy of A): as
+ * eigen_GPU_batch_packed_*, then, on the same stream, per matrix in FP64
+ * err1 = ||A Z - Z D||_F and err2 = ||Z^T Z - I||_F from the packed input
+ * (which the solve leaves intact), z and w, and flags with the reference's
+ * thresholds (bit 0: err1 > max(|w_1|,|w_n|) TOL, bit 1: err2 > n TOL;
+ * TOL = EPS (2*512-1) sqrt(n+16) for FP64, eps (2*16-1) sqrt(n+16) for
+ * FP32).  err1, err2 and flags are device arrays of L entries; any may be
+ * NULL.  The norms equal eigen_GPU_check_ex_*'s on the full matrices up to
+ * the order of the FP64 sums.
+ */
+cudaError_t eigen_GPU_batch_packed_check_DP(const int L, const int n, const double *ap, double *z, const int ldz,
+                                            double *w, void *wk, const size_t lwork, int *info,
+                                            const eigen_GPU_batch_opts *opts, double *err1, double *err2, int *flags,
+                                            const cudaStream_t stream);
+cudaError_t eigen_GPU_batch_packed_check_FP(const int L, const int n, const float *ap, float *z, const int ldz,
+                                            float *w, void *wk, const size_t lwork, int *info,
+                                            const eigen_GPU_batch_opts *opts, double *err1, double *err2, int *flags,
+                                            const cudaStream_t stream);
+
+/*
  * Interleaved layout (the reference's README:166 "flexible interleave data
  * format", not in its code): element (i, j) of matrix k (0-based) at
  * ai[(i + j*n)*L + k], i.e. the same element of every matrix contiguous, as

@@ -62,3 +62,31 @@ def test_interleaved_matches_full(oracle_mod, n, L, dtype):
     assert torch.equal(info, infof) and (info == 0).all()
     assert torch.equal(wi.t(), wf)
     assert torch.equal(zi.t().reshape(L, n, n), a)
+
+
+@pytest.mark.parametrize("n,ldz", [(2, 2), (17, 17), (32, 33), (33, 33), (64, 64), (65, 66), (128, 128),
+                                   (129, 129), (200, 200), (256, 256), (300, 300)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_packed_check_matches_the_gate(oracle_mod, n, ldz, dtype):
+    """The packed solve with the gate in the same call: the same eigenpairs
+    as eigen_GPU_batch_packed_*, and err1, err2 and flags of
+    eigen_GPU_check_ex_* on the full matrices, norms within 1e-6 relative
+    (the FP64 sums run in another order)."""
+    O = oracle_mod
+    L = 5
+    a0 = np.zeros((L, n, ldz))
+    a0[:, :, :n] = O.sym_uniform(L, n, seed=n + 29)
+    a = torch.from_numpy(a0.astype(dtype)).cuda()
+    ap = E().pack_upper(a, n, ldz)
+    ap0 = ap.clone()
+    z, w, info, e1, e2, fl = E().solve_packed_checked(ap, n, ldz)
+    zp, wp, ip = E().solve_packed(ap, n, ldz)
+    torch.cuda.synchronize()
+    assert torch.equal(ap, ap0) and torch.equal(z, zp) and torch.equal(w, wp) and (info == 0).all()
+    g1, g2, gf = E().check(a, w, z, n, ldz)
+    torch.cuda.synchronize()
+    assert torch.equal(fl, gf) and (fl == 0).all()
+    r1 = ((e1 - g1).abs() / g1.abs().clamp_min(1e-300)).max().item()
+    r2 = ((e2 - g2).abs() / g2.abs().clamp_min(1e-300)).max().item()
+    assert r1 <= 1e-6 and r2 <= 1e-6, (r1, r2)
+
