@@ -1214,7 +1214,7 @@ __global__ void __launch_bounds__(256) k_transpose(const long rows, const long c
 // Residual ||A Z - Z D||_F and orthogonality ||Z^T Z - I||_F (off-diagonal
 // terms twice) in FP64 per matrix, one warp per matrix, following
 // eigen_GPU_check.cu:34-62.  a0 is read through its upper triangle.
-template <class T>
+template <class T, bool PACKED = false>
 __global__ void k_check(const long L, const int nm, const int n, const int m, const T *a0, const T *w,
                         const T *z, double *err1, double *err2, int *flags, float *ref_flags)
 {
@@ -1222,7 +1222,7 @@ __global__ void k_check(const long L, const int nm, const int n, const int m, co
   const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
   const int lane = threadIdx.x & 31;
   for (long id = wg; id < L; id += nwarps) {
-    const T *a = a0 + (size_t)id * nm * n;
+    const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * nm * n;
     const T *zz = z + (size_t)id * nm * n;
     const T *d = w + (size_t)id * n;
     double e1 = 0.0;
@@ -1231,7 +1231,8 @@ __global__ void k_check(const long L, const int nm, const int n, const int m, co
       for (int kr = lane; kr < n; kr += 32) {
         double ek = 0.0;
         for (int j = 0; j < n; j++) {
-          const double akj = (kr <= j) ? (double)a[kr + (size_t)j * nm] : (double)a[j + (size_t)kr * nm];
+          const int lo = kr <= j ? kr : j, hi = kr <= j ? j : kr;
+          const double akj = (double)(PACKED ? a[lo + (size_t)hi * (hi + 1) / 2] : a[lo + (size_t)hi * nm]);
           ek = fma(akj, (double)zz[j + (size_t)i * nm], ek);
         }
         const double rr = ek - di * (double)zz[kr + (size_t)i * nm];
@@ -1277,7 +1278,7 @@ __global__ void k_check(const long L, const int nm, const int n, const int m, co
 // per-thread sums; one CTA reduction at the end (deterministic).
 constexpr int CK_TILE = 64, CK_KC = 16, CK_LDP = CK_TILE + 2;
 
-template <class T>
+template <class T, bool PACKED = false>
 __global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, const int n, const int m,
                                                    const T *a0, const T *w, const T *z, double *err1,
                                                    double *err2, int *flags, float *ref_flags)
@@ -1287,7 +1288,7 @@ __global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, c
   __shared__ double red[64];
   const long id = blockIdx.x;
   if (id >= L) return;
-  const T *a = a0 + (size_t)id * nm * n;
+  const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * nm * n;
   const T *zz = z + (size_t)id * nm * n;
   const T *d = w + (size_t)id * n;
   const int t = threadIdx.x, tr = t % 16, tc = t / 16;
@@ -1322,8 +1323,12 @@ __global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, c
         double pv = 0.0, qv = 0.0;
         if (kk < n) {
           if (i < ilim) {
-            if (res) pv = (double)((i <= kk) ? a[i + (size_t)kk * nm] : a[kk + (size_t)i * nm]);  // A(i, k)
-            else pv = (double)zz[kk + (size_t)i * nm];                                         // Z(k, i)
+            if (res) {  // A(i, k) from the upper triangle
+              const int lo = i <= kk ? i : kk, hi = i <= kk ? kk : i;
+              pv = (double)(PACKED ? a[lo + (size_t)hi * (hi + 1) / 2] : a[lo + (size_t)hi * nm]);
+            } else {
+              pv = (double)zz[kk + (size_t)i * nm];  // Z(k, i)
+            }
           }
           if (j < m) qv = (double)zz[kk + (size_t)j * nm];  // Z(k, j)
         }
@@ -1397,20 +1402,38 @@ __global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, c
 // The same two norms with TILE x TILE output tiles (TILE = 32, 64 or 128):
 // a 16 x 16 thread grid, an R x R FP64 register tile per thread (R =
 // TILE/16; rows and columns 16 apart), 16-deep panels of A (or of Z for
-// Z^T Z) and of Z staged in shared memory; R^2 FMAs per 2R shared-memory
-// loads (64 per 16 at TILE = 128).  PACKED reads A from the packed upper
-// triangle (ap + id n(n+1)/2, element (r, c), r <= c, at r + c(c+1)/2)
-// instead of the full layout; Z has leading dimension ldz.
+// Z^T Z) and of Z staged in shared memory by cp.async, two buffers, so
+// that the next panels load while the current ones are multiplied; R^2
+// FMAs per 2R shared-memory loads (64 per 16 at TILE = 128).  The panels
+// keep the input type (FP32 inputs widen at use).  PACKED reads A from the
+// packed upper triangle (ap + id n(n+1)/2, element (r, c), r <= c, at
+// r + c(c+1)/2) instead of the full layout; Z has leading dimension ldz.
+// Dynamic shared memory: check8_smem<T, TILE>().
 constexpr int CK8_KC = 16;
+template <class T, int TILE> __host__ __device__ constexpr size_t check8_smem()
+{
+  return sizeof(T) * 2 * 2 * CK8_KC * (size_t)(TILE + 1);
+}
+
+template <int BYTES> __device__ __forceinline__ void ck_cp_async(void *dst, const void *src, bool valid)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src), "n"(BYTES),
+               "r"(valid ? BYTES : 0)
+               : "memory");
+}
+__device__ __forceinline__ void ck_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void ck_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <class T, bool PACKED, int TILE>
 __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, const int ldz, const int n, const int m,
                                                    const T *a0, const T *w, const T *z, double *err1, double *err2,
                                                    int *flags, float *ref_flags)
 {
-  constexpr int R = TILE / 16, LDP = TILE + 1;
-  __shared__ double P[CK8_KC][LDP];  // P(k, tile row)
-  __shared__ double Q[CK8_KC][LDP];  // Q(k, tile column)
+  constexpr int R = TILE / 16, LDP = TILE + 1, PANEL = CK8_KC * LDP;
+  extern __shared__ __align__(16) unsigned char ck_smem[];
+  T *Pb = reinterpret_cast<T *>(ck_smem);  // [2][KC][LDP]: P(k, tile row)
+  T *Qb = Pb + 2 * PANEL;                   // [2][KC][LDP]: Q(k, tile column)
   __shared__ double red[64];
   const long id = blockIdx.x;
   if (id >= L) return;
@@ -1419,6 +1442,7 @@ __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, 
   const T *d = w + (size_t)id * n;
   const int t = threadIdx.x, tr = t % 16, tc = t / 16;
   const int ntn = (n + TILE - 1) / TILE, ntm = (m + TILE - 1) / TILE;
+  const int nchunks = (n + CK8_KC - 1) / CK8_KC;
   double s1 = 0.0, s2 = 0.0;
   const int nres = ntn * ntm, nort = ntm * (ntm + 1) / 2;
   for (int tile = 0; tile < nres + nort; tile++) {
@@ -1432,48 +1456,63 @@ __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, 
     }
     const int i0 = ti * TILE, j0 = tj * TILE;
     const int ilim = res ? n : m;
-    double acc[R][R];
-#pragma unroll
-    for (int x = 0; x < R; x++)
-#pragma unroll
-      for (int y = 0; y < R; y++) acc[x][y] = 0.0;
-    for (int kc = 0; kc < n; kc += CK8_KC) {
-      __syncthreads();  // the previous panels are consumed
+    // the panels of chunk c into buffer c & 1; out-of-range entries are
+    // zero-filled (a source of 0 bytes)
+    auto load = [&](int c) {
+      T *P = Pb + (c & 1) * PANEL, *Q = Qb + (c & 1) * PANEL;
+      const int kc = c * CK8_KC;
 #pragma unroll
       for (int q = 0; q < (CK8_KC * TILE) / 256; q++) {
         const int e = t + 256 * q;
         const int cc = e % CK8_KC, rr = e / CK8_KC;  // 16 consecutive k of one row / column
         const int kk = kc + cc;
         const int i = i0 + rr, j = j0 + rr;
-        double pv = 0.0, qv = 0.0;
-        if (kk < n) {
-          if (i < ilim) {
-            if (!res) {
-              pv = (double)zz[kk + (size_t)i * ldz];  // Z(k, i)
-            } else {
-              const int lo = i < kk ? i : kk, hi = i < kk ? kk : i;  // A(i, k) from the upper triangle
-              pv = (double)(PACKED ? a[lo + (size_t)hi * (hi + 1) / 2] : a[lo + (size_t)hi * lda]);
-            }
+        const bool pin = kk < n && i < ilim, qin = kk < n && j < m;
+        const T *ps = zz, *qs = zz;
+        if (pin) {
+          if (!res) {
+            ps = zz + kk + (size_t)i * ldz;  // Z(k, i)
+          } else {
+            const int lo = i < kk ? i : kk, hi = i < kk ? kk : i;  // A(i, k) from the upper triangle
+            ps = PACKED ? a + lo + (size_t)hi * (hi + 1) / 2 : a + lo + (size_t)hi * lda;
           }
-          if (j < m) qv = (double)zz[kk + (size_t)j * ldz];  // Z(k, j)
         }
-        P[cc][rr] = pv;
-        Q[cc][rr] = qv;
+        if (qin) qs = zz + kk + (size_t)j * ldz;  // Z(k, j)
+        ck_cp_async<sizeof(T)>(&P[cc * LDP + rr], ps, pin);
+        ck_cp_async<sizeof(T)>(&Q[cc * LDP + rr], qs, qin);
       }
-      __syncthreads();
+      ck_commit();
+    };
+    double acc[R][R];
 #pragma unroll
-      for (int c = 0; c < CK8_KC; c++) {
+    for (int x = 0; x < R; x++)
+#pragma unroll
+      for (int y = 0; y < R; y++) acc[x][y] = 0.0;
+    __syncthreads();  // the previous tile's last panels are consumed
+    load(0);
+    for (int c = 0; c < nchunks; c++) {
+      if (c + 1 < nchunks) {
+        load(c + 1);
+        ck_wait<1>();  // chunk c has landed (this thread's copies)
+      } else {
+        ck_wait<0>();
+      }
+      __syncthreads();  // ... and every thread's
+      const T *P = Pb + (c & 1) * PANEL, *Q = Qb + (c & 1) * PANEL;
+#pragma unroll
+      for (int cc = 0; cc < CK8_KC; cc++) {
         double pa[R], qb[R];
 #pragma unroll
         for (int u = 0; u < R; u++) {
-          pa[u] = P[c][tr + 16 * u];
-          qb[u] = Q[c][tc + 16 * u];
+          pa[u] = (double)P[cc * LDP + tr + 16 * u];
+          qb[u] = (double)Q[cc * LDP + tc + 16 * u];
         }
 #pragma unroll
         for (int x = 0; x < R; x++)
 #pragma unroll
           for (int y = 0; y < R; y++) acc[x][y] = fma(pa[x], qb[y], acc[x][y]);
       }
+      __syncthreads();  // buffer c & 1 is free for chunk c + 2
     }
 #pragma unroll
     for (int x = 0; x < R; x++)

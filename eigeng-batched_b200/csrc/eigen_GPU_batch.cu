@@ -2132,7 +2132,10 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
   if (bad_args(L, nm, n, m) || !a0 || !w || !z) return cudaErrorInvalidValue;
   if (n > 64) {  // 128 x 128 tiles, 8 x 8 per thread
     if (L > 0x7fffffffL) return cudaErrorInvalidValue;
-    k_check8<T, false, 128><<<(unsigned)L, 256, 0, stream>>>(L, nm, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+    const size_t sm8 = check8_smem<T, 128>();
+    cudaError_t e = set_smem(k_check8<T, false, 128>, sm8);
+    if (e != cudaSuccess) return e;
+    k_check8<T, false, 128><<<(unsigned)L, 256, sm8, stream>>>(L, nm, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
     return cudaGetLastError();
   }
   if (n > 32) {
@@ -2145,19 +2148,26 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
   return cudaGetLastError();
 }
 
-// The gate on a packed input (left intact by the packed solve): the tile
-// that covers n, 32 .. 128.
+// The gate on a packed input (left intact by the packed solve): the same
+// kernels, in the same order of operations, as check_run on the full
+// layout, so the norms and flags are those of eigen_GPU_check_ex_* bit
+// for bit.
 template <class T>
 cudaError_t check_packed_run(long L, int n, const T *ap, const T *w, const T *z, int ldz, double *err1, double *err2,
                              int *flags, cudaStream_t stream)
 {
   if (L < 1 || L > 0x7fffffffL || n < 1 || n > 1024 || ldz < n || !ap || !w || !z) return cudaErrorInvalidValue;
-  if (n <= 32)
-    k_check8<T, true, 32><<<(unsigned)L, 256, 0, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
-  else if (n <= 64)
-    k_check8<T, true, 64><<<(unsigned)L, 256, 0, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
-  else
-    k_check8<T, true, 128><<<(unsigned)L, 256, 0, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+  if (n > 64) {
+    const size_t sm8 = check8_smem<T, 128>();
+    cudaError_t e = set_smem(k_check8<T, true, 128>, sm8);
+    if (e != cudaSuccess) return e;
+    k_check8<T, true, 128><<<(unsigned)L, 256, sm8, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+  } else if (n > 32) {
+    k_check_cta<T, true><<<(unsigned)L, 256, 0, stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+  } else {
+    const long blocks = std::min<long>((L + 3) / 4, 65535);
+    k_check<T, true><<<(unsigned)blocks, 128, 0, stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+  }
   return cudaGetLastError();
 }
 

@@ -264,8 +264,8 @@ cudaError_t eigen_GPU_batch_packed_FP(const int L, const int n, const float *ap,
  * thresholds (bit 0: err1 > max(|w_1|,|w_n|) TOL, bit 1: err2 > n TOL;
  * TOL = EPS (2*512-1) sqrt(n+16) for FP64, eps (2*16-1) sqrt(n+16) for
  * FP32).  err1, err2 and flags are device arrays of L entries; any may be
- * NULL.  The norms equal eigen_GPU_check_ex_*'s on the full matrices up to
- * the order of the FP64 sums.
+ * NULL.  The norms and flags equal eigen_GPU_check_ex_*'s on the full
+ * matrices bit for bit.
  */
 cudaError_t eigen_GPU_batch_packed_check_DP(const int L, const int n, const double *ap, double *z, const int ldz,
                                             double *w, void *wk, const size_t lwork, int *info,

@@ -70,8 +70,8 @@ def test_interleaved_matches_full(oracle_mod, n, L, dtype):
 def test_packed_check_matches_the_gate(oracle_mod, n, ldz, dtype):
     """The packed solve with the gate in the same call: the same eigenpairs
     as eigen_GPU_batch_packed_*, and err1, err2 and flags of
-    eigen_GPU_check_ex_* on the full matrices, norms within 1e-6 relative
-    (the FP64 sums run in another order)."""
+    eigen_GPU_check_ex_* on the full matrices, bit for bit (the same
+    kernels read the packed triangle instead of the full matrix)."""
     O = oracle_mod
     L = 5
     a0 = np.zeros((L, n, ldz))
@@ -82,11 +82,11 @@ def test_packed_check_matches_the_gate(oracle_mod, n, ldz, dtype):
     z, w, info, e1, e2, fl = E().solve_packed_checked(ap, n, ldz)
     zp, wp, ip = E().solve_packed(ap, n, ldz)
     torch.cuda.synchronize()
-    assert torch.equal(ap, ap0) and torch.equal(z, zp) and torch.equal(w, wp) and (info == 0).all()
+    # rows n .. ldz-1 of each column of z are padding, never written
+    assert torch.equal(ap, ap0) and torch.equal(z[:, :, :n], zp[:, :, :n]) and torch.equal(w, wp)
+    assert (info == 0).all()
     g1, g2, gf = E().check(a, w, z, n, ldz)
     torch.cuda.synchronize()
     assert torch.equal(fl, gf) and (fl == 0).all()
-    r1 = ((e1 - g1).abs() / g1.abs().clamp_min(1e-300)).max().item()
-    r2 = ((e2 - g2).abs() / g2.abs().clamp_min(1e-300)).max().item()
-    assert r1 <= 1e-6 and r2 <= 1e-6, (r1, r2)
+    assert torch.equal(e1, g1) and torch.equal(e2, g2)
 
