@@ -97,9 +97,15 @@ template <class T> __host__ __device__ constexpr int k1w_slot() { return K1W_LD 
 // B200, phase 1 in ms at four per row / two per row: n=136 20.6 / 15.9,
 // n=160 27.8 / 23.5, n=192 47.8 / 41.7, n=224 34.5 / 32.4 (L=2048), n=240
 // 44.2 / 42.6; at n=256 52.4 against 51.0, so four stay there.
+// FP32 likewise gains from more CTAs per SM (with k1c_block's smaller
+// blocks): phase 1 in ms, the largest block at four / two per row against
+// the kept form: n=144 18.4 -> 11.5 (one per row, 64 x 64), n=192 32.2 ->
+// 24.9 (one, 64), n=256 37.8 -> 31.6 (two, 128), n=384 75.1 -> 62.2 (two,
+// 128), n=512 97.5 -> 79.8 (one, 128).
 template <class T> __host__ __device__ constexpr int k1_split(int n)
 {
-  return (sizeof(T) == 8 && n <= 240) ? 2 : (n <= 256 ? 4 : (n <= 512 ? 2 : 1));
+  return sizeof(T) == 8 ? (n <= 240 ? 2 : (n <= 256 ? 4 : (n <= 512 ? 2 : 1)))
+                        : (n <= 128 ? 4 : (n <= 224 ? 1 : (n <= 448 ? 2 : 1)));
 }
 
 // ---------------------------------------------------------------- n == 1

@@ -145,9 +145,9 @@ template <class T> int k1c_threads(int n) { return std::min(1024, ((n + 31) / 32
 // matrix when it fits; otherwise the largest that fits next to the scratch
 // arrays, for FP64 at most 128 x 128, which leaves L1 room for the outer
 // band (measured on B200 at n = 200 and 256: 15-20 % faster than the
-// largest block; FP32 is fastest with the largest).  FP64 128 < n <= 240
-// keeps a 64 x 64 (n <= 176) or 96 x 96 block: more CTAs per SM pay more
-// than a larger block (see k1_split)
+// largest block).  FP64 128 < n <= 240 keeps a 64 x 64 (n <= 176) or
+// 96 x 96 block, FP32 128 < n <= 512 a 64 x 64 (n <= 224) or 128 x 128
+// one: more CTAs per SM pay more than a larger block (see k1_split)
 template <class T> int k1c_block(int n, size_t optin)
 {
   const size_t base = sizeof(T) * k1c_smem_elems(n, k1c_threads<T>(n), 0);
@@ -155,6 +155,7 @@ template <class T> int k1c_block(int n, size_t optin)
   int B = n;
   if (sizeof(T) == 8 && base + sizeof(T) * (size_t)n * (size_t)(n | 1) > optin) B = std::min(n, 128);
   if (sizeof(T) == 8 && n > 128 && n <= 240) B = n <= 176 ? 64 : 96;
+  if (sizeof(T) == 4 && n > 128 && n <= 512) B = std::min(B, n <= 224 ? 64 : 128);
   while (B > 0 && base + sizeof(T) * (size_t)B * (size_t)(B | 1) > optin) B--;
   return B;
 }
