@@ -129,9 +129,11 @@ __global__ void k_lw_v0rows(const int n, const float *__restrict__ v0, bf16 *__r
 // ascending order of the eigenvalues mu), mu, and the sweeps it took
 // (-1: G was not positive definite; the gate then fails the matrix).
 __host__ __device__ inline int lw_ld(int n) { return n + 1; }
+// two n x ld matrices (B; L, then V), so that three CTAs share an SM: the
+// Cholesky factor waits in the output buffer Y while V is rotated
 __host__ __device__ inline size_t lw_polish_smem(int n)
 {
-  return sizeof(double) * (3 * (size_t)n * lw_ld(n) + 2 * (size_t)n + 64) + sizeof(int) * (size_t)n + 64;
+  return sizeof(double) * (2 * (size_t)n * lw_ld(n) + 2 * (size_t)n + 64) + sizeof(int) * (3 * (size_t)n + 2) + 64;
 }
 
 __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__restrict__ S,
@@ -142,11 +144,12 @@ __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__
   extern __shared__ __align__(16) unsigned char lp_smem[];
   const int ld = lw_ld(n);
   double *Bm = reinterpret_cast<double *>(lp_smem);  // n x ld, row-major: B[i*ld + j]
-  double *Lm = Bm + (size_t)n * ld;                   // Cholesky factor, then scratch
-  double *Vm = Lm + (size_t)n * ld;                   // rotations
+  double *Lm = Bm + (size_t)n * ld;                   // the Cholesky factor ...
+  double *Vm = Lm;                                    // ... then the rotations
   double *cs = Vm + (size_t)n * ld;                   // 2 per pair
   double *red = cs + 2 * n;
   int *perm = reinterpret_cast<int *>(red + 64);
+  int *pq = perm + n;                                  // the pairs of a round, 2 per pair
   __shared__ int bad;
   const long b = blockIdx.x;
   const int tid = threadIdx.x;
@@ -191,6 +194,11 @@ __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__
     }
     __syncthreads();
   }
+  // L aside in this matrix's output slot (row-major, n x n) until the
+  // back substitution; its shared-memory area takes V
+  double *Yb = Y + (size_t)b * n * n;
+  for (int idx = tid; idx < n * n; idx += 256) Yb[idx] = Lm[(idx / n) * ld + idx % n];
+  __syncthreads();
   for (int idx = tid; idx < n * n; idx += 256) {
     const int i = idx / n, j = idx % n;
     Vm[i * ld + j] = (i == j) ? 1.0 : 0.0;
@@ -235,39 +243,45 @@ __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__
         }
         cs[2 * tid] = c;
         cs[2 * tid + 1] = s;
+        pq[2 * tid] = p;
+        pq[2 * tid + 1] = q;
       }
       __syncthreads();
-      // rows p, q of B
-      for (int idx = tid; idx < half * n; idx += 256) {
-        const int k = idx / n, l = idx % n;
-        int p = k == 0 ? r : (r + k) % m, q = k == 0 ? m : (r - k + m) % m;
-        if (p > q) {
-          const int t = p;
-          p = q;
-          q = t;
-        }
-        if (q < n) {
-          const double c = cs[2 * k], s = cs[2 * k + 1];
-          const double bp = Bm[p * ld + l], bq = Bm[q * ld + l];
-          Bm[p * ld + l] = c * bp - s * bq;
-          Bm[q * ld + l] = s * bp + c * bq;
+      // B <- J^T B J in one pass: the pairs are disjoint, so entry (i, j)
+      // depends only on the 2 x 2 block of the pairs of i and of j; the
+      // rows are rotated first, then the columns, as two separate passes
+      // over B would (same operations, same order)
+      for (int idx = tid; idx < half * half; idx += 256) {
+        const int ka = idx / half, kb = idx % half;
+        const int p = pq[2 * ka], q = pq[2 * ka + 1], p2 = pq[2 * kb], q2 = pq[2 * kb + 1];
+        if (q < n && q2 < n) {
+          const double ca = cs[2 * ka], sa = cs[2 * ka + 1], cb = cs[2 * kb], sb = cs[2 * kb + 1];
+          const double b00 = Bm[p * ld + p2], b01 = Bm[p * ld + q2], b10 = Bm[q * ld + p2], b11 = Bm[q * ld + q2];
+          const double r00 = ca * b00 - sa * b10, r10 = sa * b00 + ca * b10;  // rows p, q
+          const double r01 = ca * b01 - sa * b11, r11 = sa * b01 + ca * b11;
+          Bm[p * ld + p2] = cb * r00 - sb * r01;  // columns p2, q2
+          Bm[p * ld + q2] = sb * r00 + cb * r01;
+          Bm[q * ld + p2] = cb * r10 - sb * r11;
+          Bm[q * ld + q2] = sb * r10 + cb * r11;
+        } else if (q2 < n) {  // pair ka is the dummy of odd n: p < n, only the columns turn
+          const double cb = cs[2 * kb], sb = cs[2 * kb + 1];
+          const double b0 = Bm[p * ld + p2], b1 = Bm[p * ld + q2];
+          Bm[p * ld + p2] = cb * b0 - sb * b1;
+          Bm[p * ld + q2] = sb * b0 + cb * b1;
+        } else if (q < n) {  // pair kb is the dummy: only the rows turn
+          const double ca = cs[2 * ka], sa = cs[2 * ka + 1];
+          const double b0 = Bm[p * ld + p2], b1 = Bm[q * ld + p2];
+          Bm[p * ld + p2] = ca * b0 - sa * b1;
+          Bm[q * ld + p2] = sa * b0 + ca * b1;
+        } else {  // both dummies: entry (p, p2), untouched
         }
       }
-      __syncthreads();
-      // columns p, q of B and V
+      // columns p, q of V
       for (int idx = tid; idx < half * n; idx += 256) {
         const int k = idx / n, l = idx % n;
-        int p = k == 0 ? r : (r + k) % m, q = k == 0 ? m : (r - k + m) % m;
-        if (p > q) {
-          const int t = p;
-          p = q;
-          q = t;
-        }
+        const int p = pq[2 * k], q = pq[2 * k + 1];
         if (q < n) {
           const double c = cs[2 * k], s = cs[2 * k + 1];
-          const double bp = Bm[l * ld + p], bq = Bm[l * ld + q];
-          Bm[l * ld + p] = c * bp - s * bq;
-          Bm[l * ld + q] = s * bp + c * bq;
           const double vp = Vm[l * ld + p], vq = Vm[l * ld + q];
           Vm[l * ld + p] = c * vp - s * vq;
           Vm[l * ld + q] = s * vp + c * vq;
@@ -287,17 +301,28 @@ __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__
     perm[rk] = i;
   }
   __syncthreads();
-  // Y = L^-T V (back substitution, columns in parallel), column q of Y
-  // holds eigenvector perm[q]
-  double *Yb = Y + (size_t)b * n * n;
+  // Y = L^-T V (back substitution, columns in parallel, each in place over
+  // its column of V), column q of Y holds eigenvector perm[q]; L comes back
+  // into B's area once B's diagonal, the eigenvalues, has been read
+  double muq = 0.0;
+  if (tid < n) muq = Bm[perm[tid] * ld + perm[tid]];
+  __syncthreads();  // B is free
+  double *L2 = Bm;
+  for (int idx = tid; idx < n * n; idx += 256) L2[(idx / n) * ld + idx % n] = Yb[idx];
+  __syncthreads();  // the output slot is free
   if (tid < n) {
     const int col = perm[tid];
     for (int i = n - 1; i >= 0; i--) {
       double s = Vm[i * ld + col];
-      for (int k = i + 1; k < n; k++) s -= Lm[k * ld + i] * Yb[(size_t)tid * n + k];
-      Yb[(size_t)tid * n + i] = s / Lm[i * ld + i];
+      for (int k = i + 1; k < n; k++) s -= L2[k * ld + i] * Vm[k * ld + col];
+      Vm[i * ld + col] = s / L2[i * ld + i];
     }
-    mu[(size_t)b * n + tid] = Bm[col * ld + col];
+    mu[(size_t)b * n + tid] = muq;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < n * n; idx += 256) {
+    const int i = idx % n, q = idx / n;
+    Yb[(size_t)q * n + i] = Vm[i * ld + perm[q]];
   }
   if (tid == 0) sweeps[b] = bad ? -1 : sw;
 }
