@@ -19,8 +19,9 @@
 //   k3_tmem        phase 3 for n > 32 with rows of up to 512 32-bit
 //                  columns: rows of Z in tensor memory
 //   k_jacobi_warp  cyclic Jacobi for n <= 32 (jac_tiled.hpp:3-152)
-//   k_check        FP64 residual / orthogonality gate (eigen_GPU_check.cu),
-//                  one warp per matrix; k_check_cta the tiled form for n > 32
+//   k_check_w      FP64 residual / orthogonality gate (eigen_GPU_check.cu),
+//                  one warp per matrix for n <= 32; k_check_cta (n <= 64)
+//                  and k_check8 (above) the tiled forms
 #pragma once
 #include <stdio.h>
 
@@ -1218,66 +1219,13 @@ __global__ void __launch_bounds__(256) k_transpose(const long rows, const long c
 
 // ---------------------------------------------------------------- check
 // Residual ||A Z - Z D||_F and orthogonality ||Z^T Z - I||_F (off-diagonal
-// terms twice) in FP64 per matrix, one warp per matrix, following
-// eigen_GPU_check.cu:34-62.  a0 is read through its upper triangle.
-template <class T, bool PACKED = false>
-__global__ void k_check(const long L, const int nm, const int n, const int m, const T *a0, const T *w,
-                        const T *z, double *err1, double *err2, int *flags, float *ref_flags)
-{
-  const long wg = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  for (long id = wg; id < L; id += nwarps) {
-    const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * nm * n;
-    const T *zz = z + (size_t)id * nm * n;
-    const T *d = w + (size_t)id * n;
-    double e1 = 0.0;
-    for (int i = 0; i < m; i++) {
-      const double di = (double)d[i];
-      for (int kr = lane; kr < n; kr += 32) {
-        double ek = 0.0;
-        for (int j = 0; j < n; j++) {
-          const int lo = kr <= j ? kr : j, hi = kr <= j ? j : kr;
-          const double akj = (double)(PACKED ? a[lo + (size_t)hi * (hi + 1) / 2] : a[lo + (size_t)hi * nm]);
-          ek = fma(akj, (double)zz[j + (size_t)i * nm], ek);
-        }
-        const double rr = ek - di * (double)zz[kr + (size_t)i * nm];
-        e1 = fma(rr, rr, e1);
-      }
-    }
-    e1 = sqrt(warp_sum(e1));
-    double e2 = 0.0;
-    for (int i = 0; i < m; i++) {
-      for (int j = i; j < m; j++) {
-        double rr = 0.0;
-        for (int kr = lane; kr < n; kr += 32)
-          rr = fma((double)zz[kr + (size_t)i * nm], (double)zz[kr + (size_t)j * nm], rr);
-        rr = warp_sum(rr);
-        rr -= (i == j) ? 1.0 : 0.0;
-        e2 += ((i == j) ? 1.0 : 2.0) * rr * rr;
-      }
-    }
-    e2 = sqrt(e2);
-    if (lane == 0) {
-      const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
-      const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
-      const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
-      const bool f1 = e1 > dmax * TOL, f2 = e2 > n * TOL;
-      if (err1) err1[id] = e1;
-      if (err2) err2[id] = e2;
-      if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
-      if (ref_flags) {  // the reference stores the verdict into the input copy, eigen_GPU_check.cu:76-80
-        float *ans = ref_flags + (size_t)id * nm * n * (sizeof(T) / sizeof(float));
-        ans[0] = (float)(f1 ? e1 / dmax : 0.0);
-        ans[1] = (float)(f2 ? e2 : 0.0);
-        ans[2] = (float)TOL;
-        ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
-      }
-    }
-  }
-}
-
-// The same two norms for n > 32, one CTA of 256 threads per matrix: the
+// terms twice) in FP64 per matrix, over the first m eigenpairs, and the
+// reference's flags (eigen_GPU_check.cu:34-74): bit 0 when the residual
+// exceeds max(|w_1|, |w_n|) TOL, bit 1 when the orthogonality exceeds
+// n TOL.  Three forms by size: k_check_w (n <= 32), k_check_cta (n <= 64),
+// k_check8 (above).
+//
+// k_check_cta, for 32 < n <= 64, one CTA of 256 threads per matrix: the
 // products A Z (n x m) and Z^T Z (upper triangle, m x m) are formed tile by
 // tile (64 x 64, 16-row panels staged in shared memory, a 4 x 4 FP64
 // register tile per thread, rows and columns 16 apart) and squared into
@@ -1405,7 +1353,127 @@ __global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, c
   }
 }
 
-// The same two norms with TILE x TILE output tiles (TILE = 32, 64 or 128):
+// k_check_w, for n <= 32, one warp per matrix (4 per CTA): A (full
+// symmetric, from the upper triangle or the packed one) and Z staged in
+// shared memory as FP64 (per warp 2 x 32 x 33); lane r forms row r of A Z
+// with its row of A in registers (the columns of Z broadcast) and row r of
+// the upper triangle of Z^T Z with its column of Z in registers.  Dynamic
+// shared memory: check_w_smem().
+constexpr int CKW_WARPS = 4;
+__host__ __device__ constexpr size_t check_w_smem() { return sizeof(double) * 2 * 32 * 33 * CKW_WARPS; }
+
+template <class T, bool PACKED>
+__global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const int nm, const int n, const int m,
+                                                            const T *a0, const T *w, const T *z, double *err1,
+                                                            double *err2, int *flags, float *ref_flags)
+{
+  extern __shared__ __align__(16) unsigned char ckw_smem[];
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *As = reinterpret_cast<double *>(ckw_smem) + (size_t)wid * 2 * 32 * 33;  // As[r * 33 + c]
+  double *Zs = As + 32 * 33;                                                        // Zs[r * 33 + i] = Z(r, i)
+  const long nw = (long)gridDim.x * CKW_WARPS;
+  for (long id = (long)blockIdx.x * CKW_WARPS + wid; id < L; id += nw) {
+    const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * nm * n;
+    const T *zz = z + (size_t)id * nm * n;
+    const T *d = w + (size_t)id * n;
+    __syncwarp();  // the previous matrix's reads are done
+    // eight loads in flight per lane before their stores (a store to shared
+    // memory would otherwise wait for each load in turn)
+    for (int i0 = 0; i0 < n * n; i0 += 8 * 32) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 32 + lane, r = idx % n, c = idx / n;
+        v[u] = (idx < n * n && r <= c) ? (double)(PACKED ? a[r + (size_t)c * (c + 1) / 2] : a[r + (size_t)c * nm])
+                                       : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 32 + lane, r = idx % n, c = idx / n;
+        if (idx < n * n && r <= c) {
+          As[r * 33 + c] = v[u];
+          As[c * 33 + r] = v[u];
+        }
+      }
+    }
+    for (int i0 = 0; i0 < n * m; i0 += 8 * 32) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 32 + lane;
+        v[u] = idx < n * m ? (double)zz[idx % n + (size_t)(idx / n) * nm] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 32 + lane;
+        if (idx < n * m) Zs[(idx % n) * 33 + idx / n] = v[u];
+      }
+    }
+    __syncwarp();
+    double e1 = 0.0, e2 = 0.0;
+    if (lane < n) {
+      double ar[32];
+#pragma unroll
+      for (int j = 0; j < 32; j++) ar[j] = j < n ? As[lane * 33 + j] : 0.0;
+      for (int i0 = 0; i0 < m; i0 += 4) {  // four columns, four independent chains
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+          if (j < n) {
+#pragma unroll
+            for (int u = 0; u < 4; u++) acc[u] = fma(ar[j], Zs[j * 33 + min(i0 + u, 31)], acc[u]);
+          }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (i0 + u < m) {
+            const double rr = acc[u] - (double)d[i0 + u] * Zs[lane * 33 + i0 + u];
+            e1 = fma(rr, rr, e1);
+          }
+      }
+    }
+    if (lane < m) {
+      double zc[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++) zc[k] = k < n ? Zs[k * 33 + lane] : 0.0;
+      for (int s0 = lane; s0 < m; s0 += 4) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < 32; k++)
+          if (k < n) {
+#pragma unroll
+            for (int u = 0; u < 4; u++) acc[u] = fma(zc[k], Zs[k * 33 + min(s0 + u, 31)], acc[u]);
+          }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (s0 + u < m) {
+            const int s = s0 + u;
+            const double rr = acc[u] - (s == lane ? 1.0 : 0.0);
+            e2 += (s == lane ? 1.0 : 2.0) * rr * rr;
+          }
+      }
+    }
+    e1 = sqrt(warp_sum(e1));
+    e2 = sqrt(warp_sum(e2));
+    if (lane == 0) {
+      const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
+      const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
+      const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
+      const bool f1 = e1 > dmax * TOL, f2 = e2 > n * TOL;
+      if (err1) err1[id] = e1;
+      if (err2) err2[id] = e2;
+      if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
+      if (ref_flags) {  // the reference stores the verdict into the input copy, eigen_GPU_check.cu:76-80
+        float *ans = ref_flags + (size_t)id * nm * n * (sizeof(T) / sizeof(float));
+        ans[0] = (float)(f1 ? e1 / dmax : 0.0);
+        ans[1] = (float)(f2 ? e2 : 0.0);
+        ans[2] = (float)TOL;
+        ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
+      }
+    }
+  }
+}
+
+// k_check8, with TILE x TILE output tiles (TILE = 32, 64 or 128; n > 64 uses 128):
 // a 16 x 16 thread grid, an R x R FP64 register tile per thread (R =
 // TILE/16; rows and columns 16 apart), 16-deep panels of A (or of Z for
 // Z^T Z) and of Z staged in shared memory by cp.async, two buffers, so

@@ -2144,8 +2144,11 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
     k_check_cta<T><<<(unsigned)L, 256, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
     return cudaGetLastError();
   }
-  const long blocks = std::min<long>((L + 3) / 4, 65535);
-  k_check<T><<<(unsigned)blocks, 128, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+  const long blocks = std::min<long>((L + CKW_WARPS - 1) / CKW_WARPS, 65535);
+  cudaError_t e = set_smem(k_check_w<T, false>, check_w_smem());
+  if (e != cudaSuccess) return e;
+  k_check_w<T, false><<<(unsigned)blocks, 32 * CKW_WARPS, check_w_smem(), stream>>>(L, nm, n, m, a0, w, z, err1, err2,
+                                                                                    flags, ref_flags);
   return cudaGetLastError();
 }
 
@@ -2166,8 +2169,11 @@ cudaError_t check_packed_run(long L, int n, const T *ap, const T *w, const T *z,
   } else if (n > 32) {
     k_check_cta<T, true><<<(unsigned)L, 256, 0, stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
   } else {
-    const long blocks = std::min<long>((L + 3) / 4, 65535);
-    k_check<T, true><<<(unsigned)blocks, 128, 0, stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+    const long blocks = std::min<long>((L + CKW_WARPS - 1) / CKW_WARPS, 65535);
+    cudaError_t e = set_smem(k_check_w<T, true>, check_w_smem());
+    if (e != cudaSuccess) return e;
+    k_check_w<T, true><<<(unsigned)blocks, 32 * CKW_WARPS, check_w_smem(), stream>>>(L, ldz, n, n, ap, w, z, err1,
+                                                                                     err2, flags, nullptr);
   }
   return cudaGetLastError();
 }
