@@ -147,44 +147,90 @@ __device__ __forceinline__ double blk_max(double v, double *red)
   return s;
 }
 
-// Cyclic Jacobi on the k x k symmetric matrix M (row-major in M[p*33 + q])
-// by one warp; V (same layout) receives the eigenvectors (columns), M's
-// diagonal the eigenvalues.  At most 30 sweeps.
-__device__ void warp_jacobi(double *M, double *V, const int k)
+// Jacobi on the k x k symmetric matrix M (row-major in M[p*33 + q], k <=
+// 32) by one warp, in the round-robin parallel ordering: each round turns
+// k/2 disjoint pairs at once, lanes < k/2 forming one rotation each, and
+// the warp applies them to M from both sides in one pass over the 2 x 2
+// blocks of the pairs (rows, then columns, each entry read and written
+// once) and to V's columns.  A pair whose off-diagonal entry is at rounding
+// level (|m_pq| <= 1.1e-16 (|m_pp| + |m_qq|) / 2) is left alone; a sweep
+// without a rotation ends it, at most 30 sweeps.  V (same layout)
+// receives the eigenvectors (columns), M's diagonal the eigenvalues.  PQ
+// (32 ints) and CS (32 doubles) hold the round's pairs and rotations.
+__device__ void warp_jacobi(double *M, double *V, const int k, int *PQ, double *CS)
 {
   const int l = threadIdx.x & 31;
   for (int q = 0; q < k; q++)
     if (l < k) V[l * 33 + q] = (l == q) ? 1.0 : 0.0;
+  const int np = (k + 1) & ~1, m = np - 1, half = np / 2;
   __syncwarp();
   for (int sweep = 0; sweep < 30; sweep++) {
     int rotated = 0;
-    for (int p = 0; p < k - 1; p++) {
-      for (int q = p + 1; q < k; q++) {
-        const double app = M[p * 33 + p], aqq = M[q * 33 + q], apq = M[p * 33 + q];
-        if (!(fabs(apq) > 1.1e-16 * 0.5 * (fabs(app) + fabs(aqq)))) continue;
-        rotated = 1;
-        const double th = (aqq - app) / (2.0 * apq);
-        double t = (fabs(th) > 1e150) ? 0.5 / th : copysign(1.0, th) / (fabs(th) + sqrt(fma(th, th, 1.0)));
-        const double c = 1.0 / sqrt(fma(t, t, 1.0)), s = t * c;
-        __syncwarp();
-        if (l < k) {  // columns p, q of M and V
-          const double mp = M[l * 33 + p], mq = M[l * 33 + q];
-          M[l * 33 + p] = c * mp - s * mq;
-          M[l * 33 + q] = s * mp + c * mq;
-          const double vp = V[l * 33 + p], vq = V[l * 33 + q];
-          V[l * 33 + p] = c * vp - s * vq;
-          V[l * 33 + q] = s * vp + c * vq;
+    for (int r = 0; r < m; r++) {
+      int rot = 0;
+      if (l < half) {
+        int p = l == 0 ? r : (r + l) % m, q = l == 0 ? m : (r - l + m) % m;
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
         }
-        __syncwarp();
-        if (l < k) {  // rows p, q of M
-          const double mp = M[p * 33 + l], mq = M[q * 33 + l];
-          M[p * 33 + l] = c * mp - s * mq;
-          M[q * 33 + l] = s * mp + c * mq;
+        double c = 1.0, sn = 0.0;
+        if (q < k) {
+          const double app = M[p * 33 + p], aqq = M[q * 33 + q], apq = M[p * 33 + q];
+          if (fabs(apq) > 1.1e-16 * 0.5 * (fabs(app) + fabs(aqq))) {
+            rot = 1;
+            const double th = (aqq - app) / (2.0 * apq);
+            const double t = (fabs(th) > 1e150) ? 0.5 / th : copysign(1.0, th) / (fabs(th) + sqrt(fma(th, th, 1.0)));
+            c = 1.0 / sqrt(fma(t, t, 1.0));
+            sn = t * c;
+          }
         }
-        __syncwarp();
-        if (l == 0) M[p * 33 + q] = M[q * 33 + p] = 0.0;
-        __syncwarp();
+        PQ[2 * l] = p;
+        PQ[2 * l + 1] = q;
+        CS[2 * l] = c;
+        CS[2 * l + 1] = sn;
       }
+      rotated |= __any_sync(0xffffffffu, rot);
+      __syncwarp();
+      for (int idx = l; idx < half * half; idx += 32) {
+        const int ka = idx / half, kb = idx % half;
+        const int p = PQ[2 * ka], q = PQ[2 * ka + 1], p2 = PQ[2 * kb], q2 = PQ[2 * kb + 1];
+        const double ca = CS[2 * ka], sa = CS[2 * ka + 1], cb = CS[2 * kb], sb = CS[2 * kb + 1];
+        if (q < k && q2 < k) {
+          const double b00 = M[p * 33 + p2], b01 = M[p * 33 + q2], b10 = M[q * 33 + p2], b11 = M[q * 33 + q2];
+          const double r00 = ca * b00 - sa * b10, r10 = sa * b00 + ca * b10;  // rows p, q
+          const double r01 = ca * b01 - sa * b11, r11 = sa * b01 + ca * b11;
+          M[p * 33 + p2] = cb * r00 - sb * r01;  // columns p2, q2
+          M[p * 33 + q2] = sb * r00 + cb * r01;
+          M[q * 33 + p2] = cb * r10 - sb * r11;
+          M[q * 33 + q2] = sb * r10 + cb * r11;
+        } else if (q2 < k) {  // pair ka is the dummy of odd k: only the columns turn
+          const double b0 = M[p * 33 + p2], b1 = M[p * 33 + q2];
+          M[p * 33 + p2] = cb * b0 - sb * b1;
+          M[p * 33 + q2] = sb * b0 + cb * b1;
+        } else if (q < k) {  // pair kb is the dummy: only the rows turn
+          const double b0 = M[p * 33 + p2], b1 = M[q * 33 + p2];
+          M[p * 33 + p2] = ca * b0 - sa * b1;
+          M[q * 33 + p2] = sa * b0 + ca * b1;
+        }
+      }
+      for (int idx = l; idx < k * half; idx += 32) {  // columns of V
+        const int row = idx / half, kb = idx % half;
+        const int p2 = PQ[2 * kb], q2 = PQ[2 * kb + 1];
+        if (q2 < k) {
+          const double cb = CS[2 * kb], sb = CS[2 * kb + 1];
+          const double v0 = V[row * 33 + p2], v1 = V[row * 33 + q2];
+          V[row * 33 + p2] = cb * v0 - sb * v1;
+          V[row * 33 + q2] = sb * v0 + cb * v1;
+        }
+      }
+      __syncwarp();
+      if (rot) {  // the pair's off-diagonal entries, annihilated up to rounding, set exactly
+        const int p = PQ[2 * l], q = PQ[2 * l + 1];
+        M[p * 33 + q] = M[q * 33 + p] = 0.0;
+      }
+      __syncwarp();
     }
     if (!rotated) break;
   }
@@ -194,7 +240,7 @@ __device__ void warp_jacobi(double *M, double *V, const int k)
 constexpr int REF_JW = 2;  // warps that run the cluster Jacobi (their scratch bounds the CTAs per SM)
 __host__ __device__ inline size_t ref_update_smem(int n)
 {
-  return sizeof(double) * ((size_t)n + REF_JW * 2 * 32 * 33) + sizeof(int) * 4 * (size_t)n + 64;
+  return sizeof(double) * ((size_t)n + REF_JW * (2 * 32 * 33 + 64)) + sizeof(int) * 4 * (size_t)n + 64;
 }
 
 __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
@@ -207,8 +253,8 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
   }
   const int n = p.n;
   double *lam = reinterpret_cast<double *>(ru_smem);
-  double *jw = lam + n;  // REF_JW warps x (M, V) of 32 x 33
-  int *ord = reinterpret_cast<int *>(jw + REF_JW * 2 * 32 * 33);
+  double *jw = lam + n;  // REF_JW warps x (M, V of 32 x 33, CS of 32, PQ of 32 ints)
+  int *ord = reinterpret_cast<int *>(jw + REF_JW * (2 * 32 * 33 + 64));
   int *cid = ord + n;
   int *csz = cid + n;
   int *cst = csz + n;  // sorted start positions of the clusters of 2 .. REF_CL_MAX
@@ -301,7 +347,8 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
   // cluster Rayleigh-Ritz: one warp per cluster of 2 .. REF_CL_MAX, the
   // first REF_JW warps
   const int warp = tid >> 5, l = tid & 31;
-  double *M = jw + (warp % REF_JW) * 2 * 32 * 33, *V = M + 32 * 33;
+  double *M = jw + (warp % REF_JW) * (2 * 32 * 33 + 64), *V = M + 32 * 33, *CS = V + 32 * 33;
+  int *PQ = reinterpret_cast<int *>(CS + 32);
   for (int c = warp; warp < REF_JW && c < ncl; c += REF_JW) {
     const int k0 = cst[c], sz = csz[k0];
     for (int q = 0; q < sz; q++) {
@@ -313,7 +360,7 @@ __global__ void __launch_bounds__(256) k_oa_update(const RefP p)
       }
     }
     __syncwarp();
-    warp_jacobi(M, V, sz);
+    warp_jacobi(M, V, sz, PQ, CS);
     if (l == 0) {
       // ascending eigenvalues within the cluster: column q of W is the
       // eigenvector of the q-th smallest; it replaces member ord[k0 + q]
