@@ -211,6 +211,22 @@ __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__
   __syncthreads();
   // Jacobi sweeps, round-robin ordering over np = n rounded up to even
   const int np = (n + 1) & ~1, m = np - 1, half = np / 2;
+  // this thread's 2 x 2 blocks of B (pairs ka, kb) and entries of V (pair,
+  // row), the same in every round: index arithmetic out of the loop
+  constexpr int LW_BPT = (LW_NMAX / 2) * (LW_NMAX / 2) / 256, LW_VPT = (LW_NMAX / 2) * LW_NMAX / 256;
+  int bka[LW_BPT], bkb[LW_BPT], vk[LW_VPT], vl[LW_VPT];
+#pragma unroll
+  for (int j = 0; j < LW_BPT; j++) {
+    const int idx = tid + 256 * j;
+    bka[j] = idx < half * half ? idx / half : -1;
+    bkb[j] = idx < half * half ? idx % half : 0;
+  }
+#pragma unroll
+  for (int j = 0; j < LW_VPT; j++) {
+    const int idx = tid + 256 * j;
+    vk[j] = idx < half * n ? idx / n : -1;
+    vl[j] = idx < half * n ? idx % n : 0;
+  }
   int sw = 0;
   for (; sw < max_sweeps; sw++) {
     double off = 0.0, dg = 0.0;
@@ -251,8 +267,10 @@ __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__
       // depends only on the 2 x 2 block of the pairs of i and of j; the
       // rows are rotated first, then the columns, as two separate passes
       // over B would (same operations, same order)
-      for (int idx = tid; idx < half * half; idx += 256) {
-        const int ka = idx / half, kb = idx % half;
+#pragma unroll
+      for (int jb = 0; jb < LW_BPT; jb++) {
+        const int ka = bka[jb], kb = bkb[jb];
+        if (ka < 0) continue;
         const int p = pq[2 * ka], q = pq[2 * ka + 1], p2 = pq[2 * kb], q2 = pq[2 * kb + 1];
         if (q < n && q2 < n) {
           const double ca = cs[2 * ka], sa = cs[2 * ka + 1], cb = cs[2 * kb], sb = cs[2 * kb + 1];
@@ -277,8 +295,10 @@ __global__ void __launch_bounds__(256) k_lw_polish(const int n, const double *__
         }
       }
       // columns p, q of V
-      for (int idx = tid; idx < half * n; idx += 256) {
-        const int k = idx / n, l = idx % n;
+#pragma unroll
+      for (int jv = 0; jv < LW_VPT; jv++) {
+        const int k = vk[jv], l = vl[jv];
+        if (k < 0) continue;
         const int p = pq[2 * k], q = pq[2 * k + 1];
         if (q < n) {
           const double c = cs[2 * k], s = cs[2 * k + 1];
