@@ -33,6 +33,11 @@ namespace {
 
 constexpr int kMaxDev = 64;
 constexpr size_t kWsBudget = (size_t)8 << 30;  // workspace target per call
+// the refined solve's target: its workspace holds six FP64 n x n matrices
+// and the slices per matrix (about 5.5 MB at n = 256), and each chunk pays
+// its FP32 solve's QL latency again (C4, 2048 matrices of n = 256: 119 ms
+// in two chunks of 8 GB, 106 ms in one)
+constexpr size_t kRefBudget = (size_t)16 << 30;
 constexpr long kMinChunk = 512;
 
 struct DevProps {
@@ -1291,8 +1296,8 @@ inline cudaError_t ref_plan(long L, int nm, int n, const DevProps &dp, const Ref
   for (;;) {
     cb = ref_chunk_layout(Lc, nm, n, dp, ly);
     if (cb == 0) return cudaErrorInvalidValue;
-    if (ro.chunk > 0 || cb <= kWsBudget || Lc <= 64) break;
-    Lc = std::max<long>(64, (long)((double)Lc * (double)kWsBudget / (double)cb * 0.98));
+    if (ro.chunk > 0 || cb <= kRefBudget || Lc <= 64) break;
+    Lc = std::max<long>(64, (long)((double)Lc * (double)kRefBudget / (double)cb * 0.98));
     const long nch = (L + Lc - 1) / Lc;  // equal chunks
     Lc = (L + nch - 1) / nch;
   }

@@ -209,7 +209,7 @@ typedef struct eigen_GPU_refine_opts {
   double tol;   /* convergence threshold on n max|E_ij|^2; <= 0: 1e-14 */
   int fallback; /* 1: unconverged matrices are solved by the plain FP64 path (the
                    default when opts == NULL); 0: they are left unsolved, info -1 */
-  int chunk;    /* matrices per internal chunk; <= 0: automatic (about 8 GiB) */
+  int chunk;    /* matrices per internal chunk; <= 0: automatic (about 16 GiB) */
 } eigen_GPU_refine_opts;
 cudaError_t eigen_GPU_batch_refine_BufferSize_DP(const int L, const int nm, const int n,
                                                 const eigen_GPU_refine_opts *opts, size_t *lwork);
