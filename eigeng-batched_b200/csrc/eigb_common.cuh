@@ -236,6 +236,13 @@ struct CtaTeam {
     x = warp_sum(x);
     if ((rank & 31) == 0) buf[rank >> 5] = x;
   }
+  // within one warp: the sum of post() in every lane, lane src's x, a warp barrier
+  template <class T> __device__ __forceinline__ T wsum(T x) const { return warp_sum(x); }
+  template <class T> __device__ __forceinline__ T shfl(T x, const int src) const
+  {
+    return __shfl_sync(0xffffffffu, x, src);
+  }
+  __device__ __forceinline__ void sync_warp() const { __syncwarp(); }
   template <class T> __device__ __forceinline__ T total(const T *buf, int, const int w0, const int nw) const
   {
     T s = T(0);

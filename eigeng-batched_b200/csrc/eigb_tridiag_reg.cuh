@@ -186,7 +186,8 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   // its column block substitute it in registers.
   T *sg = red, *al = red + 32;  // posted partial sums: u.u and u.(A u)
   T ur = T(0), w2r = T(0);  // step i+1's u_r and w2_r (its pivot and beta are in gram, beta_s)
-  for (int i = n - 1;; --i) {
+  T pr = T(0);              // step i+1's p_r
+  for (int i = n - 1; i >= 32; --i) {
     const int cbi = i >> 5;
     if (cb == cbi) {
       T pi = T(0), ulp = T(0);  // p_i and the pivot of step i+1
@@ -207,7 +208,6 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
         tm.post(u0 * u0, sg, 0);
       }
     }
-    if (i == 0) break;
     tm.sync();
     T *Vi = V + (size_t)i * NR;
     const bool act = (c0 < i) && (32 * rb < i);
@@ -235,7 +235,7 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
     tm.post(x, al, 1);
     tm.sync();
     const int nact = (i + 31) >> 5;
-    T pr = T(0);
+    pr = T(0);
     if (r < i) {
 #pragma unroll
       for (int q = 0; q < NB; q++)
@@ -245,6 +245,48 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
     if (cb == 0) pv[r] = pr;  // 0 for r >= i
     const T alpha = tm.total(al, 1, 0, NB * NB) * (beta * beta * T(0.5));
     w2r = fma(alpha + alpha, ur, pr);
+  }
+  // ---- steps 31 .. 0 in warp 0 ----
+  // From step 31 on only the leading 32 x 32 block changes, and warp 0
+  // holds all of it: the remaining steps run there with warp shuffles and
+  // warp barriers, the other warps wait at the next CTA barrier.  Every
+  // operation is the CTA schedule's for these steps: the partial sums of the
+  // other warps are zeros (their rows and columns are past the active part),
+  // so a total over them is 0 + this warp's sum, and p_i (the top's sum of
+  // the posted products times beta_{i+1}) is the previous step's p_r of
+  // lane i.
+  if (w == 0) {
+    T ulp = gram[32];  // step i+1's pivot
+    T *pvb = pv;
+    for (int i = 31;; --i) {
+      const T pi = tm.shfl(pr, i);
+      const T col = get32(S, i) + fma(ulp, w2r, pi * ur);
+      if (r == i) d_out[i] = col;
+      if (i == 0) break;
+      const T u0 = (r < i) ? col : T(0);
+      V[(size_t)i * NR + r] = u0;
+      const T ulast = tm.shfl(u0, i - 1);
+      const T sig = T(0) + tm.wsum(u0 * u0);
+      tm.sync_warp();  // u_i stored
+      reg_rank2<T>(S, V + (size_t)(i + 1) * NR, pvb, ur, w2r);  // step i+1's update
+      const T anorm = -copysign_t(sqr_t(sig), ulast);
+      const T ul = ulast - anorm;
+      const T beta = T(1) / flip0to1(ul * anorm);
+      if (r == i - 1) gram[i] = ul;
+      if (r == 0) {
+        e_out[i - 1] = anorm;
+        beta_s[i] = beta;
+      }
+      ur = (r == i - 1) ? ul : u0;
+      T a = reg_symv<T, true>(S, V + (size_t)i * NR, i - 1, ul);
+      a = (r < i) ? a : T(0);
+      const T alpha = (T(0) + tm.wsum(ur * a)) * (beta * beta * T(0.5));
+      pr = (r < i) ? (T(0) + a) * beta : T(0);
+      tm.sync_warp();  // every lane's reads of p_{i+1} done
+      pvb[r] = pr;
+      w2r = fma(alpha + alpha, ur, pr);
+      ulp = ul;
+    }
   }
   tm.sync();
   for (int k = 1 + t; k < n; k += tm.size()) V[(size_t)k * NR + k - 1] = gram[k];

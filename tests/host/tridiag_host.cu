@@ -12,9 +12,14 @@
 
 template <class T> struct HostShared {
   std::barrier<> bar;
+  std::barrier<> wbar;   // the barrier of warp 0 alone
   std::vector<T> slots;  // 2 x nthr, alternating halves
   std::vector<T> posted; // 2 x nthr: the buffers of post()/total()
-  explicit HostShared(int nthr) : bar(nthr), slots(2 * (size_t)nthr), posted(2 * (size_t)nthr) {}
+  std::vector<T> wsl;    // 32: the exchanges of warp 0
+  explicit HostShared(int nthr)
+      : bar(nthr), wbar(32), slots(2 * (size_t)nthr), posted(2 * (size_t)nthr), wsl(32)
+  {
+  }
 };
 
 template <class T> struct HostTeam {
@@ -34,6 +39,25 @@ template <class T> struct HostTeam {
   }
   // one slot per thread; total() adds the threads of warps w0 .. w0+nw-1
   void post(T x, T *, int id) { sh->posted[(size_t)id * nthr + rank] = x; }
+  // warp 0's own operations (only its 32 threads call them)
+  void sync_warp() const { sh->wbar.arrive_and_wait(); }
+  T shfl(T x, int src) const
+  {
+    sh->wsl[rank & 31] = x;
+    sh->wbar.arrive_and_wait();
+    const T v = sh->wsl[src];
+    sh->wbar.arrive_and_wait();
+    return v;
+  }
+  T wsum(T x) const
+  {
+    sh->wsl[rank & 31] = x;
+    sh->wbar.arrive_and_wait();
+    T s = T(0);
+    for (int k = 0; k < 32; k++) s += sh->wsl[k];
+    sh->wbar.arrive_and_wait();
+    return s;
+  }
   T total(const T *, int id, int w0, int nw) const
   {
     const T *buf = sh->posted.data() + (size_t)id * nthr;
