@@ -569,33 +569,39 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
     dt = a_host.dtype
     if w_host is None:
         w_host = torch.empty((L, n), dtype=dt, pin_memory=True)
-    # chunk boundaries: equal chunks of `chunk` matrices when given; else
-    # 1/16, 3/16, 1/4, 1/4, 3/16, 1/16 of the batch -- small first and last
-    # chunks shorten the copies that nothing overlaps at either end, while
-    # few chunks keep the per-chunk latency of the QL phase (about 2 ms at
-    # n = 128 whatever the chunk size) from adding up.  Measured on B200 at
-    # n=128 FP64, L=4096: 21.1 ms against 22.5 ms for 1/8, 3/8, 3/8, 1/8 and
-    # 23.0 ms for eight equal chunks.
+    # chunk boundaries: equal chunks of `chunk` matrices when given; else,
+    # from L = 2048 on, chunks of L/16 with half-size first and last chunks
+    # (17 in all) solved up to eight at a time on their own streams: the QL
+    # phase of a chunk has a latency of about 2 ms at n = 128 whatever its
+    # size and occupies few SMs, so the phases of the other chunks in flight
+    # fill the GPU meanwhile, and the small end chunks shorten the copies
+    # that nothing overlaps.  Host to host on B200, ms per batch, against
+    # six chunks (1/16, 3/16, 1/4, 1/4, 3/16, 1/16) on two streams: FP64
+    # n=128 L=4096 19.45 -> 16.26, n=32 L=16384 3.93 -> 3.89, n=64 L=20000
+    # 18.73 -> 15.66, n=200 L=2048 61.1 -> 50.5, n=256 L=2048 104.7 -> 91.6;
+    # FP32 n=128 L=4096 12.44 -> 10.43.  Four streams instead of eight lose
+    # most of it (n=128 FP64 18.98 ms).
     if chunk > 0:
         bounds = list(range(0, L, chunk)) + [L]
     elif L >= 2048:
-        bounds = [0, L // 16, L // 4, L // 2, L - L // 4, L - L // 16, L]
+        bounds = [0] + [(L * (2 * k - 1) + 16) // 32 for k in range(1, 17)] + [L]
     else:
         bounds = [0, L]
     nch = len(bounds) - 1
     C = max(bounds[i + 1] - bounds[i] for i in range(nch))
-    nbuf = min(4, nch)
+    # concurrent chunks, each with its own stream and workspace, and two
+    # device buffers more than that, so that a chunk's copy in proceeds while
+    # the chunks before it solve and copy out
+    nrun = min(8, nch)
+    nbuf = min(nrun + 2, nch)
     da = [torch.empty((C, n, nm), dtype=dt, device=dev) for _ in range(nbuf)]
     dw = [torch.empty((C, n), dtype=dt, device=dev) for _ in range(nbuf)]
-    # two compute streams with their own workspace: consecutive chunks solve
-    # concurrently, so one chunk's latency-bound QL phase (which occupies
-    # few SMs) overlaps the other chunk's reduction or apply phase
-    nrun = min(2, nch)
     # QL phase with eight matrices per warp when chunks solve concurrently:
-    # its lanes' chains then occupy fewer warps beside the other chunk's
-    # kernels (measured on B200 at n=128 FP64, L=4096, interleaved: 19.8 ms
-    # against 20.8 with four, 21.1 with two, 21.3 automatic; one chunk
-    # alone keeps the automatic choice)
+    # its lanes' chains then occupy fewer warps beside the other chunks'
+    # kernels (measured on B200 at n=128 FP64, L=4096, two chunks in flight:
+    # 19.8 ms against 20.8 with four, 21.1 with two, 21.3 automatic; with
+    # eight in flight 16.26 ms against 16.15 with sixteen, which is slower
+    # in FP32); one chunk alone keeps the automatic choice
     ql_mpw = 8 if nrun > 1 else 0
     if info_host is not None and (info_host.is_cuda or info_host.numel() != L or info_host.dtype != torch.int32):
         raise EigenGError("info_host must be a host int32 tensor of L entries")

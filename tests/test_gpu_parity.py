@@ -379,8 +379,9 @@ def test_chunked_batch_and_determinism(oracle_mod):
 
 
 def test_solve_host_matches_device_solve(oracle_mod):
-    """solve_host (host buffers, chunks on three streams) gives exactly the
-    device solve's results, with a ragged last chunk and padding rows."""
+    """solve_host (host buffers, chunks solved concurrently on their own
+    streams) gives exactly the device solve's results, with a ragged last
+    chunk and padding rows."""
     O = oracle_mod
     n, nm, L = 48, 50, 37
     a0 = np.zeros((L, n, nm))
@@ -398,13 +399,14 @@ def test_solve_host_matches_device_solve(oracle_mod):
     assert np.array_equal(wf.numpy(), w2)
 
 
-@pytest.mark.parametrize("n,L,chunk", [(48, 37, 5), (16, 4096, 0)])
+@pytest.mark.parametrize("n,L,chunk", [(48, 37, 2), (16, 4096, 0)])
 def test_solve_host_buffer_reuse_and_status(oracle_mod, n, L, chunk):
-    """More chunks than the four device buffers (each buffer, and its
-    status buffer, reused after its copy-out), and the default six-chunk
-    schedule of a batch of 2048 or more with the QL phase at eight matrices
-    per warp: bit for bit the device solve, status copied back per matrix.
-    One matrix carries a NaN, which QL reports in its status."""
+    """More chunks than the ten device buffers (each buffer, and its status
+    buffer, reused after its copy-out; each of the eight streams' workspace
+    reused by the stream's next chunk), and the default 17-chunk schedule of
+    a batch of 2048 or more with the QL phase at eight matrices per warp:
+    bit for bit the device solve, status copied back per matrix.  One matrix
+    carries a NaN, which QL reports in its status."""
     O = oracle_mod
     a0 = O.sym_uniform(L, n, seed=23)
     bad = L // 3
