@@ -21,7 +21,8 @@
 //   k_jacobi_warp  cyclic Jacobi for n <= 32 (jac_tiled.hpp:3-152)
 //   k_check_w      FP64 residual / orthogonality gate (eigen_GPU_check.cu),
 //                  one warp per matrix for n <= 32; k_check_cta (n <= 64)
-//                  and k_check8 (above) the tiled forms
+//                  and k_check_tc (above, on the FP64 tensor cores) the
+//                  tiled forms
 #pragma once
 #include <stdio.h>
 
@@ -1223,7 +1224,7 @@ __global__ void __launch_bounds__(256) k_transpose(const long rows, const long c
 // reference's flags (eigen_GPU_check.cu:34-74): bit 0 when the residual
 // exceeds max(|w_1|, |w_n|) TOL, bit 1 when the orthogonality exceeds
 // n TOL.  Three forms by size: k_check_w (n <= 32), k_check_cta (n <= 64),
-// k_check8 (above).
+// k_check_tc (above).
 //
 // k_check_cta, for 32 < n <= 64, one CTA of 256 threads per matrix: the
 // products A Z (n x m) and Z^T Z (upper triangle, m x m) are formed tile by
@@ -1473,20 +1474,32 @@ __global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const 
   }
 }
 
-// k_check8, with TILE x TILE output tiles (TILE = 32, 64 or 128; n > 64 uses 128):
-// a 16 x 16 thread grid, an R x R FP64 register tile per thread (R =
-// TILE/16; rows and columns 16 apart), 16-deep panels of A (or of Z for
-// Z^T Z) and of Z staged in shared memory by cp.async, two buffers, so
-// that the next panels load while the current ones are multiplied; R^2
-// FMAs per 2R shared-memory loads (64 per 16 at TILE = 128).  The panels
-// keep the input type (FP32 inputs widen at use).  PACKED reads A from the
-// packed upper triangle (ap + id n(n+1)/2, element (r, c), r <= c, at
-// r + c(c+1)/2) instead of the full layout; Z has leading dimension ldz.
-// Dynamic shared memory: check8_smem<T, TILE>().
-constexpr int CK8_KC = 16;
-template <class T, int TILE> __host__ __device__ constexpr size_t check8_smem()
+// The gate for n > 64 on the FP64 tensor cores (mma.sync m8n8k4, FP64
+// operands and accumulators): one CTA of 16 warps (four per scheduler, to
+// hide the latencies of the fragment loads and of the products) per matrix
+// walks the 128 x 128 output tiles of A Z (all) and of Z^T Z (those on and
+// above the diagonal), with 16-deep panels of A (or of Z for Z^T Z) and of
+// Z staged in shared memory by cp.async, two buffers, so that the next
+// panels load while the current ones are multiplied.  On an A Z tile or an
+// off-diagonal Z^T Z tile warp w owns the 64 x 16 block at rows 64 (w & 1),
+// columns 16 (w >> 1): 8 x 2 mma tiles, 10 fragment loads per 16 products.
+// On a diagonal Z^T Z tile only the 136 mma tiles on and above the
+// diagonal are needed: warps 2p and 2p + 1 share mma rows p and 15 - p (17
+// tiles from the diagonal rightwards), warp 2p + h taking the columns of
+// parity h, 8 or 9 tiles per warp.  The panels keep the input type (FP32
+// inputs widen at use).  PACKED reads A from the packed upper triangle
+// (ap + id n(n+1)/2, element (r, c), r <= c, at r + c(c+1)/2) instead of
+// the full layout; Z has leading dimension ldz.  Dynamic shared memory:
+// checkm_smem<T>().
+constexpr int CKM_KC = 16;   // panel depth
+// panel pitch, 8 mod 16 doubles: a fragment load (rows g = 0..7 at k = q =
+// 0..3) and a cp.async store (rows r..r+7 at k = kq = 0..3, 4 k of a row per
+// 32-byte sector of the source) both hit every bank pair twice, the least
+// that 32 lanes of 8 bytes can
+constexpr int CKM_LDP = 136;
+template <class T> __host__ __device__ constexpr size_t checkm_smem()
 {
-  return sizeof(T) * 2 * 2 * CK8_KC * (size_t)(TILE + 1);
+  return sizeof(T) * 2 * 2 * CKM_KC * (size_t)CKM_LDP;
 }
 
 template <int BYTES> __device__ __forceinline__ void ck_cp_async(void *dst, const void *src, bool valid)
@@ -1499,12 +1512,21 @@ template <int BYTES> __device__ __forceinline__ void ck_cp_async(void *dst, cons
 __device__ __forceinline__ void ck_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void ck_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <class T, bool PACKED, int TILE>
-__global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, const int ldz, const int n, const int m,
-                                                   const T *a0, const T *w, const T *z, double *err1, double *err2,
-                                                   int *flags, float *ref_flags)
+// D = A B + D for one 8 x 8 tile, k = 4: this lane's A(g, q), B(q, g) and
+// D(g, 2q), D(g, 2q + 1), g = lane / 4, q = lane % 4
+__device__ __forceinline__ void ck_dmma(double &d0, double &d1, const double a, const double b)
 {
-  constexpr int R = TILE / 16, LDP = TILE + 1, PANEL = CK8_KC * LDP;
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+template <class T, bool PACKED>
+__global__ void __launch_bounds__(512, 1) k_check_tc(const long L, const int lda, const int ldz, const int n, const int m,
+                                                     const T *a0, const T *w, const T *z, double *err1, double *err2,
+                                                     int *flags, float *ref_flags)
+{
+  constexpr int TILE = 128, LDP = CKM_LDP, PANEL = CKM_KC * LDP;
   extern __shared__ __align__(16) unsigned char ck_smem[];
   T *Pb = reinterpret_cast<T *>(ck_smem);  // [2][KC][LDP]: P(k, tile row)
   T *Qb = Pb + 2 * PANEL;                   // [2][KC][LDP]: Q(k, tile column)
@@ -1514,9 +1536,10 @@ __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, 
   const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * lda * n;
   const T *zz = z + (size_t)id * ldz * n;
   const T *d = w + (size_t)id * n;
-  const int t = threadIdx.x, tr = t % 16, tc = t / 16;
+  const int t = threadIdx.x, wp = t >> 5, lane = t & 31;
+  const int g = lane >> 2, q = lane & 3;
   const int ntn = (n + TILE - 1) / TILE, ntm = (m + TILE - 1) / TILE;
-  const int nchunks = (n + CK8_KC - 1) / CK8_KC;
+  const int nchunks = (n + CKM_KC - 1) / CKM_KC;
   double s1 = 0.0, s2 = 0.0;
   const int nres = ntn * ntm, nort = ntm * (ntm + 1) / 2;
   for (int tile = 0; tile < nres + nort; tile++) {
@@ -1530,15 +1553,17 @@ __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, 
     }
     const int i0 = ti * TILE, j0 = tj * TILE;
     const int ilim = res ? n : m;
+    const bool diag = !res && ti == tj;
     // the panels of chunk c into buffer c & 1; out-of-range entries are
     // zero-filled (a source of 0 bytes)
     auto load = [&](int c) {
       T *P = Pb + (c & 1) * PANEL, *Q = Qb + (c & 1) * PANEL;
-      const int kc = c * CK8_KC;
+      const int kc = c * CKM_KC;
 #pragma unroll
-      for (int q = 0; q < (CK8_KC * TILE) / 256; q++) {
-        const int e = t + 256 * q;
-        const int cc = e % CK8_KC, rr = e / CK8_KC;  // 16 consecutive k of one row / column
+      for (int u = 0; u < (CKM_KC * TILE) / 512; u++) {
+        const int e = t + 512 * u;
+        // 4 consecutive k of one row / column per 4 lanes, 8 rows per warp
+        const int cc = 4 * (e / (4 * TILE)) + (e & 3), rr = (e >> 2) % TILE;
         const int kk = kc + cc;
         const int i = i0 + rr, j = j0 + rr;
         const bool pin = kk < n && i < ilim, qin = kk < n && j < m;
@@ -1557,11 +1582,14 @@ __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, 
       }
       ck_commit();
     };
-    double acc[R][R];
+    // block form: acc[2 mi + ni] for mma tile (mi, ni) of the warp's 64 x 16
+    // block; diagonal form: acc[x] and acc[8 + x] for mma tiles (R0, h + 2x)
+    // and (R1, h + 2x) of the tile
+    double acc[16][2];
 #pragma unroll
-    for (int x = 0; x < R; x++)
-#pragma unroll
-      for (int y = 0; y < R; y++) acc[x][y] = 0.0;
+    for (int x = 0; x < 16; x++) acc[x][0] = acc[x][1] = 0.0;
+    const int r0 = 64 * (wp & 1), c0 = 16 * (wp >> 1);
+    const int h = wp & 1, R0 = wp >> 1, R1 = 15 - (wp >> 1);
     __syncthreads();  // the previous tile's last panels are consumed
     load(0);
     for (int c = 0; c < nchunks; c++) {
@@ -1572,37 +1600,72 @@ __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, 
         ck_wait<0>();
       }
       __syncthreads();  // ... and every thread's
-      const T *P = Pb + (c & 1) * PANEL, *Q = Qb + (c & 1) * PANEL;
+      const T *P = Pb + (c & 1) * PANEL + q * LDP + g, *Q = Qb + (c & 1) * PANEL + q * LDP + g;
+      if (!diag) {
 #pragma unroll
-      for (int cc = 0; cc < CK8_KC; cc++) {
-        double pa[R], qb[R];
+        for (int ks = 0; ks < CKM_KC; ks += 4) {
+          double af[8], bf[2];
 #pragma unroll
-        for (int u = 0; u < R; u++) {
-          pa[u] = (double)P[cc * LDP + tr + 16 * u];
-          qb[u] = (double)Q[cc * LDP + tc + 16 * u];
+          for (int mi = 0; mi < 8; mi++) af[mi] = (double)P[ks * LDP + r0 + 8 * mi];
+#pragma unroll
+          for (int ni = 0; ni < 2; ni++) bf[ni] = (double)Q[ks * LDP + c0 + 8 * ni];
+#pragma unroll
+          for (int mi = 0; mi < 8; mi++)
+#pragma unroll
+            for (int ni = 0; ni < 2; ni++) ck_dmma(acc[2 * mi + ni][0], acc[2 * mi + ni][1], af[mi], bf[ni]);
         }
+      } else {
 #pragma unroll
-        for (int x = 0; x < R; x++)
+        for (int ks = 0; ks < CKM_KC; ks += 4) {
+          const double a0f = (double)P[ks * LDP + 8 * R0], a1f = (double)P[ks * LDP + 8 * R1];
+          double bf[8];
 #pragma unroll
-          for (int y = 0; y < R; y++) acc[x][y] = fma(pa[x], qb[y], acc[x][y]);
+          for (int x = 0; x < 8; x++) bf[x] = h + 2 * x >= R0 ? (double)Q[ks * LDP + 8 * (h + 2 * x)] : 0.0;
+#pragma unroll
+          for (int x = 0; x < 8; x++)
+            if (h + 2 * x >= R0) ck_dmma(acc[x][0], acc[x][1], a0f, bf[x]);
+#pragma unroll
+          for (int x = 4; x < 8; x++)
+            if (h + 2 * x >= R1) ck_dmma(acc[8 + x][0], acc[8 + x][1], a1f, bf[x]);
+        }
       }
       __syncthreads();  // buffer c & 1 is free for chunk c + 2
     }
+    // this lane's outputs: rows i, columns j and j + 1 of each mma tile
+    auto take = [&](const int i, const int j, const double v) {
+      if (res) {
+        if (i < n && j < m) {
+          const double rr = v - (double)d[j] * (double)zz[i + (size_t)j * ldz];
+          s1 = fma(rr, rr, s1);
+        }
+      } else if (i < m && j < m && i <= j) {
+        const double rr = v - (i == j ? 1.0 : 0.0);
+        s2 += (i == j ? 1.0 : 2.0) * rr * rr;
+      }
+    };
+    if (!diag) {
 #pragma unroll
-    for (int x = 0; x < R; x++)
+      for (int mi = 0; mi < 8; mi++)
 #pragma unroll
-      for (int y = 0; y < R; y++) {
-        const int i = i0 + tr + 16 * x, j = j0 + tc + 16 * y;
-        if (res) {
-          if (i < n && j < m) {
-            const double rr = acc[x][y] - (double)d[j] * (double)zz[i + (size_t)j * ldz];
-            s1 = fma(rr, rr, s1);
-          }
-        } else if (i < m && j < m && i <= j) {
-          const double rr = acc[x][y] - (i == j ? 1.0 : 0.0);
-          s2 += (i == j ? 1.0 : 2.0) * rr * rr;
+        for (int ni = 0; ni < 2; ni++) {
+          const int i = i0 + r0 + 8 * mi + g, j = j0 + c0 + 8 * ni + 2 * q;
+          take(i, j, acc[2 * mi + ni][0]);
+          take(i, j + 1, acc[2 * mi + ni][1]);
+        }
+    } else {
+#pragma unroll
+      for (int x = 0; x < 8; x++) {
+        const int C = h + 2 * x, j = j0 + 8 * C + 2 * q;
+        if (C >= R0) {
+          take(i0 + 8 * R0 + g, j, acc[x][0]);
+          take(i0 + 8 * R0 + g, j + 1, acc[x][1]);
+        }
+        if (C >= R1) {
+          take(i0 + 8 * R1 + g, j, acc[8 + x][0]);
+          take(i0 + 8 * R1 + g, j + 1, acc[8 + x][1]);
         }
       }
+    }
   }
   s1 = warp_sum(s1);
   s2 = warp_sum(s2);
@@ -1613,9 +1676,9 @@ __global__ void __launch_bounds__(256, 1) k_check8(const long L, const int lda, 
   __syncthreads();
   if (t == 0) {
     double e1 = 0.0, e2 = 0.0;
-    for (int q = 0; q < 8; q++) {
-      e1 += red[q];
-      e2 += red[32 + q];
+    for (int k = 0; k < 16; k++) {
+      e1 += red[k];
+      e2 += red[32 + k];
     }
     e1 = sqrt(e1);
     e2 = sqrt(e2);

@@ -2136,12 +2136,12 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
                       int *flags, float *ref_flags, cudaStream_t stream)
 {
   if (bad_args(L, nm, n, m) || !a0 || !w || !z) return cudaErrorInvalidValue;
-  if (n > 64) {  // 128 x 128 tiles, 8 x 8 per thread
+  if (n > 64) {  // 128 x 128 tiles on the FP64 tensor cores
     if (L > 0x7fffffffL) return cudaErrorInvalidValue;
-    const size_t sm8 = check8_smem<T, 128>();
-    cudaError_t e = set_smem(k_check8<T, false, 128>, sm8);
+    const size_t smb = checkm_smem<T>();
+    cudaError_t e = set_smem(k_check_tc<T, false>, smb);
     if (e != cudaSuccess) return e;
-    k_check8<T, false, 128><<<(unsigned)L, 256, sm8, stream>>>(L, nm, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+    k_check_tc<T, false><<<(unsigned)L, 512, smb, stream>>>(L, nm, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
     return cudaGetLastError();
   }
   if (n > 32) {
@@ -2167,10 +2167,10 @@ cudaError_t check_packed_run(long L, int n, const T *ap, const T *w, const T *z,
 {
   if (L < 1 || L > 0x7fffffffL || n < 1 || n > 1024 || ldz < n || !ap || !w || !z) return cudaErrorInvalidValue;
   if (n > 64) {
-    const size_t sm8 = check8_smem<T, 128>();
-    cudaError_t e = set_smem(k_check8<T, true, 128>, sm8);
+    const size_t smb = checkm_smem<T>();
+    cudaError_t e = set_smem(k_check_tc<T, true>, smb);
     if (e != cudaSuccess) return e;
-    k_check8<T, true, 128><<<(unsigned)L, 256, sm8, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+    k_check_tc<T, true><<<(unsigned)L, 512, smb, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
   } else if (n > 32) {
     k_check_cta<T, true><<<(unsigned)L, 256, 0, stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
   } else {
