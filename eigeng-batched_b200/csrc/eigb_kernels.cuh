@@ -1486,20 +1486,21 @@ __global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const 
 // On a diagonal Z^T Z tile only the 136 mma tiles on and above the
 // diagonal are needed: warps 2p and 2p + 1 share mma rows p and 15 - p (17
 // tiles from the diagonal rightwards), warp 2p + h taking the columns of
-// parity h, 8 or 9 tiles per warp.  The panels keep the input type (FP32
-// inputs widen at use).  PACKED reads A from the packed upper triangle
+// parity h, 8 or 9 tiles per warp.  KC (16 or 32) is the panel depth.
+// The grid is persistent (one CTA per SM, each taking every gridDim.x-th
+// matrix) so that the panel pipeline runs on across tiles and matrices.  The panels keep
+// the input type (FP32 inputs widen at use).  PACKED reads A from the packed upper triangle
 // (ap + id n(n+1)/2, element (r, c), r <= c, at r + c(c+1)/2) instead of
 // the full layout; Z has leading dimension ldz.  Dynamic shared memory:
-// checkm_smem<T>().
-constexpr int CKM_KC = 16;   // panel depth
+// checkm_smem<T, KC>().
 // panel pitch, 8 mod 16 doubles: a fragment load (rows g = 0..7 at k = q =
 // 0..3) and a cp.async store (rows r..r+7 at k = kq = 0..3, 4 k of a row per
 // 32-byte sector of the source) both hit every bank pair twice, the least
 // that 32 lanes of 8 bytes can
 constexpr int CKM_LDP = 136;
-template <class T> __host__ __device__ constexpr size_t checkm_smem()
+template <class T, int KC> __host__ __device__ constexpr size_t checkm_smem()
 {
-  return sizeof(T) * 2 * 2 * CKM_KC * (size_t)CKM_LDP;
+  return sizeof(T) * 2 * 2 * KC * (size_t)CKM_LDP;
 }
 
 template <int BYTES> __device__ __forceinline__ void ck_cp_async(void *dst, const void *src, bool valid)
@@ -1521,180 +1522,195 @@ __device__ __forceinline__ void ck_dmma(double &d0, double &d1, const double a, 
       : "d"(a), "d"(b));
 }
 
-template <class T, bool PACKED>
+template <class T, bool PACKED, int KC>
 __global__ void __launch_bounds__(512, 1) k_check_tc(const long L, const int lda, const int ldz, const int n, const int m,
                                                      const T *a0, const T *w, const T *z, double *err1, double *err2,
                                                      int *flags, float *ref_flags)
 {
-  constexpr int TILE = 128, LDP = CKM_LDP, PANEL = CKM_KC * LDP;
+  constexpr int TILE = 128, LDP = CKM_LDP, PANEL = KC * LDP;
   extern __shared__ __align__(16) unsigned char ck_smem[];
   T *Pb = reinterpret_cast<T *>(ck_smem);  // [2][KC][LDP]: P(k, tile row)
   T *Qb = Pb + 2 * PANEL;                   // [2][KC][LDP]: Q(k, tile column)
   __shared__ double red[64];
-  const long id = blockIdx.x;
-  if (id >= L) return;
-  const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * lda * n;
-  const T *zz = z + (size_t)id * ldz * n;
-  const T *d = w + (size_t)id * n;
   const int t = threadIdx.x, wp = t >> 5, lane = t & 31;
   const int g = lane >> 2, q = lane & 3;
   const int ntn = (n + TILE - 1) / TILE, ntm = (m + TILE - 1) / TILE;
-  const int nchunks = (n + CKM_KC - 1) / CKM_KC;
-  double s1 = 0.0, s2 = 0.0;
-  const int nres = ntn * ntm, nort = ntm * (ntm + 1) / 2;
-  for (int tile = 0; tile < nres + nort; tile++) {
-    const bool res = tile < nres;
-    int ti, tj;
-    if (res) {
+  const int nchunks = (n + KC - 1) / KC;
+  const int nres = ntn * ntm, nort = ntm * (ntm + 1) / 2, ntiles = nres + nort;
+  auto tile_of = [&](const int tile, int &ti, int &tj) {
+    if (tile < nres) {
       ti = tile % ntn;
       tj = tile / ntn;
     } else {
       symf_tile(tile - nres, ntm, ti, tj);
     }
-    const int i0 = ti * TILE, j0 = tj * TILE;
-    const int ilim = res ? n : m;
-    const bool diag = !res && ti == tj;
-    // the panels of chunk c into buffer c & 1; out-of-range entries are
-    // zero-filled (a source of 0 bytes)
-    auto load = [&](int c) {
-      T *P = Pb + (c & 1) * PANEL, *Q = Qb + (c & 1) * PANEL;
-      const int kc = c * CKM_KC;
+  };
+  // the panels of chunk c of tile `tile` of matrix `id` into buffer b;
+  // out-of-range entries are zero-filled (a source of 0 bytes)
+  auto load = [&](const long id, const int tile, const int c, const int b) {
+    const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * lda * n;
+    const T *zz = z + (size_t)id * ldz * n;
+    const bool res = tile < nres;
+    int ti, tj;
+    tile_of(tile, ti, tj);
+    const int i0 = ti * TILE, j0 = tj * TILE, ilim = res ? n : m;
+    T *P = Pb + b * PANEL, *Q = Qb + b * PANEL;
+    const int kc = c * KC;
 #pragma unroll
-      for (int u = 0; u < (CKM_KC * TILE) / 512; u++) {
-        const int e = t + 512 * u;
-        // 4 consecutive k of one row / column per 4 lanes, 8 rows per warp
-        const int cc = 4 * (e / (4 * TILE)) + (e & 3), rr = (e >> 2) % TILE;
-        const int kk = kc + cc;
-        const int i = i0 + rr, j = j0 + rr;
-        const bool pin = kk < n && i < ilim, qin = kk < n && j < m;
-        const T *ps = zz, *qs = zz;
-        if (pin) {
-          if (!res) {
-            ps = zz + kk + (size_t)i * ldz;  // Z(k, i)
-          } else {
-            const int lo = i < kk ? i : kk, hi = i < kk ? kk : i;  // A(i, k) from the upper triangle
-            ps = PACKED ? a + lo + (size_t)hi * (hi + 1) / 2 : a + lo + (size_t)hi * lda;
+    for (int u = 0; u < (KC * TILE) / 512; u++) {
+      const int e = t + 512 * u;
+      // 4 consecutive k of one row / column per 4 lanes, 8 rows per warp
+      const int cc = 4 * (e / (4 * TILE)) + (e & 3), rr = (e >> 2) % TILE;
+      const int kk = kc + cc;
+      const int i = i0 + rr, j = j0 + rr;
+      const bool pin = kk < n && i < ilim, qin = kk < n && j < m;
+      const T *ps = zz, *qs = zz;
+      if (pin) {
+        if (!res) {
+          ps = zz + kk + (size_t)i * ldz;  // Z(k, i)
+        } else {
+          const int lo = i < kk ? i : kk, hi = i < kk ? kk : i;  // A(i, k) from the upper triangle
+          ps = PACKED ? a + lo + (size_t)hi * (hi + 1) / 2 : a + lo + (size_t)hi * lda;
+        }
+      }
+      if (qin) qs = zz + kk + (size_t)j * ldz;  // Z(k, j)
+      ck_cp_async<sizeof(T)>(&P[cc * LDP + rr], ps, pin);
+      ck_cp_async<sizeof(T)>(&Q[cc * LDP + rr], qs, qin);
+    }
+    ck_commit();
+  };
+  const int r0 = 64 * (wp & 1), c0 = 16 * (wp >> 1);
+  const int h = wp & 1, R0 = wp >> 1, R1 = 15 - (wp >> 1);
+  // The CTA takes matrices blockIdx.x, + gridDim.x, ...; the chunks of all
+  // its tiles form one pipeline, so the first panels of the next tile (or
+  // of the next matrix) are in flight while a tile ends and its norms are
+  // taken.
+  int b = 0;
+  if ((long)blockIdx.x < L) load(blockIdx.x, 0, 0, 0);
+  for (long id = blockIdx.x; id < L; id += gridDim.x) {
+    const T *zz = z + (size_t)id * ldz * n;
+    const T *d = w + (size_t)id * n;
+    double s1 = 0.0, s2 = 0.0;
+    for (int tile = 0; tile < ntiles; tile++) {
+      const bool res = tile < nres;
+      int ti, tj;
+      tile_of(tile, ti, tj);
+      const int i0 = ti * TILE, j0 = tj * TILE;
+      const bool diag = !res && ti == tj;
+      // block form: acc[2 mi + ni] for mma tile (mi, ni) of the warp's 64 x 16
+      // block; diagonal form: acc[x] and acc[8 + x] for mma tiles (R0, h + 2x)
+      // and (R1, h + 2x) of the tile
+      double acc[16][2];
+#pragma unroll
+      for (int x = 0; x < 16; x++) acc[x][0] = acc[x][1] = 0.0;
+      for (int c = 0; c < nchunks; c++) {
+        // the next chunk of the pipeline: of this tile, of the next tile, or
+        // the first of the CTA's next matrix
+        bool more = true;
+        if (c + 1 < nchunks) load(id, tile, c + 1, b ^ 1);
+        else if (tile + 1 < ntiles) load(id, tile + 1, 0, b ^ 1);
+        else if (id + gridDim.x < L) load(id + gridDim.x, 0, 0, b ^ 1);
+        else more = false;
+        if (more) ck_wait<1>();  // this chunk has landed (this thread's copies)
+        else ck_wait<0>();
+        __syncthreads();  // ... and every thread's
+        const T *P = Pb + b * PANEL + q * LDP + g, *Q = Qb + b * PANEL + q * LDP + g;
+        if (!diag) {
+#pragma unroll
+          for (int ks = 0; ks < KC; ks += 4) {
+            double af[8], bf[2];
+#pragma unroll
+            for (int mi = 0; mi < 8; mi++) af[mi] = (double)P[ks * LDP + r0 + 8 * mi];
+#pragma unroll
+            for (int ni = 0; ni < 2; ni++) bf[ni] = (double)Q[ks * LDP + c0 + 8 * ni];
+#pragma unroll
+            for (int mi = 0; mi < 8; mi++)
+#pragma unroll
+              for (int ni = 0; ni < 2; ni++) ck_dmma(acc[2 * mi + ni][0], acc[2 * mi + ni][1], af[mi], bf[ni]);
+          }
+        } else {
+#pragma unroll
+          for (int ks = 0; ks < KC; ks += 4) {
+            const double a0f = (double)P[ks * LDP + 8 * R0], a1f = (double)P[ks * LDP + 8 * R1];
+            double bf[8];
+#pragma unroll
+            for (int x = 0; x < 8; x++) bf[x] = h + 2 * x >= R0 ? (double)Q[ks * LDP + 8 * (h + 2 * x)] : 0.0;
+#pragma unroll
+            for (int x = 0; x < 8; x++)
+              if (h + 2 * x >= R0) ck_dmma(acc[x][0], acc[x][1], a0f, bf[x]);
+#pragma unroll
+            for (int x = 4; x < 8; x++)
+              if (h + 2 * x >= R1) ck_dmma(acc[8 + x][0], acc[8 + x][1], a1f, bf[x]);
           }
         }
-        if (qin) qs = zz + kk + (size_t)j * ldz;  // Z(k, j)
-        ck_cp_async<sizeof(T)>(&P[cc * LDP + rr], ps, pin);
-        ck_cp_async<sizeof(T)>(&Q[cc * LDP + rr], qs, qin);
+        __syncthreads();  // buffer b is free for the chunk after next
+        b ^= 1;
       }
-      ck_commit();
-    };
-    // block form: acc[2 mi + ni] for mma tile (mi, ni) of the warp's 64 x 16
-    // block; diagonal form: acc[x] and acc[8 + x] for mma tiles (R0, h + 2x)
-    // and (R1, h + 2x) of the tile
-    double acc[16][2];
-#pragma unroll
-    for (int x = 0; x < 16; x++) acc[x][0] = acc[x][1] = 0.0;
-    const int r0 = 64 * (wp & 1), c0 = 16 * (wp >> 1);
-    const int h = wp & 1, R0 = wp >> 1, R1 = 15 - (wp >> 1);
-    __syncthreads();  // the previous tile's last panels are consumed
-    load(0);
-    for (int c = 0; c < nchunks; c++) {
-      if (c + 1 < nchunks) {
-        load(c + 1);
-        ck_wait<1>();  // chunk c has landed (this thread's copies)
-      } else {
-        ck_wait<0>();
-      }
-      __syncthreads();  // ... and every thread's
-      const T *P = Pb + (c & 1) * PANEL + q * LDP + g, *Q = Qb + (c & 1) * PANEL + q * LDP + g;
+      // this lane's outputs: rows i, columns j and j + 1 of each mma tile
+      auto take = [&](const int i, const int j, const double v) {
+        if (res) {
+          if (i < n && j < m) {
+            const double rr = v - (double)d[j] * (double)zz[i + (size_t)j * ldz];
+            s1 = fma(rr, rr, s1);
+          }
+        } else if (i < m && j < m && i <= j) {
+          const double rr = v - (i == j ? 1.0 : 0.0);
+          s2 += (i == j ? 1.0 : 2.0) * rr * rr;
+        }
+      };
       if (!diag) {
 #pragma unroll
-        for (int ks = 0; ks < CKM_KC; ks += 4) {
-          double af[8], bf[2];
+        for (int mi = 0; mi < 8; mi++)
 #pragma unroll
-          for (int mi = 0; mi < 8; mi++) af[mi] = (double)P[ks * LDP + r0 + 8 * mi];
-#pragma unroll
-          for (int ni = 0; ni < 2; ni++) bf[ni] = (double)Q[ks * LDP + c0 + 8 * ni];
-#pragma unroll
-          for (int mi = 0; mi < 8; mi++)
-#pragma unroll
-            for (int ni = 0; ni < 2; ni++) ck_dmma(acc[2 * mi + ni][0], acc[2 * mi + ni][1], af[mi], bf[ni]);
-        }
+          for (int ni = 0; ni < 2; ni++) {
+            const int i = i0 + r0 + 8 * mi + g, j = j0 + c0 + 8 * ni + 2 * q;
+            take(i, j, acc[2 * mi + ni][0]);
+            take(i, j + 1, acc[2 * mi + ni][1]);
+          }
       } else {
 #pragma unroll
-        for (int ks = 0; ks < CKM_KC; ks += 4) {
-          const double a0f = (double)P[ks * LDP + 8 * R0], a1f = (double)P[ks * LDP + 8 * R1];
-          double bf[8];
-#pragma unroll
-          for (int x = 0; x < 8; x++) bf[x] = h + 2 * x >= R0 ? (double)Q[ks * LDP + 8 * (h + 2 * x)] : 0.0;
-#pragma unroll
-          for (int x = 0; x < 8; x++)
-            if (h + 2 * x >= R0) ck_dmma(acc[x][0], acc[x][1], a0f, bf[x]);
-#pragma unroll
-          for (int x = 4; x < 8; x++)
-            if (h + 2 * x >= R1) ck_dmma(acc[8 + x][0], acc[8 + x][1], a1f, bf[x]);
-        }
-      }
-      __syncthreads();  // buffer c & 1 is free for chunk c + 2
-    }
-    // this lane's outputs: rows i, columns j and j + 1 of each mma tile
-    auto take = [&](const int i, const int j, const double v) {
-      if (res) {
-        if (i < n && j < m) {
-          const double rr = v - (double)d[j] * (double)zz[i + (size_t)j * ldz];
-          s1 = fma(rr, rr, s1);
-        }
-      } else if (i < m && j < m && i <= j) {
-        const double rr = v - (i == j ? 1.0 : 0.0);
-        s2 += (i == j ? 1.0 : 2.0) * rr * rr;
-      }
-    };
-    if (!diag) {
-#pragma unroll
-      for (int mi = 0; mi < 8; mi++)
-#pragma unroll
-        for (int ni = 0; ni < 2; ni++) {
-          const int i = i0 + r0 + 8 * mi + g, j = j0 + c0 + 8 * ni + 2 * q;
-          take(i, j, acc[2 * mi + ni][0]);
-          take(i, j + 1, acc[2 * mi + ni][1]);
-        }
-    } else {
-#pragma unroll
-      for (int x = 0; x < 8; x++) {
-        const int C = h + 2 * x, j = j0 + 8 * C + 2 * q;
-        if (C >= R0) {
-          take(i0 + 8 * R0 + g, j, acc[x][0]);
-          take(i0 + 8 * R0 + g, j + 1, acc[x][1]);
-        }
-        if (C >= R1) {
-          take(i0 + 8 * R1 + g, j, acc[8 + x][0]);
-          take(i0 + 8 * R1 + g, j + 1, acc[8 + x][1]);
+        for (int x = 0; x < 8; x++) {
+          const int C = h + 2 * x, j = j0 + 8 * C + 2 * q;
+          if (C >= R0) {
+            take(i0 + 8 * R0 + g, j, acc[x][0]);
+            take(i0 + 8 * R0 + g, j + 1, acc[x][1]);
+          }
+          if (C >= R1) {
+            take(i0 + 8 * R1 + g, j, acc[8 + x][0]);
+            take(i0 + 8 * R1 + g, j + 1, acc[8 + x][1]);
+          }
         }
       }
     }
-  }
-  s1 = warp_sum(s1);
-  s2 = warp_sum(s2);
-  if ((t & 31) == 0) {
-    red[t >> 5] = s1;
-    red[32 + (t >> 5)] = s2;
-  }
-  __syncthreads();
-  if (t == 0) {
-    double e1 = 0.0, e2 = 0.0;
-    for (int k = 0; k < 16; k++) {
-      e1 += red[k];
-      e2 += red[32 + k];
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    if ((t & 31) == 0) {
+      red[t >> 5] = s1;
+      red[32 + (t >> 5)] = s2;
     }
-    e1 = sqrt(e1);
-    e2 = sqrt(e2);
-    const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
-    const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
-    const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
-    const bool f1 = e1 > dmax * TOL, f2 = e2 > n * TOL;
-    if (err1) err1[id] = e1;
-    if (err2) err2[id] = e2;
-    if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
-    if (ref_flags) {
-      float *ans = ref_flags + (size_t)id * lda * n * (sizeof(T) / sizeof(float));
-      ans[0] = (float)(f1 ? e1 / dmax : 0.0);
-      ans[1] = (float)(f2 ? e2 : 0.0);
-      ans[2] = (float)TOL;
-      ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
+    __syncthreads();
+    if (t == 0) {
+      double e1 = 0.0, e2 = 0.0;
+      for (int k = 0; k < 16; k++) {
+        e1 += red[k];
+        e2 += red[32 + k];
+      }
+      e1 = sqrt(e1);
+      e2 = sqrt(e2);
+      const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
+      const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
+      const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
+      const bool f1 = e1 > dmax * TOL, f2 = e2 > n * TOL;
+      if (err1) err1[id] = e1;
+      if (err2) err2[id] = e2;
+      if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
+      if (ref_flags) {
+        float *ans = ref_flags + (size_t)id * lda * n * (sizeof(T) / sizeof(float));
+        ans[0] = (float)(f1 ? e1 / dmax : 0.0);
+        ans[1] = (float)(f2 ? e2 : 0.0);
+        ans[2] = (float)TOL;
+        ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
+      }
     }
   }
 }

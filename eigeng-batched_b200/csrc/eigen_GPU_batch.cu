@@ -2131,6 +2131,29 @@ cudaError_t symfunc_run(long L, int nm, int n, const T *v, const T *w, T *z, int
   return cudaGetLastError();
 }
 
+// the tensor-core gate, 32-deep panels from n = 128 on (16 below, where a
+// 32-deep panel would be mostly padding); one persistent CTA per SM
+template <class T, bool PACKED>
+cudaError_t launch_check_tc(long L, int lda, int ldz, int n, int m, const T *a, const T *w, const T *z, double *err1,
+                            double *err2, int *flags, float *ref_flags, cudaStream_t stream)
+{
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = (unsigned)std::min<long>(L, std::max(sms, 1));
+  if (n >= 128) {
+    const size_t smb = checkm_smem<T, 32>();
+    if ((e = set_smem(k_check_tc<T, PACKED, 32>, smb)) != cudaSuccess) return e;
+    k_check_tc<T, PACKED, 32><<<grid, 512, smb, stream>>>(L, lda, ldz, n, m, a, w, z, err1, err2, flags, ref_flags);
+  } else {
+    const size_t smb = checkm_smem<T, 16>();
+    if ((e = set_smem(k_check_tc<T, PACKED, 16>, smb)) != cudaSuccess) return e;
+    k_check_tc<T, PACKED, 16><<<grid, 512, smb, stream>>>(L, lda, ldz, n, m, a, w, z, err1, err2, flags, ref_flags);
+  }
+  return cudaGetLastError();
+}
+
 template <class T>
 cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, const T *z, double *err1, double *err2,
                       int *flags, float *ref_flags, cudaStream_t stream)
@@ -2138,11 +2161,7 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
   if (bad_args(L, nm, n, m) || !a0 || !w || !z) return cudaErrorInvalidValue;
   if (n > 64) {  // 128 x 128 tiles on the FP64 tensor cores
     if (L > 0x7fffffffL) return cudaErrorInvalidValue;
-    const size_t smb = checkm_smem<T>();
-    cudaError_t e = set_smem(k_check_tc<T, false>, smb);
-    if (e != cudaSuccess) return e;
-    k_check_tc<T, false><<<(unsigned)L, 512, smb, stream>>>(L, nm, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
-    return cudaGetLastError();
+    return launch_check_tc<T, false>(L, nm, nm, n, m, a0, w, z, err1, err2, flags, ref_flags, stream);
   }
   if (n > 32) {
     if (L > 0x7fffffffL) return cudaErrorInvalidValue;
@@ -2167,10 +2186,8 @@ cudaError_t check_packed_run(long L, int n, const T *ap, const T *w, const T *z,
 {
   if (L < 1 || L > 0x7fffffffL || n < 1 || n > 1024 || ldz < n || !ap || !w || !z) return cudaErrorInvalidValue;
   if (n > 64) {
-    const size_t smb = checkm_smem<T>();
-    cudaError_t e = set_smem(k_check_tc<T, true>, smb);
+    cudaError_t e = launch_check_tc<T, true>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr, stream);
     if (e != cudaSuccess) return e;
-    k_check_tc<T, true><<<(unsigned)L, 512, smb, stream>>>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
   } else if (n > 32) {
     k_check_cta<T, true><<<(unsigned)L, 256, 0, stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
   } else {
