@@ -706,9 +706,15 @@ def learned_block(torch, E, args, stream, L=65536):
         wv, info, sw, resid = holder["r"]
         swn = sw.cpu().numpy()
         ok = swn >= 0
+        rn = resid.cpu().numpy()
+        # the residual gate's largest relative residual among the matrices
+        # it passed (those it failed, set to infinity there, went to the
+        # plain solve and are counted in "fallback")
         out[name] = {"matrices_per_s": L / ms * 1e3, "ms": ms, "gate_pass": float(ok.mean()),
+                     "fallback": int((~ok).sum()),
                      "mean_sweeps": float(swn[ok].mean()) if ok.any() else None,
-                     "max_gate_residual": float(resid.max()), "info_nonzero": int((info != 0).sum())}
+                     "max_gate_residual": float(rn[ok].max()) if ok.any() else None,
+                     "info_nonzero": int((info != 0).sum())}
     return out
 
 
