@@ -1356,12 +1356,25 @@ __global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, c
 
 // k_check_w, for n <= 32, one warp per matrix (4 per CTA): A (full
 // symmetric, from the upper triangle or the packed one) and Z staged in
-// shared memory as FP64 (per warp 2 x 32 x 33); lane r forms row r of A Z
-// with its row of A in registers (the columns of Z broadcast) and row r of
-// the upper triangle of Z^T Z with its column of Z in registers.  Dynamic
-// shared memory: check_w_smem().
+// shared memory as FP64 (per warp 2 x 32 x 36, zero padded to 32 x 32), then
+// A Z (4 x 4 mma tiles) and the upper triangle of Z^T Z (10 mma tiles) on
+// the FP64 tensor cores (mma.sync m8n8k4), 8 fragment loads per 26 products
+// per k-step of 4: the fragments of Z serve as the B operand of A Z and as
+// the A operand of Z^T Z.  The pitch of 36 doubles (4 mod 16) keeps the
+// fragment loads free of bank conflicts.  Dynamic shared memory:
+// check_w_smem().
 constexpr int CKW_WARPS = 4;
-__host__ __device__ constexpr size_t check_w_smem() { return sizeof(double) * 2 * 32 * 33 * CKW_WARPS; }
+constexpr int CKW_LD = 36;
+__host__ __device__ constexpr size_t check_w_smem() { return sizeof(double) * 2 * 32 * CKW_LD * CKW_WARPS; }
+
+// D = A B + D for one 8 x 8 tile, k = 4: this lane's A(g, q), B(q, g) and
+// D(g, 2q), D(g, 2q + 1), g = lane / 4, q = lane % 4
+__device__ __forceinline__ void ck_dmma(double &d0, double &d1, const double a, const double b)
+{
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
 
 template <class T, bool PACKED>
 __global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const int nm, const int n, const int m,
@@ -1369,15 +1382,25 @@ __global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const 
                                                             double *err2, int *flags, float *ref_flags)
 {
   extern __shared__ __align__(16) unsigned char ckw_smem[];
+  constexpr int LD = CKW_LD;
   const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double *As = reinterpret_cast<double *>(ckw_smem) + (size_t)wid * 2 * 32 * 33;  // As[r * 33 + c]
-  double *Zs = As + 32 * 33;                                                        // Zs[r * 33 + i] = Z(r, i)
+  const int g = lane >> 2, q = lane & 3;
+  double *As = reinterpret_cast<double *>(ckw_smem) + (size_t)wid * 2 * 32 * LD;  // As[i * LD + k] = A(i, k)
+  double *Zs = As + 32 * LD;                                                       // Zs[j * LD + k] = Z(k, j)
   const long nw = (long)gridDim.x * CKW_WARPS;
   for (long id = (long)blockIdx.x * CKW_WARPS + wid; id < L; id += nw) {
     const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * nm * n;
     const T *zz = z + (size_t)id * nm * n;
     const T *d = w + (size_t)id * n;
     __syncwarp();  // the previous matrix's reads are done
+    // zero padding past n (A) and past n, m (Z)
+    if (n < 32 || m < 32) {
+      for (int idx = lane; idx < 32 * 32; idx += 32) {
+        const int r = idx & 31, c = idx >> 5;
+        if (r >= n || c >= n) As[c * LD + r] = 0.0;
+        if (r >= n || c >= m) Zs[c * LD + r] = 0.0;
+      }
+    }
     // eight loads in flight per lane before their stores (a store to shared
     // memory would otherwise wait for each load in turn)
     for (int i0 = 0; i0 < n * n; i0 += 8 * 32) {
@@ -1392,8 +1415,8 @@ __global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const 
       for (int u = 0; u < 8; u++) {
         const int idx = i0 + u * 32 + lane, r = idx % n, c = idx / n;
         if (idx < n * n && r <= c) {
-          As[r * 33 + c] = v[u];
-          As[c * 33 + r] = v[u];
+          As[c * LD + r] = v[u];
+          As[r * LD + c] = v[u];
         }
       }
     }
@@ -1407,51 +1430,62 @@ __global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const 
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         const int idx = i0 + u * 32 + lane;
-        if (idx < n * m) Zs[(idx % n) * 33 + idx / n] = v[u];
+        if (idx < n * m) Zs[(idx / n) * LD + idx % n] = v[u];
       }
     }
     __syncwarp();
+    // acc[4 R + C]: A Z mma tile (R, C); acz[x]: Z^T Z mma tile x of the
+    // upper triangle, (R, C) = (0,0) (0,1) (0,2) (0,3) (1,1) (1,2) (1,3)
+    // (2,2) (2,3) (3,3)
+    double acc[16][2], acz[10][2];
+#pragma unroll
+    for (int x = 0; x < 16; x++) acc[x][0] = acc[x][1] = 0.0;
+#pragma unroll
+    for (int x = 0; x < 10; x++) acz[x][0] = acz[x][1] = 0.0;
+#pragma unroll
+    for (int k0 = 0; k0 < 32; k0 += 4) {
+      double af[4], zf[4];
+#pragma unroll
+      for (int R = 0; R < 4; R++) af[R] = As[(8 * R + g) * LD + k0 + q];  // A(8R + g, k0 + q)
+#pragma unroll
+      for (int C = 0; C < 4; C++) zf[C] = Zs[(8 * C + g) * LD + k0 + q];  // Z(k0 + q, 8C + g)
+#pragma unroll
+      for (int R = 0; R < 4; R++)
+#pragma unroll
+        for (int C = 0; C < 4; C++) ck_dmma(acc[4 * R + C][0], acc[4 * R + C][1], af[R], zf[C]);
+      int x = 0;
+#pragma unroll
+      for (int R = 0; R < 4; R++)
+#pragma unroll
+        for (int C = R; C < 4; C++, x++) ck_dmma(acz[x][0], acz[x][1], zf[R], zf[C]);
+    }
     double e1 = 0.0, e2 = 0.0;
-    if (lane < n) {
-      double ar[32];
 #pragma unroll
-      for (int j = 0; j < 32; j++) ar[j] = j < n ? As[lane * 33 + j] : 0.0;
-      for (int i0 = 0; i0 < m; i0 += 4) {  // four columns, four independent chains
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int R = 0; R < 4; R++)
 #pragma unroll
-        for (int j = 0; j < 32; j++)
-          if (j < n) {
+      for (int C = 0; C < 4; C++)
 #pragma unroll
-            for (int u = 0; u < 4; u++) acc[u] = fma(ar[j], Zs[j * 33 + min(i0 + u, 31)], acc[u]);
-          }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (i0 + u < m) {
-            const double rr = acc[u] - (double)d[i0 + u] * Zs[lane * 33 + i0 + u];
+        for (int h = 0; h < 2; h++) {
+          const int i = 8 * R + g, j = 8 * C + 2 * q + h;
+          if (i < n && j < m) {
+            const double rr = acc[4 * R + C][h] - (double)d[j] * Zs[j * LD + i];
             e1 = fma(rr, rr, e1);
           }
-      }
-    }
-    if (lane < m) {
-      double zc[32];
+        }
+    {
+      int x = 0;
 #pragma unroll
-      for (int k = 0; k < 32; k++) zc[k] = k < n ? Zs[k * 33 + lane] : 0.0;
-      for (int s0 = lane; s0 < m; s0 += 4) {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int R = 0; R < 4; R++)
 #pragma unroll
-        for (int k = 0; k < 32; k++)
-          if (k < n) {
+        for (int C = R; C < 4; C++, x++)
 #pragma unroll
-            for (int u = 0; u < 4; u++) acc[u] = fma(zc[k], Zs[k * 33 + min(s0 + u, 31)], acc[u]);
+          for (int h = 0; h < 2; h++) {
+            const int i = 8 * R + g, j = 8 * C + 2 * q + h;
+            if (i < m && j < m && i <= j) {
+              const double rr = acz[x][h] - (i == j ? 1.0 : 0.0);
+              e2 += (i == j ? 1.0 : 2.0) * rr * rr;
+            }
           }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (s0 + u < m) {
-            const int s = s0 + u;
-            const double rr = acc[u] - (s == lane ? 1.0 : 0.0);
-            e2 += (s == lane ? 1.0 : 2.0) * rr * rr;
-          }
-      }
     }
     e1 = sqrt(warp_sum(e1));
     e2 = sqrt(warp_sum(e2));
@@ -1513,14 +1547,6 @@ template <int BYTES> __device__ __forceinline__ void ck_cp_async(void *dst, cons
 __device__ __forceinline__ void ck_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void ck_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// D = A B + D for one 8 x 8 tile, k = 4: this lane's A(g, q), B(q, g) and
-// D(g, 2q), D(g, 2q + 1), g = lane / 4, q = lane % 4
-__device__ __forceinline__ void ck_dmma(double &d0, double &d1, const double a, const double b)
-{
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-      : "+d"(d0), "+d"(d1)
-      : "d"(a), "d"(b));
-}
 
 template <class T, bool PACKED, int KC>
 __global__ void __launch_bounds__(512, 1) k_check_tc(const long L, const int lda, const int ldz, const int n, const int m,
