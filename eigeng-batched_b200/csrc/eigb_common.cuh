@@ -236,6 +236,11 @@ struct CtaTeam {
     x = warp_sum(x);
     if ((rank & 31) == 0) buf[rank >> 5] = x;
   }
+  // post(0) without the shuffles
+  template <class T> __device__ __forceinline__ void post_zero(T *buf, int) const
+  {
+    if ((rank & 31) == 0) buf[rank >> 5] = T(0);
+  }
   // within one warp: the sum of post() in every lane, lane src's x, a warp barrier
   template <class T> __device__ __forceinline__ T wsum(T x) const { return warp_sum(x); }
   template <class T> __device__ __forceinline__ T shfl(T x, const int src) const

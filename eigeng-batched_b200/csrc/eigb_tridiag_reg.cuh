@@ -189,6 +189,16 @@ __host__ __device__ void tridiag_qt_reg(Team &tm, T *A, const int nm, const int 
   T pr = T(0);              // step i+1's p_r
   for (int i = n - 1; i >= 32; --i) {
     const int cbi = i >> 5;
+    // Warps past the active part (row or column block beyond cbi) stay
+    // there: they keep the barriers and post the zeros their sums would be,
+    // without the step's arithmetic (NB = 2 has none before step 31).
+    if (NB > 2 && (rb > cbi || cb > cbi)) {
+      if (cb == cbi) tm.post_zero(sg, 0);
+      tm.sync();
+      tm.post_zero(al, 1);
+      tm.sync();
+      continue;
+    }
     if (cb == cbi) {
       T pi = T(0), ulp = T(0);  // p_i and the pivot of step i+1
       if (i < n - 1) {

@@ -39,6 +39,7 @@ template <class T> struct HostTeam {
   }
   // one slot per thread; total() adds the threads of warps w0 .. w0+nw-1
   void post(T x, T *, int id) { sh->posted[(size_t)id * nthr + rank] = x; }
+  void post_zero(T *, int id) { sh->posted[(size_t)id * nthr + rank] = T(0); }
   // warp 0's own operations (only its 32 threads call them)
   void sync_warp() const { sh->wbar.arrive_and_wait(); }
   T shfl(T x, int src) const
