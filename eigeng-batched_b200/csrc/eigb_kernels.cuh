@@ -1226,130 +1226,170 @@ __global__ void __launch_bounds__(256) k_transpose(const long rows, const long c
 // n TOL.  Three forms by size: k_check_w (n <= 32), k_check_cta (n <= 64),
 // k_check_tc (above).
 //
-// k_check_cta, for 32 < n <= 64, one CTA of 256 threads per matrix: the
-// products A Z (n x m) and Z^T Z (upper triangle, m x m) are formed tile by
-// tile (64 x 64, 16-row panels staged in shared memory, a 4 x 4 FP64
-// register tile per thread, rows and columns 16 apart) and squared into
-// per-thread sums; one CTA reduction at the end (deterministic).
-constexpr int CK_TILE = 64, CK_KC = 16, CK_LDP = CK_TILE + 2;
+// D = A B + D for one 8 x 8 tile, k = 4: this lane's A(g, q), B(q, g) and
+// D(g, 2q), D(g, 2q + 1), g = lane / 4, q = lane % 4
+__device__ __forceinline__ void ck_dmma(double &d0, double &d1, const double a, const double b)
+{
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+// k_check_cta, for 32 < n <= 64, one CTA of 4 warps per matrix: A (full
+// symmetric, from the upper triangle or the packed one) and Z staged in
+// shared memory as FP64 (64 x 68 each, zero padded to 64 x 64), then A Z
+// (8 x 8 mma tiles, warp w the mma rows 2w and 2w + 1) and the upper
+// triangle of Z^T Z (36 mma tiles, warp w the mma rows w and 7 - w from the
+// diagonal rightwards, 9 tiles) on the FP64 tensor cores (mma.sync
+// m8n8k4); the fragments of Z serve as the B operand of both products.
+// The pitch of 68 doubles (4 mod 16) keeps the fragment loads free of bank
+// conflicts.  Dynamic shared memory: check_cta_smem().
+constexpr int CKC_LD = 68;
+__host__ __device__ constexpr size_t check_cta_smem() { return sizeof(double) * 2 * 64 * CKC_LD; }
 
 template <class T, bool PACKED = false>
-__global__ void __launch_bounds__(256) k_check_cta(const long L, const int nm, const int n, const int m,
+__global__ void __launch_bounds__(128) k_check_cta(const long L, const int nm, const int n, const int m,
                                                    const T *a0, const T *w, const T *z, double *err1,
                                                    double *err2, int *flags, float *ref_flags)
 {
-  __shared__ double P[CK_KC][CK_LDP];  // P(tile row, k)
-  __shared__ double Q[CK_KC][CK_LDP];  // Q(k, tile column)
-  __shared__ double red[64];
-  const long id = blockIdx.x;
-  if (id >= L) return;
-  const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * nm * n;
-  const T *zz = z + (size_t)id * nm * n;
-  const T *d = w + (size_t)id * n;
-  const int t = threadIdx.x, tr = t % 16, tc = t / 16;
-  const int ntn = (n + CK_TILE - 1) / CK_TILE, ntm = (m + CK_TILE - 1) / CK_TILE;
-  double s1 = 0.0, s2 = 0.0;
-  // tiles: ntn x ntm of A Z, then the upper ntm x ntm of Z^T Z
-  const int nres = ntn * ntm, nort = ntm * (ntm + 1) / 2;
-  for (int tile = 0; tile < nres + nort; tile++) {
-    const bool res = tile < nres;
-    int ti, tj;
-    if (res) {
-      ti = tile % ntn;
-      tj = tile / ntn;
-    } else {
-      symf_tile(tile - nres, ntm, ti, tj);
+  extern __shared__ __align__(16) unsigned char ckc_smem[];
+  constexpr int LD = CKC_LD;
+  __shared__ double red[8];
+  const int t = threadIdx.x, wp = t >> 5, lane = t & 31;
+  const int g = lane >> 2, q = lane & 3;
+  double *As = reinterpret_cast<double *>(ckc_smem);  // As[i * LD + k] = A(i, k)
+  double *Zs = As + 64 * LD;                          // Zs[j * LD + k] = Z(k, j)
+  const int R0 = wp, R1 = 7 - wp;                     // the warp's mma rows of Z^T Z
+  for (long id = blockIdx.x; id < L; id += gridDim.x) {
+    const T *a = PACKED ? a0 + (size_t)id * ((size_t)n * (n + 1) / 2) : a0 + (size_t)id * nm * n;
+    const T *zz = z + (size_t)id * nm * n;
+    const T *d = w + (size_t)id * n;
+    __syncthreads();  // the previous matrix's reads are done
+    for (int idx = t; idx < 64 * 64; idx += 128) {  // zero padding past n (A) and past n, m (Z)
+      const int r = idx & 63, c = idx >> 6;
+      if (r >= n || c >= n) As[c * LD + r] = 0.0;
+      if (r >= n || c >= m) Zs[c * LD + r] = 0.0;
     }
-    const int i0 = ti * CK_TILE, j0 = tj * CK_TILE;
-    const int ilim = res ? n : m;
-    double acc[4][4];
+    // eight loads in flight per thread before their stores
+    for (int i0 = 0; i0 < n * n; i0 += 8 * 128) {
+      double v[8];
 #pragma unroll
-    for (int x = 0; x < 4; x++)
-#pragma unroll
-      for (int y = 0; y < 4; y++) acc[x][y] = 0.0;
-    for (int kc = 0; kc < n; kc += CK_KC) {
-      __syncthreads();  // the previous panels are consumed
-#pragma unroll
-      for (int q = 0; q < (CK_KC * CK_TILE) / 256; q++) {
-        const int e = t + 256 * q;
-        const int rr = e % CK_TILE, cc = e / CK_TILE;  // rr: tile row / column, cc: k offset
-        const int kk = kc + cc;
-        const int i = i0 + rr, j = j0 + rr;
-        double pv = 0.0, qv = 0.0;
-        if (kk < n) {
-          if (i < ilim) {
-            if (res) {  // A(i, k) from the upper triangle
-              const int lo = i <= kk ? i : kk, hi = i <= kk ? kk : i;
-              pv = (double)(PACKED ? a[lo + (size_t)hi * (hi + 1) / 2] : a[lo + (size_t)hi * nm]);
-            } else {
-              pv = (double)zz[kk + (size_t)i * nm];  // Z(k, i)
-            }
-          }
-          if (j < m) qv = (double)zz[kk + (size_t)j * nm];  // Z(k, j)
-        }
-        P[cc][rr] = pv;
-        Q[cc][rr] = qv;
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 128 + t, r = idx % n, c = idx / n;
+        v[u] = (idx < n * n && r <= c) ? (double)(PACKED ? a[r + (size_t)c * (c + 1) / 2] : a[r + (size_t)c * nm])
+                                       : 0.0;
       }
-      __syncthreads();
 #pragma unroll
-      for (int c = 0; c < CK_KC; c++) {
-        double pa[4], qb[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          pa[u] = P[c][tr + 16 * u];
-          qb[u] = Q[c][tc + 16 * u];
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 128 + t, r = idx % n, c = idx / n;
+        if (idx < n * n && r <= c) {
+          As[c * LD + r] = v[u];
+          As[r * LD + c] = v[u];
         }
-#pragma unroll
-        for (int x = 0; x < 4; x++)
-#pragma unroll
-          for (int y = 0; y < 4; y++) acc[x][y] = fma(pa[x], qb[y], acc[x][y]);
       }
     }
+    for (int i0 = 0; i0 < n * m; i0 += 8 * 128) {
+      double v[8];
 #pragma unroll
-    for (int x = 0; x < 4; x++)
-#pragma unroll
-      for (int y = 0; y < 4; y++) {
-        const int i = i0 + tr + 16 * x, j = j0 + tc + 16 * y;
-        if (res) {
-          if (i < n && j < m) {
-            const double rr = acc[x][y] - (double)d[j] * (double)zz[i + (size_t)j * nm];
-            s1 = fma(rr, rr, s1);
-          }
-        } else if (i < m && j < m && i <= j) {
-          const double rr = acc[x][y] - (i == j ? 1.0 : 0.0);
-          s2 += (i == j ? 1.0 : 2.0) * rr * rr;
-        }
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 128 + t;
+        v[u] = idx < n * m ? (double)zz[idx % n + (size_t)(idx / n) * nm] : 0.0;
       }
-  }
-  // CTA sums of s1, s2
-  s1 = warp_sum(s1);
-  s2 = warp_sum(s2);
-  if ((t & 31) == 0) {
-    red[t >> 5] = s1;
-    red[32 + (t >> 5)] = s2;
-  }
-  __syncthreads();
-  if (t == 0) {
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int idx = i0 + u * 128 + t;
+        if (idx < n * m) Zs[(idx / n) * LD + idx % n] = v[u];
+      }
+    }
+    __syncthreads();
+    // acc[8 h + C]: A Z mma tile (2 wp + h, C); acz[C]: Z^T Z mma tile
+    // (R0, C), C >= R0; acz[8 + C - 4]: (R1, C), C >= R1 (R1 >= 4)
+    double acc[16][2], acz[12][2];
+#pragma unroll
+    for (int x = 0; x < 16; x++) acc[x][0] = acc[x][1] = 0.0;
+#pragma unroll
+    for (int x = 0; x < 12; x++) acz[x][0] = acz[x][1] = 0.0;
+#pragma unroll 4
+    for (int k0 = 0; k0 < 64; k0 += 4) {
+      double af[2], zf[8];
+#pragma unroll
+      for (int h = 0; h < 2; h++) af[h] = As[(16 * wp + 8 * h + g) * LD + k0 + q];  // A(16 wp + 8h + g, k0 + q)
+#pragma unroll
+      for (int C = 0; C < 8; C++) zf[C] = Zs[(8 * C + g) * LD + k0 + q];        // Z(k0 + q, 8C + g)
+      const double z0 = Zs[(8 * R0 + g) * LD + k0 + q], z1 = Zs[(8 * R1 + g) * LD + k0 + q];
+#pragma unroll
+      for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int C = 0; C < 8; C++) ck_dmma(acc[8 * h + C][0], acc[8 * h + C][1], af[h], zf[C]);
+#pragma unroll
+      for (int C = 0; C < 8; C++)
+        if (C >= R0) ck_dmma(acz[C][0], acz[C][1], z0, zf[C]);
+#pragma unroll
+      for (int C = 4; C < 8; C++)
+        if (C >= R1) ck_dmma(acz[4 + C][0], acz[4 + C][1], z1, zf[C]);
+    }
     double e1 = 0.0, e2 = 0.0;
-    for (int q = 0; q < 8; q++) {
-      e1 += red[q];
-      e2 += red[32 + q];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int C = 0; C < 8; C++)
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int i = 16 * wp + 8 * h + g, j = 8 * C + 2 * q + u;
+          if (i < n && j < m) {
+            const double rr = acc[8 * h + C][u] - (double)d[j] * Zs[j * LD + i];
+            e1 = fma(rr, rr, e1);
+          }
+        }
+#pragma unroll
+    for (int C = 0; C < 8; C++)
+#pragma unroll
+      for (int u = 0; u < 2; u++) {
+        const int j = 8 * C + 2 * q + u;
+        if (C >= R0) {
+          const int i = 8 * R0 + g;
+          if (i < m && j < m && i <= j) {
+            const double rr = acz[C][u] - (i == j ? 1.0 : 0.0);
+            e2 += (i == j ? 1.0 : 2.0) * rr * rr;
+          }
+        }
+        if (C >= 4 && C >= R1) {
+          const int i = 8 * R1 + g;
+          if (i < m && j < m && i <= j) {
+            const double rr = acz[C >= 4 ? 4 + C : 0][u] - (i == j ? 1.0 : 0.0);
+            e2 += (i == j ? 1.0 : 2.0) * rr * rr;
+          }
+        }
+      }
+    e1 = warp_sum(e1);
+    e2 = warp_sum(e2);
+    if (lane == 0) {
+      red[wp] = e1;
+      red[4 + wp] = e2;
     }
-    e1 = sqrt(e1);
-    e2 = sqrt(e2);
-    const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
-    const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
-    const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
-    const bool f1 = e1 > dmax * TOL, f2 = e2 > n * TOL;
-    if (err1) err1[id] = e1;
-    if (err2) err2[id] = e2;
-    if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
-    if (ref_flags) {
-      float *ans = ref_flags + (size_t)id * nm * n * (sizeof(T) / sizeof(float));
-      ans[0] = (float)(f1 ? e1 / dmax : 0.0);
-      ans[1] = (float)(f2 ? e2 : 0.0);
-      ans[2] = (float)TOL;
-      ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
+    __syncthreads();
+    if (t == 0) {
+      double s1 = 0.0, s2 = 0.0;
+      for (int k = 0; k < 4; k++) {
+        s1 += red[k];
+        s2 += red[4 + k];
+      }
+      s1 = sqrt(s1);
+      s2 = sqrt(s2);
+      const double dmax = fmax(fabs((double)d[0]), fabs((double)d[n - 1]));
+      const double EPS = 2.220446049250313080847e-16, eps = 1.1920928955078125e-07;
+      const double TOL = (sizeof(T) == 8 ? EPS * (2 * 512 - 1) : eps * (2 * 16 - 1)) * sqrt((double)(n + 16));
+      const bool f1 = s1 > dmax * TOL, f2 = s2 > n * TOL;
+      if (err1) err1[id] = s1;
+      if (err2) err2[id] = s2;
+      if (flags) flags[id] = (f1 ? 1 : 0) | (f2 ? 2 : 0);
+      if (ref_flags) {  // the reference stores the verdict into the input copy, eigen_GPU_check.cu:76-80
+        float *ans = ref_flags + (size_t)id * nm * n * (sizeof(T) / sizeof(float));
+        ans[0] = (float)(f1 ? s1 / dmax : 0.0);
+        ans[1] = (float)(f2 ? s2 : 0.0);
+        ans[2] = (float)TOL;
+        ans[3] = (float)(sizeof(T) == 8 ? EPS : eps);
+      }
     }
   }
 }
@@ -1367,14 +1407,6 @@ constexpr int CKW_WARPS = 4;
 constexpr int CKW_LD = 36;
 __host__ __device__ constexpr size_t check_w_smem() { return sizeof(double) * 2 * 32 * CKW_LD * CKW_WARPS; }
 
-// D = A B + D for one 8 x 8 tile, k = 4: this lane's A(g, q), B(q, g) and
-// D(g, 2q), D(g, 2q + 1), g = lane / 4, q = lane % 4
-__device__ __forceinline__ void ck_dmma(double &d0, double &d1, const double a, const double b)
-{
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-      : "+d"(d0), "+d"(d1)
-      : "d"(a), "d"(b));
-}
 
 template <class T, bool PACKED>
 __global__ void __launch_bounds__(32 * CKW_WARPS) k_check_w(const long L, const int nm, const int n, const int m,

@@ -2165,7 +2165,10 @@ cudaError_t check_run(long L, int nm, int n, int m, const T *a0, const T *w, con
   }
   if (n > 32) {
     if (L > 0x7fffffffL) return cudaErrorInvalidValue;
-    k_check_cta<T><<<(unsigned)L, 256, 0, stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags, ref_flags);
+    cudaError_t e = set_smem(k_check_cta<T, false>, check_cta_smem());
+    if (e != cudaSuccess) return e;
+    k_check_cta<T, false><<<(unsigned)L, 128, check_cta_smem(), stream>>>(L, nm, n, m, a0, w, z, err1, err2, flags,
+                                                                         ref_flags);
     return cudaGetLastError();
   }
   const long blocks = std::min<long>((L + CKW_WARPS - 1) / CKW_WARPS, 65535);
@@ -2189,7 +2192,10 @@ cudaError_t check_packed_run(long L, int n, const T *ap, const T *w, const T *z,
     cudaError_t e = launch_check_tc<T, true>(L, 0, ldz, n, n, ap, w, z, err1, err2, flags, nullptr, stream);
     if (e != cudaSuccess) return e;
   } else if (n > 32) {
-    k_check_cta<T, true><<<(unsigned)L, 256, 0, stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags, nullptr);
+    cudaError_t e = set_smem(k_check_cta<T, true>, check_cta_smem());
+    if (e != cudaSuccess) return e;
+    k_check_cta<T, true><<<(unsigned)L, 128, check_cta_smem(), stream>>>(L, ldz, n, n, ap, w, z, err1, err2, flags,
+                                                                        nullptr);
   } else {
     const long blocks = std::min<long>((L + CKW_WARPS - 1) / CKW_WARPS, 65535);
     cudaError_t e = set_smem(k_check_w<T, true>, check_w_smem());
