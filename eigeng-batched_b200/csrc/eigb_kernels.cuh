@@ -19,10 +19,10 @@
 //   k3_tmem        phase 3 for n > 32 with rows of up to 512 32-bit
 //                  columns: rows of Z in tensor memory
 //   k_jacobi_warp  cyclic Jacobi for n <= 32 (jac_tiled.hpp:3-152)
-//   k_check_w      FP64 residual / orthogonality gate (eigen_GPU_check.cu),
-//                  one warp per matrix for n <= 32; k_check_cta (n <= 64)
-//                  and k_check_tc (above, on the FP64 tensor cores) the
-//                  tiled forms
+//   k_check_w      FP64 residual / orthogonality gate (eigen_GPU_check.cu)
+//                  on the FP64 tensor cores, one warp per matrix for
+//                  n <= 32; k_check_cta (one CTA per matrix, n <= 64) and
+//                  k_check_tc (128 x 128 tiles, above) the larger forms
 #pragma once
 #include <stdio.h>
 
