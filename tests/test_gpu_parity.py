@@ -245,13 +245,16 @@ def test_reference_check_api_writes_flags():
     assert flags[2, 0] > 0 and flags[2, 1] > 0
 
 
-@pytest.mark.parametrize("n,nm,m", [(20, 20, 20), (40, 43, 40), (100, 100, 77), (200, 201, 200)])
+@pytest.mark.parametrize("n,nm,m", [(20, 20, 20), (30, 33, 17), (40, 43, 40), (48, 50, 31), (64, 64, 64),
+                                     (100, 100, 77), (128, 130, 128), (200, 201, 200)])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_gate_norms_match_numpy(oracle_mod, n, nm, m, dtype):
-    """eigen_GPU_check_ex (one warp per matrix for n <= 32, tiled CTA form
-    above): ||A Z - Z D||_F over the first m pairs and ||Z^T Z - I||_F
+    """eigen_GPU_check_ex (one warp per matrix for n <= 32, one CTA per
+    matrix for n <= 64, 128 x 128 tiles above, all on the FP64 tensor
+    cores): ||A Z - Z D||_F over the first m pairs and ||Z^T Z - I||_F
     (m x m) in FP64, on eigenvectors perturbed by ~1e-6 so that the norms
-    are far above rounding."""
+    are far above rounding; m < n and padded leading dimensions in each
+    form."""
     import ctypes
     import eigeng_b200 as e
     O = oracle_mod
