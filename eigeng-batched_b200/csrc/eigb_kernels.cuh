@@ -1612,6 +1612,7 @@ __global__ void __launch_bounds__(512, 1) k_check_tc(const long L, const int lda
     int ti, tj;
     tile_of(tile, ti, tj);
     const int i0 = ti * TILE, j0 = tj * TILE, ilim = res ? n : m;
+    const bool same = !res && ti == tj;  // a diagonal tile of Z^T Z: P would equal Q, only Q is loaded
     T *P = Pb + b * PANEL, *Q = Qb + b * PANEL;
     const int kc = c * KC;
 #pragma unroll
@@ -1632,7 +1633,7 @@ __global__ void __launch_bounds__(512, 1) k_check_tc(const long L, const int lda
         }
       }
       if (qin) qs = zz + kk + (size_t)j * ldz;  // Z(k, j)
-      ck_cp_async<sizeof(T)>(&P[cc * LDP + rr], ps, pin);
+      if (!same) ck_cp_async<sizeof(T)>(&P[cc * LDP + rr], ps, pin);
       ck_cp_async<sizeof(T)>(&Q[cc * LDP + rr], qs, qin);
     }
     ck_commit();
@@ -1688,8 +1689,8 @@ __global__ void __launch_bounds__(512, 1) k_check_tc(const long L, const int lda
           }
         } else {
 #pragma unroll
-          for (int ks = 0; ks < KC; ks += 4) {
-            const double a0f = (double)P[ks * LDP + 8 * R0], a1f = (double)P[ks * LDP + 8 * R1];
+          for (int ks = 0; ks < KC; ks += 4) {  // the A operand Z^T from the Q panel (P was not loaded)
+            const double a0f = (double)Q[ks * LDP + 8 * R0], a1f = (double)Q[ks * LDP + 8 * R1];
             double bf[8];
 #pragma unroll
             for (int x = 0; x < 8; x++) bf[x] = h + 2 * x >= R0 ? (double)Q[ks * LDP + 8 * (h + 2 * x)] : 0.0;
