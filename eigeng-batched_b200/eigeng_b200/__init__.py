@@ -539,6 +539,18 @@ def symfunc(v, w, n, func=FUNC_POW, p=0.5, nm=None, z=None, stream=None):
     return z
 
 
+def host_chunks(L, chunk=0):
+    """Chunk boundaries of solve_host for a batch of L matrices: equal
+    chunks of ``chunk`` (the last one ragged) when ``chunk`` > 0; else, from
+    L = 2048 on, 17 chunks of about L/16 with half-size first and last ones;
+    below that one chunk."""
+    if chunk > 0:
+        return list(range(0, L, chunk)) + [L]
+    if L >= 2048:
+        return [0] + [(L * (2 * k - 1) + 16) // 32 for k in range(1, 17)] + [L]
+    return [0, L]
+
+
 def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True, max_sweep=100,
                stream=None, device=None, z_host=None, info_host=None):
     """Solves a batch held in host memory (pinned for the copies to be
@@ -581,12 +593,7 @@ def solve_host(a_host, n, nm=None, w_host=None, chunk=0, method=TQL2, sort=True,
     # 18.73 -> 15.66, n=200 L=2048 61.1 -> 50.5, n=256 L=2048 104.7 -> 91.6;
     # FP32 n=128 L=4096 12.44 -> 10.43.  Four streams instead of eight lose
     # most of it (n=128 FP64 18.98 ms).
-    if chunk > 0:
-        bounds = list(range(0, L, chunk)) + [L]
-    elif L >= 2048:
-        bounds = [0] + [(L * (2 * k - 1) + 16) // 32 for k in range(1, 17)] + [L]
-    else:
-        bounds = [0, L]
+    bounds = host_chunks(L, chunk)
     nch = len(bounds) - 1
     C = max(bounds[i + 1] - bounds[i] for i in range(nch))
     # concurrent chunks, each with its own stream and workspace, and two

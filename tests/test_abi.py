@@ -121,3 +121,24 @@ def test_launch_params_report_the_launched_geometry(tmp_path):
     finally:
         E.tune_set([])
     assert (lp["grpSZ"], lp["numGR"], lp["numTH"]) == (8 * 512, 1, 512) and lp["numTB"] % 8 == 0
+
+
+@pytest.mark.parametrize("L,chunk", [(1, 0), (37, 0), (2047, 0), (2048, 0), (2049, 0), (3000, 0), (4096, 0),
+                                     (100000, 0), (37, 2), (37, 5), (4096, 1000)])
+def test_host_chunk_schedule(L, chunk):
+    """solve_host's chunks tile [0, L) in order: the given size (last one
+    ragged), else 17 chunks from L = 2048 on (half-size ends, the middle
+    ones within one matrix of L/16), else one."""
+    import eigeng_b200 as E
+    b = E.host_chunks(L, chunk)
+    assert b[0] == 0 and b[-1] == L
+    sizes = [b[i + 1] - b[i] for i in range(len(b) - 1)]
+    assert all(x > 0 for x in sizes)
+    if chunk > 0:
+        assert all(x == chunk for x in sizes[:-1]) and 0 < sizes[-1] <= chunk
+    elif L >= 2048:
+        assert len(sizes) == 17
+        assert all(abs(x - L / 16) <= 1 for x in sizes[1:-1])
+        assert all(abs(x - L / 32) <= 1 for x in (sizes[0], sizes[-1]))
+    else:
+        assert sizes == [L]
